@@ -1,0 +1,367 @@
+"""Drop-in ``ContactSolver`` / ``solve_nested`` / ``ContactResult`` for the
+fft and periodic backends, running on the B200 through libaspher_b200.so.
+
+Mirrors the pybind11 surface of the reference (python/bindings.cpp:115-234
+``PyContactSolver``, :362-432 ``py_solve_nested``, :637-879 the module defs):
+same argument names, defaults, result fields and errors (ValueError for
+invalid input, a status string for numerical outcomes).  PyTorch provides
+the device memory and the current CUDA stream; all arithmetic runs in the
+library's sm_100a kernels.
+"""
+
+import ctypes as C
+import time
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev():
+    if not torch.cuda.is_available():
+        raise RuntimeError("aspher_b200 needs a CUDA device (no CPU fallback)")
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _as_vector(a, expected, name="array"):
+    a = np.ascontiguousarray(np.asarray(a, dtype=np.float64)).reshape(-1)
+    if a.size != expected:
+        raise ValueError("%s has %d entries, expected %d" % (name, a.size, expected))
+    return a
+
+
+class Operator:
+    """Device operator handle (free-space FFT or periodic)."""
+
+    def __init__(self, backend, grid_size, domain_size=1.0, E_star=1.0):
+        if backend not in L.BACKEND:
+            raise ValueError("unknown backend: %s (this build implements 'fft' and "
+                             "'periodic')" % backend)
+        _dev()
+        self.backend = backend
+        self.Ns = int(grid_size)
+        self.N = self.Ns * self.Ns
+        self.domain_size = float(domain_size)
+        self.E_star = float(E_star)
+        h = C.c_void_p()
+        L.check(L.lib().aspher_op_create(L.BACKEND[backend], self.Ns, self.domain_size,
+                                         self.E_star, C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                L.lib().aspher_op_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def matvec_(self, x, y):
+        """y = S x on device tensors (float32 or float64, Ns*Ns, contiguous)."""
+        dt = L.F64 if x.dtype == torch.float64 else L.F32
+        if x.dtype not in (torch.float32, torch.float64) or y.dtype != x.dtype:
+            raise ValueError("matvec: float32/float64 tensors of one dtype expected")
+        if x.numel() != self.N or y.numel() != self.N:
+            raise ValueError("matvec: x size != Ns*Ns")
+        if not (x.is_contiguous() and y.is_contiguous()):
+            raise ValueError("matvec: contiguous tensors expected")
+        L.check(L.lib().aspher_op_matvec(self._h, dt, _ptr(x), _ptr(y), _stream()))
+        return y
+
+    def info(self):
+        inf = L.OpInfo()
+        L.check(L.lib().aspher_op_get_info(self._h, C.byref(inf)))
+        return inf
+
+    def love_table(self):
+        out = np.empty((self.Ns, self.Ns), dtype=np.float64)
+        L.check(L.lib().aspher_op_love_table(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def precond_(self, precond, g, contact, z, radius=2):
+        dt = L.F64 if g.dtype == torch.float64 else L.F32
+        L.check(L.lib().aspher_precond_apply(self._h, L.PRECOND[precond], int(radius), dt,
+                                             _ptr(g), _ptr(contact), _ptr(z), _stream()))
+        return z
+
+
+def stencil_taps(grid_size, radius=2):
+    cap = 64
+    dx = (C.c_int * cap)()
+    dy = (C.c_int * cap)()
+    w = (C.c_double * cap)()
+    n = C.c_int()
+    L.check(L.lib().aspher_stencil_taps(int(grid_size), int(radius), dx, dy, w, cap,
+                                        C.byref(n)))
+    return list(dx[:n.value]), list(dy[:n.value]), list(w[:n.value])
+
+
+class ContactResult:
+    """Fields of the reference ``ContactResult`` (bindings.cpp:637-802)."""
+
+    def __init__(self, res, Ns, pressure, displacement=None, gap=None, history=None):
+        self._r = res
+        self.Ns = Ns
+        self._p = pressure
+        self._u = displacement
+        self._g = gap
+        self.error_history = np.asarray(history if history is not None else [], np.float64)
+        self.stage_stats = []
+        self.time_build = 0.0
+        self.time_coarse = 0.0
+        self.active_rounds = 0
+        self.active_fallback = False
+
+    def _grid(self, t):
+        if t is None:
+            return None
+        if isinstance(t, torch.Tensor):
+            return t.detach().to("cpu").numpy().reshape(self.Ns, self.Ns)
+        return np.asarray(t).reshape(self.Ns, self.Ns)
+
+    @property
+    def pressure(self):
+        return self._grid(self._p)
+
+    @property
+    def pressure_device(self):
+        return self._p
+
+    @property
+    def displacement(self):
+        return self._grid(self._u)
+
+    @property
+    def gap(self):
+        return self._grid(self._g)
+
+    status = property(lambda s: L.STATUS_NAMES[s._r.status]
+                      if 0 <= s._r.status < len(L.STATUS_NAMES) else "unknown")
+    status_reason = property(lambda s: s._r.status_reason.decode())
+    iterations = property(lambda s: s._r.iterations)
+    converged = property(lambda s: bool(s._r.converged))
+    contact_area = property(lambda s: s._r.contact_fraction)
+    contact_fraction = property(lambda s: s._r.contact_fraction)
+    mean_pressure = property(lambda s: s._r.mean_pressure)
+    approach = property(lambda s: s._r.approach)
+    objective = property(lambda s: s._r.objective)
+    error = property(lambda s: s._r.error)
+    pk_error = property(lambda s: s._r.pk_error)
+    fw_gap = property(lambda s: s._r.fw_gap)
+    fw_error = property(lambda s: s._r.fw_error)
+    load_error = property(lambda s: s._r.load_error)
+    pressure_violation = property(lambda s: s._r.pressure_violation)
+    penetration_error = property(lambda s: s._r.penetration_error)
+    requested_tol = property(lambda s: s._r.requested_tol)
+    effective_tol = property(lambda s: s._r.effective_tol)
+    p_ref = property(lambda s: s._r.p_ref)
+    g_ref = property(lambda s: s._r.g_ref)
+    matvec_count = property(lambda s: s._r.matvec_count)
+    verification_matvec_count = property(lambda s: 0)
+    precond_count = property(lambda s: s._r.precond_count)
+    identification_steps = property(lambda s: s._r.identification_steps)
+    returned_best = property(lambda s: bool(s._r.returned_best))
+    precond_dropped = property(lambda s: False)
+    validation_scope = property(lambda s: "solve_operator")
+    operator_error_kind = property(lambda s: "unavailable")
+    operator_error = property(lambda s: None)
+    objective_error_bound = property(lambda s: None)
+
+    @property
+    def memory(self):
+        r = self._r
+        return dict(cg_state=r.mem_cg_state, best_iterate=r.mem_best_iterate,
+                    contact_mask=r.mem_contact_mask, output_arrays=r.mem_output_arrays,
+                    peak=r.mem_peak)
+
+    @property
+    def timings(self):
+        return dict(total=self._r.time_total, matvec=0.0, precond=0.0, build=self.time_build,
+                    coarse=self.time_coarse, verification=0.0, candidate=0.0, output=0.0)
+
+    def __repr__(self):
+        return ("<ContactResult: %s in %d iters, fw_error %g, penetration %g, contact area %g,"
+                " mean p %g>" % (self.status, self.iterations, self.fw_error,
+                                 self.penetration_error, self.contact_area,
+                                 self.mean_pressure))
+
+
+def solve_device(op, g0, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precond="none",
+                 p_init=None, dtype=torch.float64, light=False, record_history=False,
+                 keep_best=None, requested_tol=0.0, allow_tolerance_relaxation=False,
+                 g_ref=0.0, p_ref=0.0, datum_mode="automatic", datum=0.0, precond_radius=2,
+                 load_tol=0.0, stall_limit=200, pressure_out=None):
+    """solve_contact_impl<Real> on device tensors (Real = dtype).
+
+    g0 / p_init: device tensors of ``dtype`` (Ns*Ns); the FP64 pressure is
+    written to ``pressure_out`` (allocated when None) and stays on the device.
+    """
+    N = op.N
+    if g0.numel() != N:
+        raise ValueError("array has %d entries, expected %d" % (g0.numel(), N))
+    if precond not in L.PRECOND:
+        raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
+    dev = g0.device
+    g0 = g0.to(dtype).contiguous()
+    if p_init is not None:
+        p_init = p_init.to(device=dev, dtype=dtype).contiguous().reshape(-1)
+        if p_init.numel() != N:
+            raise ValueError("solve_contact: p_init size mismatch")
+    o = L.SolveOpts()
+    L.lib().aspher_solve_opts_default(C.byref(o))
+    o.tol = float(tol)
+    o.requested_tol = float(requested_tol)
+    o.max_iter = int(max_iter)
+    o.use_pr = int(bool(use_pr))
+    o.light = int(bool(light))
+    o.record_history = int(bool(record_history))
+    o.keep_best = int(not light) if keep_best is None else int(bool(keep_best))
+    o.load_tol = float(load_tol)
+    o.stall_limit = int(stall_limit)
+    o.allow_tolerance_relaxation = int(bool(allow_tolerance_relaxation))
+    o.precond = L.PRECOND[precond]
+    o.precond_radius = int(precond_radius)
+    o.p_ref = float(p_ref)
+    o.g_ref = float(g_ref)
+    o.datum_mode = L.DATUM[datum_mode]
+    o.datum = float(datum)
+    o.dtype = L.F64 if dtype == torch.float64 else L.F32
+    p_out = pressure_out if pressure_out is not None else torch.empty(N, dtype=torch.float64,
+                                                                    device=dev)
+    u_out = g_out = None
+    if not light:
+        u_out = torch.empty(N, dtype=torch.float64, device=dev)
+        g_out = torch.empty(N, dtype=torch.float64, device=dev)
+    hist = None
+    hcap = 0
+    if record_history:
+        hcap = int(max_iter) + 1
+        hist = np.zeros(hcap, dtype=np.float64)
+    res = L.Result()
+    L.check(L.lib().aspher_solve(
+        op.handle, C.byref(o), _ptr(g0), C.c_double(float(p_nominal)), _ptr(p_init),
+        _ptr(p_out), _ptr(u_out), _ptr(g_out),
+        hist.ctypes.data_as(C.c_void_p) if hist is not None else C.c_void_p(0), hcap,
+        C.byref(res), _stream()))
+    h = hist[:res.history_len].copy() if hist is not None else None
+    return ContactResult(res, op.Ns, p_out, u_out, g_out, h)
+
+
+class ContactSolver:
+    """``aspher.ContactSolver`` for backend='fft' / 'periodic' (bindings.cpp:805-834).
+
+    The H-matrix / H2 / dense arguments are accepted for signature
+    compatibility and ignored; any backend other than 'fft' or 'periodic'
+    raises ValueError (those backends are not part of this build).
+    """
+
+    def __init__(self, grid_size, domain_size=1.0, E_star=1.0, eta=2.0, aca_tol=1e-6,
+                 leaf_size=64, use_hmatrix=True, use_acagp=False, central_fraction=0.3,
+                 inline_svd_tol=0.0, backend="", q=4, near_radius=1, h2_leaf_side=8):
+        if grid_size <= 0:
+            raise ValueError("grid_size must be positive")
+        if not domain_size > 0.0:
+            raise ValueError("domain_size must be positive")
+        if not E_star > 0.0:
+            raise ValueError("E_star must be positive")
+        if backend == "":
+            backend = "hmatrix" if use_hmatrix else "dense"
+        if backend not in ("fft", "periodic"):
+            raise ValueError("unknown backend: %s (aspher_b200 implements 'fft' and "
+                             "'periodic')" % backend)
+        self.Ns = int(grid_size)
+        self.backend = backend
+        self.op = Operator(backend, grid_size, domain_size, E_star)
+
+    def matvec(self, p):
+        """u = S p for a float64 array of shape (N,) or (Ns, Ns); returns (N,)."""
+        v = _as_vector(p, self.Ns * self.Ns)
+        dev = _dev()
+        x = torch.from_numpy(v).to(dev)
+        y = torch.empty_like(x)
+        self.op.matvec_(x, y)
+        return y.cpu().numpy()
+
+    def solve(self, gap, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precond="none",
+              p_init=None, *, precision="double"):
+        """Normal contact solve (bindings.cpp:186-234); always FP64 by default.
+
+        ``precision`` (keyword-only extension): 'double' (reference),
+        'float' (FP32 vectors and transforms, FP64 reductions) or
+        'float_then_double' (FP32 at tol, then an FP64 polish).
+        """
+        N = self.Ns * self.Ns
+        g0 = _as_vector(gap, N, "array")
+        if precond not in ("none", "", "fourier", "fourier-fft"):
+            raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
+        if not np.all(np.isfinite(g0)):
+            raise ValueError("solve_contact: g0 contains non-finite values")
+        dev = _dev()
+        g0d = torch.from_numpy(g0).to(dev)
+        p0 = None
+        if p_init is not None:
+            p0 = torch.from_numpy(_as_vector(p_init, N)).to(dev)
+        t0 = time.perf_counter()
+        if precision == "double":
+            r = solve_device(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
+                             torch.float64)
+        elif precision in ("float", "float_then_double"):
+            r = _solve_float(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
+                             polish=(precision == "float_then_double"))
+        else:
+            raise ValueError("precision must be 'double', 'float' or 'float_then_double'")
+        r.wall = time.perf_counter() - t0
+        return r
+
+    def hmatrix_info(self):
+        inf = self.op.info()
+        d = {"backend": self.backend, "n": int(inf.n)}
+        if self.backend == "fft":
+            d.update(padded_side=int(inf.padded_side), bytes=int(inf.bytes_total),
+                     bytes_spectrum=int(inf.bytes_spectrum),
+                     bytes_scratch=int(inf.bytes_scratch),
+                     compression=float(inf.bytes_total) / (8.0 * inf.n * inf.n))
+        else:
+            d.update(periodic_x=True, periodic_y=True, bytes_scratch=int(inf.bytes_scratch))
+        return d
+
+
+def _solve_float(op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0, polish,
+                 float_floor=None):
+    """FP32 stage (datum removed inside the cast, nested_solve.cpp:871-917),
+    optionally followed by an FP64 polish warm-started from it (:931-974)."""
+    gmin, gmax = float(g0d.min()), float(g0d.max())
+    datum = gmin + 0.5 * (gmax - gmin)
+    g_ref = gmax - gmin
+    gf = (g0d - datum).to(torch.float32)
+    tol_f = tol if float_floor is None else max(tol, float_floor)
+    r = solve_device(op, gf, p_nominal, tol_f, max_iter, use_pr, precond,
+                     None if p0 is None else p0.to(torch.float32), torch.float32,
+                     g_ref=g_ref, datum_mode="caller", datum=datum,
+                     requested_tol=tol, allow_tolerance_relaxation=polish)
+    if not polish:
+        return r
+    before = r
+    r = solve_device(op, g0d, p_nominal, tol, max_iter, use_pr, precond,
+                     before.pressure_device, torch.float64, g_ref=g_ref,
+                     datum_mode="solver", datum=datum)
+    r.stage_stats = [dict(name="float", precision="float", iterations=before.iterations,
+                          status=before.status),
+                     dict(name="polish", precision="double", iterations=r.iterations,
+                          status=r.status)]
+    r.float_iterations = before.iterations
+    return r

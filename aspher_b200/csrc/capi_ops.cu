@@ -1,0 +1,114 @@
+// C-ABI entry points for the operators (declared in include/aspher_b200.h).
+// No exception crosses this boundary: every call returns an int status and
+// leaves a message for aspher_last_error().
+#include "../../include/aspher_b200.h"
+#include "ops.hpp"
+
+#include <cstring>
+#include <string>
+
+namespace asb {
+thread_local std::string g_last_error;
+void set_last_error(const std::string& m) { g_last_error = m; }
+}  // namespace asb
+
+struct aspher_op {
+    asb::Operator* impl;
+};
+
+#define ASB_API_BEGIN try {
+#define ASB_API_END                                               \
+    }                                                             \
+    catch (const asb::Error& e) {                                 \
+        asb::set_last_error(e.what());                            \
+        return e.code;                                            \
+    }                                                             \
+    catch (const std::exception& e) {                             \
+        asb::set_last_error(e.what());                            \
+        return ASPHER_ECUDA;                                      \
+    }                                                             \
+    catch (...) {                                                 \
+        asb::set_last_error("unknown error");                     \
+        return ASPHER_ECUDA;                                      \
+    }
+
+extern "C" {
+
+int aspher_abi_version(void) { return ASPHER_B200_ABI_VERSION; }
+
+const char* aspher_last_error(void) { return asb::g_last_error.c_str(); }
+
+int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
+                     aspher_op** out) {
+    ASB_API_BEGIN
+    if (!out) throw asb::Error(ASPHER_EINVAL, "aspher_op_create: out is NULL");
+    *out = nullptr;
+    if (backend != ASPHER_BACKEND_FFT && backend != ASPHER_BACKEND_PERIODIC)
+        throw asb::Error(ASPHER_EINVAL, "unknown backend (expected fft or periodic)");
+    auto* op = new aspher_op{nullptr};
+    try {
+        op->impl = new asb::Operator(backend, grid_size, domain_size, E_star);
+    } catch (...) {
+        delete op;
+        throw;
+    }
+    *out = op;
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_destroy(aspher_op* op) {
+    ASB_API_BEGIN
+    if (!op) return ASPHER_OK;
+    delete op->impl;
+    delete op;
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_matvec(aspher_op* op, int dtype, const void* x, void* y, void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl) throw asb::Error(ASPHER_EINVAL, "aspher_op_matvec: NULL operator");
+    if (!x || !y) throw asb::Error(ASPHER_EINVAL, "aspher_op_matvec: NULL buffer");
+    if (dtype != ASPHER_F32 && dtype != ASPHER_F64)
+        throw asb::Error(ASPHER_EINVAL, "aspher_op_matvec: dtype must be F32 or F64");
+    const size_t align = dtype == ASPHER_F64 ? 16 : 8;
+    if (((uintptr_t)x % align) || ((uintptr_t)y % align))
+        throw asb::Error(ASPHER_EINVAL, "aspher_op_matvec: buffers must be 16-byte aligned");
+    op->impl->matvec(dtype == ASPHER_F64, x, y, static_cast<cudaStream_t>(stream));
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_get_info(const aspher_op* op, aspher_op_info* info) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !info) throw asb::Error(ASPHER_EINVAL, "aspher_op_get_info: NULL");
+    const asb::Operator& o = *op->impl;
+    std::memset(info, 0, sizeof(*info));
+    info->backend = o.kind;
+    info->grid_size = o.Ns;
+    info->padded_side = o.kind == asb::OP_FFT ? 2 * o.Ns : o.Ns;
+    info->n = (int64_t)o.Ns * o.Ns;
+    if (o.kind == asb::OP_FFT) {
+        info->bytes_spectrum = (int64_t)(o.Ns / o.ct_d + 1) * (o.Ns + 1) * o.ct_d * 8 +
+                               (int64_t)(o.Ns / o.ct_f + 1) * (o.Ns + 1) * o.ct_f * 4;
+    }
+    info->bytes_scratch = (int64_t)(o.spec_d_bytes + o.spec_f_bytes);
+    info->bytes_total = (int64_t)o.resident_bytes();
+    info->max_im_ratio = o.max_im_ratio;
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_love_table(const aspher_op* op, double* host_out) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !host_out) throw asb::Error(ASPHER_EINVAL, "aspher_op_love_table: NULL");
+    if (op->impl->kind != asb::OP_FFT || !op->impl->table)
+        throw asb::Error(ASPHER_EINVAL, "aspher_op_love_table: only the fft backend has a table");
+    const size_t n = (size_t)op->impl->Ns * op->impl->Ns;
+    ASB_CUDA(cudaMemcpy(host_out, op->impl->table, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,125 @@
+// C-ABI entry points of the solver and the preconditioners.
+#include "../../include/aspher_b200.h"
+#include "ops.hpp"
+#include "pcg.hpp"
+
+#include <cstring>
+
+struct aspher_op {
+    asb::Operator* impl;
+};
+
+#define ASB_API_BEGIN try {
+#define ASB_API_END                                               \
+    }                                                             \
+    catch (const asb::Error& e) {                                 \
+        asb::set_last_error(e.what());                            \
+        return e.code;                                            \
+    }                                                             \
+    catch (const std::exception& e) {                             \
+        asb::set_last_error(e.what());                            \
+        return ASPHER_ECUDA;                                      \
+    }                                                             \
+    catch (...) {                                                 \
+        asb::set_last_error("unknown error");                     \
+        return ASPHER_ECUDA;                                      \
+    }
+
+extern "C" {
+
+const char* aspher_status_string(int s) {
+    switch (s) {
+        case ASPHER_CONVERGED: return "converged";
+        case ASPHER_STAGNATED: return "stagnated";
+        case ASPHER_MAX_ITERATIONS: return "max_iterations";
+        case ASPHER_NONPOSITIVE_CURVATURE: return "nonpositive_curvature";
+        case ASPHER_NONFINITE: return "nonfinite";
+        case ASPHER_VERIFICATION_FAILED: return "verification_failed";
+        case ASPHER_RESOURCE_LIMIT: return "resource_limit";
+    }
+    return "unknown";
+}
+
+void aspher_solve_opts_default(aspher_solve_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-8;
+    o->requested_tol = 0.0;
+    o->max_iter = 5000;
+    o->use_pr = 1;
+    o->light = 0;
+    o->record_history = 0;
+    o->keep_best = 1;
+    o->load_tol = 0.0;
+    o->stall_limit = 200;
+    o->allow_tolerance_relaxation = 0;
+    o->precond = ASPHER_PRECOND_NONE;
+    o->precond_radius = 2;
+    o->p_ref = 0.0;
+    o->g_ref = 0.0;
+    o->datum_mode = ASPHER_DATUM_AUTOMATIC;
+    o->datum = 0.0;
+    o->dtype = ASPHER_F64;
+}
+
+int aspher_solve(aspher_op* op, const aspher_solve_opts* opts, const void* g0_dev, double p_bar,
+                 const void* p_init_dev, double* pressure_dev, double* displacement_dev,
+                 double* gap_dev, double* history_host, int history_cap, aspher_result* res,
+                 void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !opts || !g0_dev || !pressure_dev || !res)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve: NULL argument");
+    if (opts->dtype != ASPHER_F32 && opts->dtype != ASPHER_F64)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve: dtype must be F32 or F64");
+    const uintptr_t a = (uintptr_t)g0_dev | (uintptr_t)pressure_dev |
+                        (uintptr_t)p_init_dev | (uintptr_t)displacement_dev |
+                        (uintptr_t)gap_dev;
+    if (a % 16) throw asb::Error(ASPHER_EINVAL, "aspher_solve: buffers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (opts->dtype == ASPHER_F64)
+        asb::solve_impl<double>(*op->impl, *opts, g0_dev, p_bar, p_init_dev, pressure_dev,
+                                displacement_dev, gap_dev, history_host, history_cap, *res, s);
+    else
+        asb::solve_impl<float>(*op->impl, *opts, g0_dev, p_bar, p_init_dev, pressure_dev,
+                               displacement_dev, gap_dev, history_host, history_cap, *res, s);
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_precond_apply(aspher_op* op, int precond, int radius, int dtype, const void* g_dev,
+                         const uint8_t* contact_dev, void* z_dev, void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !g_dev || !contact_dev || !z_dev)
+        throw asb::Error(ASPHER_EINVAL, "aspher_precond_apply: NULL argument");
+    if (precond != ASPHER_PRECOND_STENCIL && precond != ASPHER_PRECOND_FFT)
+        throw asb::Error(ASPHER_EINVAL, "aspher_precond_apply: precond must be STENCIL or FFT");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == ASPHER_F64)
+        asb::precond_apply_impl<double>(*op->impl, precond, radius, (const double*)g_dev,
+                                        contact_dev, (double*)z_dev, s);
+    else if (dtype == ASPHER_F32)
+        asb::precond_apply_impl<float>(*op->impl, precond, radius, (const float*)g_dev,
+                                       contact_dev, (float*)z_dev, s);
+    else
+        throw asb::Error(ASPHER_EINVAL, "aspher_precond_apply: dtype must be F32 or F64");
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_stencil_taps(int grid_size, int radius, int* dx, int* dy, double* w, int cap,
+                        int* ntaps) {
+    ASB_API_BEGIN
+    if (!dx || !dy || !w || !ntaps) throw asb::Error(ASPHER_EINVAL, "aspher_stencil_taps: NULL");
+    const asb::StencilTaps t = asb::make_stencil_taps(grid_size, radius);
+    const int n = t.n < cap ? t.n : cap;
+    for (int i = 0; i < n; ++i) {
+        dx[i] = t.dx[i];
+        dy[i] = t.dy[i];
+        w[i] = t.w[i];
+    }
+    *ntaps = t.n;
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+}  // extern "C"

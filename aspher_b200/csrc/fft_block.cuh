@@ -1,0 +1,164 @@
+// Register-resident Stockham FFT for one CTA-cooperative transform.
+//
+// A length-L complex transform is carried by L/RPT threads, each holding RPT
+// elements in registers.  Thread t always holds elements t + m*(L/RPT),
+// m = 0..RPT-1 (the "strided pattern") before and after the transform, and
+// the output is in natural order.  The transform is the Stockham autosort
+// formulation (Govindaraju et al., "High performance discrete Fourier
+// transforms on graphics processors", SC'08): stage s with radix R and span
+// Ns reads x[j + r L/R], twiddles input r by w_{Ns R}^{r (j mod Ns)}, does a
+// radix-R DFT and writes y[(j div Ns) Ns R + (j mod Ns) + r Ns].  Each thread
+// runs RPT/R butterflies per stage (j = t + q L/RPT), whose inputs are exactly
+// its own strided registers, so only the stage outputs go through shared
+// memory; the last stage's outputs land back in the strided pattern and stay
+// in registers.  Stages are radix 16 (the remainder last), so a 4096-point
+// transform makes two shared-memory round trips.
+//
+// Shared memory is addressed as (i + i/16) * S + off: the 1-in-16 padding
+// breaks the power-of-two strides of the stage writes, S > 1 interleaves S
+// independent transforms element by element (the column kernels).
+#pragma once
+
+#include "common.cuh"
+
+namespace asb {
+
+// cos/sin(2 pi k / 16), k = 0..7, as plain mathematical constants.
+template <typename T>
+__device__ __forceinline__ void unit16(int k, T& c, T& s) {
+    const T c1 = T(0.92387953251128675613), s1 = T(0.38268343236508977173);
+    const T h = T(0.70710678118654752440);
+    switch (k) {
+        case 0: c = T(1); s = T(0); break;
+        case 1: c = c1; s = s1; break;
+        case 2: c = h; s = h; break;
+        case 3: c = s1; s = c1; break;
+        case 4: c = T(0); s = T(1); break;
+        case 5: c = -s1; s = c1; break;
+        case 6: c = -h; s = h; break;
+        default: c = -c1; s = s1; break;
+    }
+}
+
+// a * exp(DIR * 2 pi i k / R) for a compile-time R in {2,4,8,16}.
+template <int R, int DIR, typename T>
+__device__ __forceinline__ cplx<T> rot_const(cplx<T> a, int k) {
+    const int k16 = k * (16 / R);
+    if (k16 == 0) return a;
+    if (k16 == 4) return mul_i<DIR>(a);
+    T c, s;
+    unit16<T>(k16, c, s);
+    const T sn = DIR < 0 ? -s : s;
+    return mk<T>(a.x * c - a.y * sn, a.x * sn + a.y * c);
+}
+
+// In-register DFT of R points (natural order in and out), radix-2 DIT split.
+template <int R, int DIR, typename T>
+__device__ __forceinline__ void dft(cplx<T>* a) {
+    if constexpr (R == 1) {
+        return;
+    } else if constexpr (R == 2) {
+        const cplx<T> t = a[0];
+        a[0] = cadd(t, a[1]);
+        a[1] = csub(t, a[1]);
+    } else if constexpr (R == 4) {
+        const cplx<T> s02 = cadd(a[0], a[2]), d02 = csub(a[0], a[2]);
+        const cplx<T> s13 = cadd(a[1], a[3]);
+        const cplx<T> d13 = mul_i<DIR>(csub(a[1], a[3]));
+        a[0] = cadd(s02, s13);
+        a[2] = csub(s02, s13);
+        a[1] = cadd(d02, d13);
+        a[3] = csub(d02, d13);
+    } else {
+        cplx<T> e[R / 2], o[R / 2];
+#pragma unroll
+        for (int i = 0; i < R / 2; ++i) { e[i] = a[2 * i]; o[i] = a[2 * i + 1]; }
+        dft<R / 2, DIR, T>(e);
+        dft<R / 2, DIR, T>(o);
+#pragma unroll
+        for (int k = 0; k < R / 2; ++k) {
+            const cplx<T> w = rot_const<R, DIR, T>(o[k], k);
+            a[k] = cadd(e[k], w);
+            a[k + R / 2] = csub(e[k], w);
+        }
+    }
+}
+
+__host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
+
+// Radix of stage `s` for a length-L transform with at most RMAX per stage.
+__host__ __device__ constexpr int stage_radix(int L, int RMAX, int s) {
+    int rem = L;
+    for (int i = 0; i < s; ++i) rem /= (rem >= RMAX ? RMAX : rem);
+    return rem >= RMAX ? RMAX : rem;
+}
+__host__ __device__ constexpr int num_stages(int L, int RMAX) {
+    int n = 0, rem = L;
+    while (rem > 1) { rem /= (rem >= RMAX ? RMAX : rem); ++n; }
+    return n;
+}
+
+__device__ __forceinline__ int smaddr(int i, int S, int off) { return (i + (i >> 4)) * S + off; }
+
+// Shared-memory elements needed by one transform of length L (padded).
+__host__ __device__ constexpr int sm_len(int L) { return L + L / 16 + 1; }
+
+template <typename T, int L, int RPT, int DIR, int S, int STAGE, int SPAN>
+__device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
+                                           const cplx<T>* __restrict__ tw) {
+    constexpr int RMAX = RPT < 16 ? RPT : 16;
+    constexpr int NST = num_stages(L, RMAX);
+    if constexpr (STAGE < NST) {
+        constexpr int R = stage_radix(L, RMAX, STAGE);
+        constexpr int TT = L / RPT;   // threads per transform
+        constexpr int Q = RPT / R;    // butterflies per thread
+        constexpr bool LAST = (STAGE == NST - 1);
+        static_assert(RPT % R == 0, "radix must divide RPT");
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const int j = t + q * TT;
+            cplx<T> a[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) a[r] = v[q + r * Q];
+            if constexpr (SPAN > 1) {
+                const int jm = j % SPAN;
+                constexpr int TS = L / (SPAN * R);
+#pragma unroll
+                for (int r = 1; r < R; ++r) {
+                    const cplx<T> w = __ldg(&tw[r * jm * TS]);
+                    a[r] = DIR < 0 ? cmul(a[r], w) : cmulc(a[r], w);
+                }
+            }
+            dft<R, DIR, T>(a);
+            if constexpr (LAST) {
+#pragma unroll
+                for (int r = 0; r < R; ++r) v[q + r * Q] = a[r];
+            } else {
+                const int base = (j / SPAN) * SPAN * R + (j % SPAN);
+#pragma unroll
+                for (int r = 0; r < R; ++r) sm[smaddr(base + r * SPAN, S, off)] = a[r];
+            }
+        }
+        if constexpr (!LAST) {
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) v[m] = sm[smaddr(t + m * TT, S, off)];
+            __syncthreads();
+            fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R>(v, t, sm, off, tw);
+        }
+    }
+}
+
+// Length-L transform of the strided register pattern; DIR = -1 forward
+// (exp(-2 pi i jk/L)), +1 inverse, both unnormalised.  tw points at the
+// length-L table exp(-2 pi i k / L), k < L.  Every thread of the CTA must
+// call this (it contains __syncthreads), including threads whose transform
+// is a dummy.
+template <typename T, int L, int RPT, int DIR, int S>
+__device__ __forceinline__ void block_fft(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
+                                          const cplx<T>* __restrict__ tw) {
+    static_assert(L % RPT == 0, "L must be a multiple of RPT");
+    fft_stages<T, L, RPT, DIR, S, 0, 1>(v, t, sm, off, tw);
+}
+
+}  // namespace asb

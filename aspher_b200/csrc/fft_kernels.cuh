@@ -1,0 +1,194 @@
+// Row and column pass kernels of the 2-D real transforms.
+//
+// A 2-D r2c/c2r pair over an (nrows x 2*LR) real grid is split as:
+//   row_fwd : per row, the real FFT of length 2*LR via a length-LR complex
+//             FFT of z[n] = x[2n] + i x[2n+1] and the usual split step,
+//             producing the LR+1 half-spectrum columns;
+//   col     : per column, forward FFT of length LC, pointwise multiplier,
+//             inverse FFT (fused: the spectrum never leaves the CTA);
+//   row_inv : per row, the inverse split step and a length-LR complex FFT.
+// PAD=true is the zero-padded (Hockney) case of the free-space operator:
+// rows hold Ns real values padded to 2*Ns (so half of z is zero and those
+// registers are never loaded), and columns hold Ns values padded to LC=2*Ns
+// of which only the first Ns outputs are kept.
+//
+// The half spectrum lives in HBM in a column-tiled layout:
+//   elem(row, k) = base[(k / CT) * nrows * CT + row * CT + (k % CT)]
+// so a column CTA streams one contiguous tile and a row CTA of RB rows
+// touches RB*CT contiguous elements per tile.
+#pragma once
+
+#include "fft_block.cuh"
+
+namespace asb {
+
+template <typename T>
+struct TiledSpec {
+    cplx<T>* base;
+    int nrows;
+    int ct;
+    __device__ __forceinline__ size_t idx(int row, int k) const {
+        return (size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct);
+    }
+};
+
+// ---- launch shapes ----------------------------------------------------------
+__host__ __device__ constexpr int rpt_for(int L) { return L >= 16 ? 16 : L; }
+
+template <typename T>
+__host__ __device__ constexpr int row_rb(int LR) {
+    const int tt = LR / rpt_for(LR);
+    int rb = 512 / tt;
+    if (rb < 1) rb = 1;
+    if (rb > 16) rb = 16;
+    const int per_row = sm_len(LR + 1) * (int)sizeof(cplx<T>);
+    while (rb > 1 && rb * per_row > 100 * 1024) rb >>= 1;
+    return rb;
+}
+template <typename T>
+__host__ __device__ constexpr int row_smem(int LR) {
+    return row_rb<T>(LR) * sm_len(LR + 1) * (int)sizeof(cplx<T>);
+}
+template <typename T>
+__host__ __device__ constexpr int col_ct(int LC, int ncols_minus1) {
+    const int tt = LC / rpt_for(LC);
+    int ct = 16;
+    while (ct > 1 && (ct * tt > 512 ||
+                      ct * (sm_len(LC) + 1) * (int)sizeof(cplx<T>) > 200 * 1024 ||
+                      ct > ncols_minus1))
+        ct >>= 1;
+    return ct;
+}
+template <typename T>
+__host__ __device__ constexpr int col_smem(int LC, int ct) {
+    return (ct * sm_len(LC) + ct) * (int)sizeof(cplx<T>);
+}
+
+// ---- row forward ---------------------------------------------------------------
+// Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1])
+// Store: void operator()(int row, int k, cplx<T> X), k in [0, LR]
+//        static constexpr bool kFinish; when true, every thread calls
+//        finish(double* scratch) after a __syncthreads() at the end
+template <typename T, int LR, bool PAD, class Load, class Store>
+__global__ void __launch_bounds__(row_rb<T>(LR) * (LR / rpt_for(LR)), 1)
+row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
+               const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
+    if (gate && *gate) return;
+    constexpr int RPT = rpt_for(LR);
+    constexpr int TT = LR / RPT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    const int r = threadIdx.x / TT, t = threadIdx.x % TT;
+    const int row = blockIdx.x * row_rb<T>(LR) + r;
+    const bool valid = row < nrows;
+    const int off = r * sm_len(LR + 1);
+    cplx<T> v[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+        else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
+    }
+    block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        const int k = t + m * TT;
+        const cplx<T> zk = v[m];
+        const cplx<T> zn = sm[smaddr((LR - k) & (LR - 1), 1, off)];
+        // E = (Zk + conj Zn)/2, O = (Zk - conj Zn)/(2i), X = E + w^k O
+        const cplx<T> A = mk<T>(zk.x + zn.x, zk.y - zn.y);
+        const cplx<T> B = mk<T>(zk.x - zn.x, zk.y + zn.y);
+        const cplx<T> O = mk<T>(B.y * T(0.5), -B.x * T(0.5));
+        const cplx<T> w = __ldg(&tw_2lr[k]);
+        const cplx<T> X = cadd(cscale(A, T(0.5)), cmul(w, O));
+        if (valid) st(row, k, X);
+    }
+    if (t == 0 && valid) {
+        const cplx<T> z0 = v[0];
+        st(row, LR, mk<T>(z0.x - z0.y, T(0)));
+    }
+    if constexpr (Store::kFinish) {
+        __syncthreads();
+        st.finish(reinterpret_cast<double*>(smraw));
+    }
+}
+
+// ---- row inverse ----------------------------------------------------------------
+// Load:  cplx<T> operator()(int row, int k), k in [0, LR]
+// Store: void operator()(int row, int n, cplx<T> z) -> (x[2n], x[2n+1]);
+//        static constexpr bool kFinish (see row_fwd_kernel)
+template <typename T, int LR, bool PAD, class Load, class Store>
+__global__ void __launch_bounds__(row_rb<T>(LR) * (LR / rpt_for(LR)), 1)
+row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
+               const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
+    if (gate && *gate) return;
+    constexpr int RPT = rpt_for(LR);
+    constexpr int TT = LR / RPT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    const int r = threadIdx.x / TT, t = threadIdx.x % TT;
+    const int row = blockIdx.x * row_rb<T>(LR) + r;
+    const bool valid = row < nrows;
+    const int off = r * sm_len(LR + 1);
+    for (int k = t; k <= LR; k += TT)
+        sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
+    __syncthreads();
+    cplx<T> v[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        const int k = t + m * TT;
+        const cplx<T> xk = sm[smaddr(k, 1, off)];
+        const cplx<T> xn = sm[smaddr(LR - k, 1, off)];
+        const cplx<T> A = mk<T>(xk.x + xn.x, xk.y - xn.y);
+        const cplx<T> B = mk<T>(xk.x - xn.x, xk.y + xn.y);
+        const cplx<T> Bw = cmulc(B, __ldg(&tw_2lr[k]));  // B * exp(+2 pi i k / 2LR)
+        v[m] = mk<T>(A.x - Bw.y, A.y + Bw.x);             // A + i Bw
+    }
+    __syncthreads();
+    block_fft<T, LR, RPT, +1, 1>(v, t, sm, off, tw_lr);
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        if (PAD && m >= RPT / 2) continue;
+        if (valid) st(row, t + m * TT, v[m]);
+    }
+    if constexpr (Store::kFinish) {
+        __syncthreads();
+        st.finish(reinterpret_cast<double*>(smraw));
+    }
+}
+
+// ---- column forward * multiplier * inverse --------------------------------------
+// Mult: cplx<T> operator()(cplx<T> X, int kx, int ky)
+template <typename T, int LC, int CT, bool PAD, class Mult>
+__global__ void __launch_bounds__(CT * (LC / rpt_for(LC)), 1)
+col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
+           const cplx<T>* __restrict__ tw_lc, const int* __restrict__ gate) {
+    if (gate && *gate) return;
+    constexpr int RPT = rpt_for(LC);
+    constexpr int TT = LC / RPT;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    const int c = threadIdx.x % CT, t = threadIdx.x / CT;
+    const int tile = blockIdx.x;
+    cplx<T>* base = spec + (size_t)tile * nrows * CT;
+    cplx<T> v[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+        else v[m] = base[(size_t)(t + m * TT) * CT + c];
+    }
+    block_fft<T, LC, RPT, -1, CT>(v, t, sm, c, tw_lc);
+    const int kx = tile * CT + c;
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, t + m * TT);
+    block_fft<T, LC, RPT, +1, CT>(v, t, sm, c, tw_lc);
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        if (PAD && m >= RPT / 2) continue;
+        base[(size_t)(t + m * TT) * CT + c] = v[m];
+    }
+}
+
+}  // namespace asb

@@ -1,0 +1,90 @@
+// Internal (non-ABI) declarations shared by the translation units of
+// libaspher_b200.so: the operator objects, the twiddle tables and the error
+// plumbing behind aspher_last_error().
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+
+namespace asb {
+
+// Exceptions never cross the C ABI: every entry point catches and converts.
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define ASB_CUDA(call)                                                           \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess)                                                   \
+            throw ::asb::Error(-2, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+void set_last_error(const std::string& m);
+
+// exp(-2 pi i k / L), k < L, for every power of two L <= kMaxTw, on the
+// current device; tw_f(L)/tw_d(L) return the length-L table.
+constexpr int kMaxTw = 32768;
+const void* tw_table(bool dbl, int L);
+template <typename T> inline const typename std::conditional<sizeof(T) == 4, float2, double2>::type*
+tw(int L) {
+    return static_cast<const typename std::conditional<sizeof(T) == 4, float2, double2>::type*>(
+        tw_table(sizeof(T) == 8, L));
+}
+
+enum OpKind : int { OP_FFT = 0, OP_PERIODIC = 1 };
+
+bool is_pow2(long v);
+
+// Opt into >48 KB dynamic shared memory once per kernel per device.
+void smem_optin(const void* func, int bytes);
+
+struct Operator {
+    int kind = OP_FFT;
+    int Ns = 0;
+    double L = 1.0, E_star = 1.0;
+    int device = 0;
+    // free space: tiled real half spectrum Kh (1/M^2 folded in), rows
+    // ky in [0, Ns] only (Kh is even in ky), tile widths per precision
+    double* kh_d = nullptr;
+    float* kh_f = nullptr;
+    int ct_d = 1, ct_f = 1;
+    double max_im_ratio = 0.0;
+    // periodic: symbol scale L / (pi E* Ns^2)
+    double scale = 0.0;
+    // scratch half spectra per precision (lazily sized)
+    void* spec_d = nullptr;
+    void* spec_f = nullptr;
+    size_t spec_d_bytes = 0, spec_f_bytes = 0;
+    // Love table (free space only), kept for tests/diagnostics
+    double* table = nullptr;
+
+    Operator(int kind, int Ns, double L, double E_star);
+    ~Operator();
+    Operator(const Operator&) = delete;
+    Operator& operator=(const Operator&) = delete;
+
+    // u = S x on `stream`; x, y device arrays of Ns*Ns values of the dtype.
+    // gate: optional device int; when nonzero at kernel start, kernels return.
+    void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr);
+    void* spectrum(bool dbl, cudaStream_t s);
+    size_t spectrum_bytes(bool dbl) const;
+    size_t resident_bytes() const;
+};
+
+// Full-grid |k| preconditioner (FourierPreconditioner) on the Ns periodic grid.
+// g is centred by gmean (device scalar, already in T), masked by contact,
+// transformed, multiplied by |k|/Ns^2 and gathered on contact into z.
+// The contact sum of z (double) goes to *zsum_out via per-block partials and
+// a last-block reduction (deterministic); counter must be zero on entry.
+void fourier_precond_apply(Operator& op_shape_src, bool dbl, const void* g,
+                           const uint8_t* contact, const double* gmean,
+                           void* z, double* zsum_out, double* partials,
+                           unsigned* counter, cudaStream_t s, const int* gate);
+
+}  // namespace asb

@@ -1,0 +1,1090 @@
+// Polonsky-Keer projected CG with certified termination on the device.
+//
+// Reference: solve_contact_impl<Real> (src/contact_solver.cpp:150-587),
+// project_load_simplex (:31-60), identification step (:314-364),
+// evaluate()/refine_contact_mean (:69-99, :260-303).  Real = T in {float,
+// double}; every reduction is accumulated in FP64 as in the reference.
+//
+// One CG iteration is the kernel sequence
+//   [apply p->u] eval1 eval2 [precond] dots tupd [apply t->r] rsum den pupd rescale
+// where each pass is one HBM sweep and each reduction's scalar logic runs in
+// the last block of its pass (see pk_state.hpp).  The host enqueues several
+// iterations between synchronisations; once a pass sets `halt`, the rest are
+// no-ops.
+#include "../../include/aspher_b200.h"
+#include "ops.hpp"
+#include "pk_state.hpp"
+#include "pcg.hpp"
+#include "reduce.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <mutex>
+#include <vector>
+
+namespace asb {
+
+// ---- vector helpers ------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void ld4(const T* __restrict__ p, long i4, T (&a)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p) + i4);
+        a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+    } else {
+        const double2 v0 = __ldg(reinterpret_cast<const double2*>(p) + 2 * i4);
+        const double2 v1 = __ldg(reinterpret_cast<const double2*>(p) + 2 * i4 + 1);
+        a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y;
+    }
+}
+// load through L2 without the read-only path (for arrays written earlier in
+// the same kernel sequence by other kernels it does not matter; kept plain)
+template <typename T>
+__device__ __forceinline__ void ldp4(const T* p, long i4, T (&a)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        const float4 v = reinterpret_cast<const float4*>(p)[i4];
+        a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+    } else {
+        const double2 v0 = reinterpret_cast<const double2*>(p)[2 * i4];
+        const double2 v1 = reinterpret_cast<const double2*>(p)[2 * i4 + 1];
+        a[0] = v0.x; a[1] = v0.y; a[2] = v1.x; a[3] = v1.y;
+    }
+}
+template <typename T>
+__device__ __forceinline__ void st4(T* p, long i4, const T (&a)[4]) {
+    if constexpr (sizeof(T) == 4) {
+        reinterpret_cast<float4*>(p)[i4] = make_float4(a[0], a[1], a[2], a[3]);
+    } else {
+        reinterpret_cast<double2*>(p)[2 * i4] = make_double2(a[0], a[1]);
+        reinterpret_cast<double2*>(p)[2 * i4 + 1] = make_double2(a[2], a[3]);
+    }
+}
+__device__ __forceinline__ void ldm4(const uint8_t* m, long i4, uint8_t (&a)[4]) {
+    const uchar4 v = reinterpret_cast<const uchar4*>(m)[i4];
+    a[0] = v.x; a[1] = v.y; a[2] = v.z; a[3] = v.w;
+}
+__device__ __forceinline__ void stm4(uint8_t* m, long i4, const uint8_t (&a)[4]) {
+    reinterpret_cast<uchar4*>(m)[i4] = make_uchar4(a[0], a[1], a[2], a[3]);
+}
+
+#define GRID_LOOP4(N) \
+    for (long i4 = blockIdx.x * (long)blockDim.x + threadIdx.x; i4 < (N) / 4; i4 += (long)gridDim.x * blockDim.x)
+
+__device__ __forceinline__ void set_halt(PkState* st, int h) {
+    st->halt = h;
+    st->skip_mv1 = 1;
+}
+
+// ---- evaluate() -----------------------------------------------------------------
+// pass 1: v = u + (g0 - gshift) -> g; sum of v over p>0, count, min v.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_eval1(PkParams P, PkState* st, const T* u,
+                                                       const T* g0, const T* p, T* g,
+                                                       double* part, int final_mode) {
+    if (!final_mode && st->halt) return;
+    const T gs = (T)P.gshift;
+    double acc[3] = {0.0, 0.0, (double)INFINITY};
+    GRID_LOOP4(P.N) {
+        T uu[4], gg0[4], pp[4], vv[4];
+        ldp4(u, i4, uu);
+        ldp4(g0, i4, gg0);
+        ldp4(p, i4, pp);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const T v = uu[j] + (gg0[j] - gs);
+            vv[j] = v;
+            const double vd = (double)v;
+            acc[2] = fmin(acc[2], vd);
+            if (pp[j] > T(0)) { acc[0] += vd; acc[1] += 1.0; }
+        }
+        st4(g, i4, vv);
+    }
+    const int kinds[3] = {0, 0, 1};
+    if (grid_reduce_last<3>(acc, kinds, part, &st->counter[0]) && threadIdx.x == 0) {
+        if (!final_mode) {
+            if (!st->u_fresh) st->mv++;
+            st->u_fresh = 0;
+            st->skip_mv1 = 0;
+        }
+        const int nc = (int)acc[1];
+        st->nc = nc;
+        st->gsum = acc[0];
+        st->vmin = acc[2];
+        st->alpha = nc ? acc[0] / nc : acc[2];
+        st->gmin = acc[2] - st->alpha;
+    }
+}
+
+// pass 2: centre g, certificate sums, contact mask; last block runs the
+// convergence test and the best/stall bookkeeping (contact_solver.cpp:379-412).
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_eval2(PkParams P, PkState* st, const T* p, T* g,
+                                                       uint8_t* mask, double* part, double* hist,
+                                                       int final_mode) {
+    if (!final_mode && st->halt) return;
+    const T aT = (T)st->alpha, gmT = (T)st->gmin;
+    double acc[5] = {0, 0, 0, 0, 0};  // pv, gcs, e, Gc, psum
+    GRID_LOOP4(P.N) {
+        T pp[4], gv[4];
+        uint8_t mm[4];
+        ldp4(p, i4, pp);
+        ldp4(g, i4, gv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double pd = (double)pp[j];
+            acc[0] += pd * (double)gv[j];
+            const T gi = gv[j] - aT;
+            gv[j] = gi;
+            const double gid = (double)gi;
+            if (pd > 0.0) acc[1] += gid;
+            acc[2] += pd * fabs(gid);
+            acc[3] += pd * (double)(gi - gmT);
+            acc[4] += pd;
+            mm[j] = pp[j] > T(0) ? 1 : 0;
+        }
+        st4(g, i4, gv);
+        stm4(mask, i4, mm);
+    }
+    const int kinds[5] = {0, 0, 0, 0, 0};
+    if (grid_reduce_last<5>(acc, kinds, part, &st->counter[1]) && threadIdx.x == 0) {
+        const int nc = st->nc;
+        double alpha = st->alpha, gmin = st->gmin;
+        if (nc > 0) {  // refine_contact_mean (contact_solver.cpp:94-99)
+            const double d = acc[1] / nc;
+            alpha += d;
+            gmin -= d;
+        }
+        const double PG = P.P_total * P.g_ref;
+        st->alpha_ref = alpha;
+        st->gmin_ref = gmin;
+        st->pv = acc[0];
+        st->gcs = acc[1];
+        st->pk = acc[2] / PG;
+        st->G = acc[3];
+        st->fw = acc[3] / PG;
+        st->pen = fmax(0.0, -gmin) / P.g_ref;
+        st->psum = acc[4];
+        st->load = fabs(acc[4] - P.P_total) / P.P_total;
+        st->finite = isfinite(st->gsum) && isfinite(st->vmin) && isfinite(acc[4]) &&
+                     isfinite(acc[2]) && isfinite(acc[3]);
+        if (final_mode) return;
+        if (!st->finite) {
+            st->status = ST_NONFINITE;
+            set_halt(st, H_FINAL);
+            return;
+        }
+        if (P.record_history && hist) hist[st->it] = st->pk;
+        if (st->load <= P.load_tol && st->fw <= P.tol && st->pen <= P.tol) {
+            st->status = ST_CONVERGED;
+            st->u_fresh = 1;
+            set_halt(st, H_FINAL);
+            return;
+        }
+        const double merit = fmax(st->fw, st->pen);
+        if (P.keep_best && merit < st->best_merit) {
+            st->best_merit = merit;
+            st->copy_best = 1;
+        }
+        if (merit < st->seen_merit * (1.0 - 1e-4)) {
+            st->seen_merit = merit;
+            st->stall = 0;
+        } else if (++st->stall >= P.stall_limit) {
+            set_halt(st, H_STALL);
+            return;
+        }
+        if (nc < 2) set_halt(st, H_IDENT);
+    }
+}
+
+// ---- stencil preconditioner (stencil_precond.cpp:63-109) ---------------------
+// z = T(sum_t w_t gc(i + d_t)) on contact, gc = contact ? g - gmean : 0 with
+// periodic wrap; the contact mean of z is removed downstream (dots/tupd read
+// z - zmean).  2-D tile of 64 x 16 outputs with an R-cell halo in shared memory.
+constexpr int kStX = 64, kStY = 16, kMaxR = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_stencil(PkParams P, PkState* st, StencilTaps taps,
+                                                 const T* g, const uint8_t* mask, T* z,
+                                                 double* part, int gated) {
+    if (gated && st->halt) return;
+    __shared__ double tile[(kStY + 2 * kMaxR) * (kStX + 2 * kMaxR)];
+    const int Ns = P.Ns, R = taps.R;
+    const int TW = kStX + 2 * R, TH = kStY + 2 * R;
+    const double gmean = st->nc ? st->gcs / st->nc : 0.0;
+    const int ntx = (Ns + kStX - 1) / kStX, nty = (Ns + kStY - 1) / kStY;
+    double acc[1] = {0.0};
+    for (int tid = blockIdx.x; tid < ntx * nty; tid += gridDim.x) {
+        const int tx0 = (tid % ntx) * kStX, ty0 = (tid / ntx) * kStY;
+        for (int idx = threadIdx.x; idx < TW * TH; idx += blockDim.x) {
+            const int ly = idx / TW, lx = idx % TW;
+            int gy = ty0 + ly - R, gx = tx0 + lx - R;
+            gy = gy < 0 ? gy + Ns : (gy >= Ns ? gy - Ns : gy);
+            gx = gx < 0 ? gx + Ns : (gx >= Ns ? gx - Ns : gx);
+            const size_t j = (size_t)gy * Ns + gx;
+            tile[ly * TW + lx] = mask[j] ? (double)g[j] - gmean : 0.0;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < kStX * kStY; o += blockDim.x) {
+            const int ly = o / kStX, lx = o % kStX;
+            const int gy = ty0 + ly, gx = tx0 + lx;
+            if (gy >= Ns || gx >= Ns) continue;
+            const size_t i = (size_t)gy * Ns + gx;
+            if (!mask[i]) { z[i] = T(0); continue; }
+            double a = 0.0;
+            for (int t = 0; t < taps.n; ++t)
+                a += taps.w[t] * tile[(ly + R + taps.dy[t]) * TW + (lx + R + taps.dx[t])];
+            z[i] = (T)a;
+            acc[0] += a;
+        }
+        __syncthreads();
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
+        st->zmean = st->nc ? (double)(T)(acc[0] / st->nc) : 0.0;
+        st->pc++;
+    }
+}
+
+inline int stencil_grid(int Ns) {
+    const int n = ((Ns + kStX - 1) / kStX) * ((Ns + kStY - 1) / kStY);
+    return n < kMaxBlocks ? n : kMaxBlocks;
+}
+
+// ---- CG passes (contact_solver.cpp:420-501) ------------------------------------
+template <typename T>
+__device__ __forceinline__ T zfinal(const PkParams& P, T z, T g, T zm) {
+    return P.precond ? (T)(z - zm) : g;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_dots(PkParams P, PkState* st, const T* z,
+                                                      const T* g, const T* gprev,
+                                                      const uint8_t* mask, double* part) {
+    if (st->halt) return;
+    const T zm = (T)st->zmean;
+    double acc[3] = {0, 0, 0};  // G, G_pr, gg
+    GRID_LOOP4(P.N) {
+        T zz[4], gv[4], gp[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(g, i4, gv);
+        ldp4(gprev, i4, gp);
+        if (P.precond) ldp4(z, i4, zz);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!mm[j]) continue;
+            const T zf = zfinal(P, zz[j], gv[j], zm);
+            const double gd = (double)gv[j];
+            acc[0] += (double)zf * gd;
+            acc[1] += (double)zf * (double)(gv[j] - gp[j]);
+            acc[2] += gd * gd;
+        }
+    }
+    const int kinds[3] = {0, 0, 0};
+    if (grid_reduce_last<3>(acc, kinds, part, &st->counter[3]) && threadIdx.x == 0) {
+        const double G_old = st->G_old;
+        const double bv = (G_old != 0.0) ? (P.use_pr ? fmax(0.0, acc[1] / G_old) : acc[0] / G_old)
+                                         : 0.0;
+        st->beta = (double)((T)st->delta * (T)bv);
+        st->G_old = acc[0];
+        st->gg = acc[2];
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_tupd(PkParams P, PkState* st, const T* z,
+                                                      const T* g, T* gprev, T* t,
+                                                      const uint8_t* mask, const T* p, T* best) {
+    if (st->halt) return;
+    const T zm = (T)st->zmean, beta = (T)st->beta;
+    const int cb = st->copy_best;
+    GRID_LOOP4(P.N) {
+        T zz[4], gv[4], tt[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(g, i4, gv);
+        ldp4(t, i4, tt);
+        if (P.precond) ldp4(z, i4, zz);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            tt[j] = mm[j] ? (T)(zfinal(P, zz[j], gv[j], zm) + beta * tt[j]) : T(0);
+        st4(t, i4, tt);
+        st4(gprev, i4, gv);
+        if (cb) {
+            T pp[4];
+            ldp4(p, i4, pp);
+            st4(best, i4, pp);
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_rsum(PkParams P, PkState* st, const T* r,
+                                                      const T* g, const T* t,
+                                                      const uint8_t* mask, double* part) {
+    if (st->halt) return;
+    double acc[2] = {0, 0};
+    GRID_LOOP4(P.N) {
+        T rr[4], gv[4], tt[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(r, i4, rr);
+        ldp4(g, i4, gv);
+        ldp4(t, i4, tt);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!mm[j]) continue;
+            acc[0] += (double)rr[j];
+            acc[1] += (double)gv[j] * (double)tt[j];
+        }
+    }
+    const int kinds[2] = {0, 0};
+    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[4]) && threadIdx.x == 0) {
+        st->mv++;
+        if (st->copy_best) {
+            st->copy_best = 0;
+            st->have_best = 1;
+        }
+        st->rsum = acc[0];
+        st->num = acc[1];
+        st->rmean = (double)(T)(st->nc ? acc[0] / st->nc : 0.0);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_den(PkParams P, PkState* st, const T* r,
+                                                     const T* t, const uint8_t* mask,
+                                                     double* part) {
+    if (st->halt) return;
+    const T rm = (T)st->rmean;
+    double acc[1] = {0};
+    GRID_LOOP4(P.N) {
+        T rr[4], tt[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(r, i4, rr);
+        ldp4(t, i4, tt);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (mm[j]) acc[0] += (double)(T)(rr[j] - rm) * (double)tt[j];
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[5]) && threadIdx.x == 0) {
+        const double den = acc[0], num = st->num;
+        st->den = den;
+        if (den > 0.0 && isfinite(den) && isfinite(num)) {
+            const T tau = (T)(num / den);
+            st->tau = (double)tau;
+            st->tau_ov = st->gg > 0.0 ? (double)(T)(num * num / (den * st->gg)) : (double)tau;
+        } else {
+            set_halt(st, H_IDENT);  // no usable direction: identification step
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_pupd(PkParams P, PkState* st, T* p, const T* t,
+                                                      const T* g, double* part) {
+    if (st->halt) return;
+    const T tau = (T)st->tau, tov = (T)st->tau_ov;
+    double acc[2] = {0, 0};  // changed (max), total
+    GRID_LOOP4(P.N) {
+        T pp[4], tt[4], gv[4];
+        ldp4(p, i4, pp);
+        ldp4(t, i4, tt);
+        ldp4(g, i4, gv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            T pi = pp[j];
+            const bool was = pi > T(0);
+            if (was) {
+                const T q = pi - tau * tt[j];
+                pi = q < T(0) ? T(0) : q;
+            }
+            if (pi == T(0) && gv[j] < T(0)) pi -= tov * gv[j];
+            if ((pi > T(0)) != was) acc[0] = 1.0;
+            pp[j] = pi;
+            acc[1] += (double)pi;
+        }
+        st4(p, i4, pp);
+    }
+    const int kinds[2] = {2, 0};
+    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[6]) && threadIdx.x == 0) {
+        st->delta = acc[0] > 0.0 ? 0.0 : 1.0;
+        st->total = acc[1];
+        if (acc[1] > 0.0) {
+            st->scale = (double)(T)(P.P_total / acc[1]);
+            st->fill = 0;
+        } else {
+            st->fill = 1;
+        }
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_rescale(PkParams P, PkState* st, T* p,
+                                                         double* part) {
+    if (st->halt) return;
+    const int fill = st->fill;
+    const T f = (T)st->scale, pb = (T)P.p_bar;
+    GRID_LOOP4(P.N) {
+        T pp[4];
+        ldp4(p, i4, pp);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pp[j] = fill ? pb : pp[j] * f;
+        st4(p, i4, pp);
+    }
+    double acc[1] = {0};
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[7]) && threadIdx.x == 0) {
+        st->it++;
+        if (st->it >= P.max_iter) set_halt(st, H_FINAL);  // status stays max_iterations
+    }
+}
+
+// ---- host-driven helpers (identification step, validation, outputs) -----------
+// generic reduction: mode 0: [min g0, max g0, nonfinite count]
+//                    1: [sum x]
+//                    2: f_cur = sum p(0.5u + g0s), pp = sum p^2, pu = sum p u
+//                    3: f_try = sum z(0.5r + g0s), gd = sum g (z - p)
+//                    4: count/sum of x > theta
+//                    5: objective = sum p(0.5u + g0s)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_reduce(PkParams P, PkState* st, int mode,
+                                                        const T* a, const T* b, const T* c,
+                                                        const T* d, double theta,
+                                                        double* part) {
+    const T gs = (T)P.gshift;
+    double acc[3] = {0, 0, 0};
+    if (mode == 0) { acc[0] = (double)INFINITY; acc[1] = -(double)INFINITY; }
+    GRID_LOOP4(P.N) {
+        T A[4], B[4], C[4], D[4];
+        ldp4(a, i4, A);
+        if (b) ldp4(b, i4, B);
+        if (c) ldp4(c, i4, C);
+        if (d) ldp4(d, i4, D);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const double x = (double)A[j];
+            switch (mode) {
+                case 0:
+                    acc[0] = fmin(acc[0], x);
+                    acc[1] = fmax(acc[1], x);
+                    if (!isfinite(x)) acc[2] += 1.0;
+                    break;
+                case 1: acc[0] += x; break;
+                case 2:  // a=p b=u c=g0
+                case 5:
+                    acc[0] += x * (0.5 * (double)B[j] + (double)(T)(C[j] - gs));
+                    acc[1] += x * x;
+                    acc[2] += x * (double)B[j];
+                    break;
+                case 3:  // a=z b=r c=g0 d=g ; p in `d`? see host: d=g, p via theta-less extra
+                    acc[0] += x * (0.5 * (double)B[j] + (double)(T)(C[j] - gs));
+                    break;
+                case 4:
+                    if (x > theta) { acc[0] += x; acc[1] += 1.0; }
+                    break;
+            }
+        }
+    }
+    int kinds[3] = {0, 0, 0};
+    if (mode == 0) { kinds[0] = 1; kinds[1] = 2; }
+    if (grid_reduce_last<3>(acc, kinds, part, &st->counter[8]) && threadIdx.x == 0) {
+        st->red[0] = acc[0];
+        st->red[1] = acc[1];
+        st->red[2] = acc[2];
+    }
+}
+
+// gd = sum double(g) * double(z - p)  (contact_solver.cpp:345-346)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_gd(PkParams P, PkState* st, const T* g,
+                                                    const T* z, const T* p, double* part) {
+    double acc[1] = {0};
+    GRID_LOOP4(P.N) {
+        T G[4], Z[4], Pp[4];
+        ldp4(g, i4, G);
+        ldp4(z, i4, Z);
+        ldp4(p, i4, Pp);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[0] += (double)G[j] * (double)(T)(Z[j] - Pp[j]);
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[9]) && threadIdx.x == 0)
+        st->red[3] = acc[0];
+}
+
+template <typename T>
+__global__ void k_axpy_trial(long N, T* z, const T* p, const T* g, T s) {
+    GRID_LOOP4(N) {
+        T Pp[4], G[4], Z[4];
+        ldp4(p, i4, Pp);
+        ldp4(g, i4, G);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) Z[j] = Pp[j] - s * G[j];
+        st4(z, i4, Z);
+    }
+}
+
+template <typename T>
+__global__ void k_threshold(long N, T* z, T th) {
+    GRID_LOOP4(N) {
+        T Z[4];
+        ldp4(z, i4, Z);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) Z[j] = Z[j] > th ? (T)(Z[j] - th) : T(0);
+        st4(z, i4, Z);
+    }
+}
+
+template <typename T>
+__global__ void k_fill(long N, T* x, T v) {
+    GRID_LOOP4(N) {
+        T X[4] = {v, v, v, v};
+        st4(x, i4, X);
+    }
+}
+
+template <typename T>
+__global__ void k_clamp_pos(long N, T* x, const T* src) {
+    GRID_LOOP4(N) {
+        T X[4];
+        ldp4(src, i4, X);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) X[j] = X[j] < T(0) ? T(0) : X[j];  // cwiseMax(0)
+        st4(x, i4, X);
+    }
+}
+
+template <typename T>
+__global__ void k_scale(long N, T* x, T f) {
+    GRID_LOOP4(N) {
+        T X[4];
+        ldp4(x, i4, X);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) X[j] = X[j] * f;
+        st4(x, i4, X);
+    }
+}
+
+template <typename T>
+__global__ void k_to_f64(long N, double* out, const T* x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        out[i] = (double)x[i];
+}
+
+// z[C] -= T(zmean) (the standalone preconditioner entry point)
+template <typename T>
+__global__ void k_sub_zmean(long N, T* z, const uint8_t* mask, const PkState* st) {
+    const T zm = (T)st->zmean;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        if (mask[i]) z[i] = z[i] - zm;
+}
+
+// contact sum / count of g for the standalone preconditioner
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, const T* g,
+                                                       const uint8_t* mask, double* part) {
+    double acc[2] = {0, 0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        if (mask[i]) { acc[0] += (double)g[i]; acc[1] += 1.0; }
+    const int kinds[2] = {0, 0};
+    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[10]) && threadIdx.x == 0) {
+        st->gcs = acc[0];
+        st->nc = (int)acc[1];
+    }
+}
+
+// ---- host driver -----------------------------------------------------------------
+namespace {
+
+int red_grid(long N) {
+    long g = (N / 4 + kRedThreads - 1) / kRedThreads;
+    if (g > kMaxBlocks / 2) g = kMaxBlocks / 2;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+template <typename T>
+struct Workspace {
+    long N = 0;
+    T *p = nullptr, *t = nullptr, *u = nullptr, *g = nullptr, *gprev = nullptr, *z = nullptr,
+      *r = nullptr, *best = nullptr;
+    uint8_t* mask = nullptr;
+    double* part = nullptr;
+    double* hist = nullptr;
+    PkState* st = nullptr;
+    cudaStream_t s = nullptr;
+    void alloc(long n, bool keep_best, int hist_len, cudaStream_t stream) {
+        N = n;
+        s = stream;
+        const size_t b = (size_t)n * sizeof(T);
+        T** vecs[] = {&p, &t, &u, &g, &gprev, &z, &r};
+        for (T** v : vecs) ASB_CUDA(cudaMallocAsync((void**)v, b, s));
+        if (keep_best) ASB_CUDA(cudaMallocAsync((void**)&best, b, s));
+        ASB_CUDA(cudaMallocAsync((void**)&mask, (size_t)n, s));
+        ASB_CUDA(cudaMallocAsync((void**)&part, kMaxBlocks * 8 * sizeof(double), s));
+        ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
+        if (hist_len > 0) ASB_CUDA(cudaMallocAsync((void**)&hist, hist_len * sizeof(double), s));
+        ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));
+    }
+    ~Workspace() {
+        void* all[] = {p, t, u, g, gprev, z, r, best, mask, part, hist, st};
+        for (void* v : all)
+            if (v) cudaFreeAsync(v, s);
+    }
+};
+
+template <typename T>
+struct Solver {
+    Operator& op;
+    PkParams P{};
+    Workspace<T> w;
+    StencilTaps taps{};
+    cudaStream_t s;
+    int grid;
+    PkState h{};  // host mirror
+
+    Solver(Operator& o, cudaStream_t st) : op(o), s(st) {}
+
+    void read_state() {
+        ASB_CUDA(cudaMemcpyAsync(&h, w.st, sizeof(PkState), cudaMemcpyDeviceToHost, s));
+        ASB_CUDA(cudaStreamSynchronize(s));
+    }
+    void write_state() {
+        ASB_CUDA(cudaMemcpyAsync(w.st, &h, sizeof(PkState), cudaMemcpyHostToDevice, s));
+        ASB_CUDA(cudaStreamSynchronize(s));
+    }
+    // results of the helper reductions live in st->red; only that slice is
+    // read back so the host mirror `h` is never clobbered mid-update
+    void read_red(double (&r)[8]) {
+        ASB_CUDA(cudaMemcpyAsync(r, w.st->red, sizeof(r), cudaMemcpyDeviceToHost, s));
+        ASB_CUDA(cudaStreamSynchronize(s));
+    }
+    double reduce(int mode, const T* a, const T* b, const T* c, const T* d, double theta,
+                  double* out3 = nullptr) {
+        k_reduce<T><<<grid, kRedThreads, 0, s>>>(P, w.st, mode, a, b, c, d, theta, w.part);
+        ASB_CUDA(cudaGetLastError());
+        double r[8];
+        read_red(r);
+        if (out3) { out3[0] = r[0]; out3[1] = r[1]; out3[2] = r[2]; }
+        return r[0];
+    }
+
+    void apply(const T* x, T* y, const int* gate) {
+        op.matvec(sizeof(T) == 8, x, y, s, gate);
+    }
+
+    void precond_apply(const int* gate) {
+        if (P.precond == 1) {
+            k_stencil<T><<<stencil_grid(P.Ns), 256, 0, s>>>(P, w.st, taps, w.g, w.mask, w.z, w.part,
+                                                           gate != nullptr);
+            ASB_CUDA(cudaGetLastError());
+        } else if (P.precond == 2) {
+            fourier_precond_pk<T>(op, w.g, w.mask, w.st, w.z, w.part, s, gate);
+        }
+    }
+
+    // one CG iteration (common path), all gated on the device
+    void enqueue_iteration() {
+        apply(w.p, w.u, &w.st->skip_mv1);
+        k_eval1<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.u, g0, w.p, w.g, w.part, 0);
+        k_eval2<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.g, w.mask, w.part, w.hist, 0);
+        if (P.precond) precond_apply(&w.st->halt);
+        k_dots<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.z, w.g, w.gprev, w.mask, w.part);
+        k_tupd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.z, w.g, w.gprev, w.t, w.mask, w.p,
+                                               w.best);
+        apply(w.t, w.r, &w.st->halt);
+        k_rsum<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.r, w.g, w.t, w.mask, w.part);
+        k_den<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.r, w.t, w.mask, w.part);
+        k_pupd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.t, w.g, w.part);
+        k_rescale<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.part);
+        ASB_CUDA(cudaGetLastError());
+    }
+
+    // project_load_simplex on w.z (contact_solver.cpp:31-60)
+    void project_simplex(double P_total) {
+        const long N = P.N;
+        double ssum = reduce(1, w.z, nullptr, nullptr, nullptr, 0.0);
+        long nact = N;
+        double theta = (ssum - P_total) / (double)nact;
+        for (int pass = 0; pass < 64; ++pass) {
+            double o[3];
+            reduce(4, w.z, nullptr, nullptr, nullptr, theta, o);
+            const long n2 = (long)o[1];
+            if (n2 == 0) break;
+            if (n2 == nact) break;
+            nact = n2;
+            ssum = o[0];
+            theta = (ssum - P_total) / (double)nact;
+        }
+        k_threshold<T><<<grid, kRedThreads, 0, s>>>(N, w.z, (T)theta);
+        ASB_CUDA(cudaGetLastError());
+    }
+
+    // identification step (contact_solver.cpp:314-364); state h is current
+    bool identification_step(double& s_id, int& id_steps) {
+        double o[3];
+        reduce(2, w.p, w.u, g0, nullptr, 0.0, o);
+        const double f_cur = o[0];
+        if (!(s_id > 0.0)) {
+            const double pp = o[1], pu = o[2];
+            s_id = (pu > 0.0 && pp > 0.0) ? pp / pu : 1.0;
+        }
+        for (int trial = 0; trial < 12; ++trial) {
+            k_axpy_trial<T><<<grid, kRedThreads, 0, s>>>(P.N, w.z, w.p, w.g, (T)s_id);
+            project_simplex(P.P_total);
+            apply(w.z, w.r, nullptr);
+            mv_host++;
+            reduce(3, w.z, w.r, g0, nullptr, 0.0, o);
+            const double f_try = o[0];
+            k_gd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.g, w.z, w.p, w.part);
+            double rr[8];
+            read_red(rr);
+            const double gd = rr[3];
+            if (std::isfinite(f_try) && gd < 0.0 && f_try <= f_cur + 1e-4 * gd) {
+                const size_t b = (size_t)P.N * sizeof(T);
+                ASB_CUDA(cudaMemcpyAsync(w.p, w.z, b, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemcpyAsync(w.u, w.r, b, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemsetAsync(w.t, 0, b, s));
+                ASB_CUDA(cudaMemsetAsync(w.gprev, 0, b, s));
+                h.u_fresh = 1;
+                h.delta = 0.0;
+                h.G_old = 1.0;
+                ++id_steps;
+                if (trial == 0) s_id *= 2.0;
+                return true;
+            }
+            s_id *= 0.25;
+        }
+        return false;
+    }
+
+    const T* g0 = nullptr;
+    long long mv_host = 0;
+
+    void run(const aspher_solve_opts& o, const T* g0_, double p_bar, const T* p_init,
+             double* pressure, double* disp, double* gap, double* hist_host, int hist_cap,
+             aspher_result& res) {
+        const auto t_start = std::chrono::steady_clock::now();
+        g0 = g0_;
+        const int Ns = op.Ns;
+        const long N = (long)Ns * Ns;
+        constexpr bool is_double = sizeof(T) == 8;
+        if (!(p_bar > 0.0) || !std::isfinite(p_bar))
+            throw Error(ASPHER_EINVAL, "solve_contact: empty gap or p_bar <= 0");
+        if (!(o.tol > 0.0)) throw Error(ASPHER_EINVAL, "solve_contact: tol must be positive");
+        if (o.max_iter < 0) throw Error(ASPHER_EINVAL, "solve_contact: max_iter must be >= 0");
+        if (o.precond < 0 || o.precond > 2) throw Error(ASPHER_EINVAL, "solve_contact: bad precond");
+        if (o.precond == 1) taps = make_stencil_taps(Ns, o.precond_radius);
+        grid = red_grid(N);
+        const int hist_len = o.record_history ? o.max_iter + 1 : 0;
+        w.alloc(N, o.keep_best != 0, hist_len, s);
+        P.N = N;
+        P.Ns = Ns;
+        // validation before any operator apply (contact_solver.cpp:159-168)
+        double mm[3];
+        reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
+        if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
+        const double P_total = (double)(T)p_bar * (double)N;
+        const double gmin_v = mm[0], gmax_v = mm[1];
+        double g_ref = o.g_ref;
+        if (!(g_ref > 0.0)) g_ref = gmax_v - gmin_v;
+        if (!(g_ref > 0.0)) g_ref = 1.0;
+        const double p_ref = o.p_ref > 0.0 ? o.p_ref : (double)(T)p_bar;
+        const double load_tol = o.load_tol > 0.0 ? o.load_tol : (is_double ? 1e-12 : 5e-7);
+        const double tol = o.tol;
+        const double req_tol = o.requested_tol > 0.0 ? o.requested_tol : tol;
+        double datum = 0.0;
+        bool subtract = false;
+        if (o.datum_mode == ASPHER_DATUM_AUTOMATIC) {
+            datum = gmin_v + 0.5 * (gmax_v - gmin_v);
+            subtract = true;
+        } else if (o.datum_mode == ASPHER_DATUM_SOLVER) {
+            datum = o.datum;
+            subtract = true;
+        } else {
+            datum = o.datum;
+        }
+        P.max_iter = o.max_iter;
+        P.stall_limit = o.stall_limit > 0 ? o.stall_limit : 200;
+        P.keep_best = o.keep_best;
+        P.record_history = o.record_history && hist_len > 0;
+        P.use_pr = o.use_pr;
+        P.precond = o.precond;
+        P.P_total = P_total;
+        P.g_ref = g_ref;
+        P.tol = tol;
+        P.load_tol = load_tol;
+        P.p_bar = (double)(T)p_bar;
+        P.gshift = subtract ? (double)(T)datum : 0.0;
+
+        // initial pressure (contact_solver.cpp:204-223)
+        const T pb = (T)p_bar;
+        if (p_init) {
+            k_clamp_pos<T><<<grid, kRedThreads, 0, s>>>(N, w.p, p_init);
+            const double ssum = reduce(1, w.p, nullptr, nullptr, nullptr, 0.0);
+            if (ssum > 0.0) k_scale<T><<<grid, kRedThreads, 0, s>>>(N, w.p, (T)(P_total / ssum));
+            else k_fill<T><<<grid, kRedThreads, 0, s>>>(N, w.p, pb);
+        } else {
+            k_fill<T><<<grid, kRedThreads, 0, s>>>(N, w.p, pb);
+        }
+        ASB_CUDA(cudaMemsetAsync(w.t, 0, (size_t)N * sizeof(T), s));
+        ASB_CUDA(cudaMemsetAsync(w.gprev, 0, (size_t)N * sizeof(T), s));
+        ASB_CUDA(cudaMemsetAsync(w.z, 0, (size_t)N * sizeof(T), s));
+        std::memset(&h, 0, sizeof(h));
+        h.G_old = 1.0;
+        h.delta = 0.0;
+        h.best_merit = std::numeric_limits<double>::infinity();
+        h.seen_merit = std::numeric_limits<double>::infinity();
+        h.status = ST_MAX_ITERATIONS;
+        h.halt = o.max_iter > 0 ? H_RUN : H_FINAL;
+        h.skip_mv1 = h.halt ? 1 : 0;
+        write_state();
+
+        double s_id = 0.0;
+        int forced_id = 0, id_steps = 0;
+        std::string reason;
+        int batch = 2;
+        while (h.halt == H_RUN) {
+            for (int k = 0; k < batch; ++k) enqueue_iteration();
+            read_state();
+            if (batch < 16) batch *= 2;
+            if (h.halt == H_RUN) continue;
+            if (h.halt == H_FINAL) break;
+            if (h.copy_best) {
+                ASB_CUDA(cudaMemcpyAsync(w.best, w.p, (size_t)N * sizeof(T),
+                                         cudaMemcpyDeviceToDevice, s));
+                h.copy_best = 0;
+                h.have_best = 1;
+            }
+            if (h.halt == H_STALL) {
+                if (forced_id < 3 && identification_step(s_id, id_steps)) {
+                    ++forced_id;
+                    h.stall = 0;
+                } else {
+                    h.status = ST_STAGNATED;
+                    reason = "stall";
+                    h.halt = H_FINAL;
+                    break;
+                }
+            } else if (h.halt == H_IDENT) {
+                if (!identification_step(s_id, id_steps)) {
+                    h.status = ST_NONPOSITIVE_CURVATURE;
+                    h.halt = H_FINAL;
+                    break;
+                }
+            }
+            // resume: the loop body's end increments the iteration counter
+            h.it++;
+            h.mv += mv_host;
+            mv_host = 0;
+            if (h.it >= o.max_iter) {
+                h.halt = H_FINAL;
+                break;
+            }
+            h.halt = H_RUN;
+            h.skip_mv1 = h.u_fresh ? 1 : 0;
+            write_state();
+            batch = 2;
+        }
+        h.mv += mv_host;
+        mv_host = 0;
+        int status = h.status;
+        // ---- final, freshly evaluated diagnostics (contact_solver.cpp:518-586)
+        bool returned_best = false;
+        if (status != ST_CONVERGED && o.keep_best && h.have_best) {
+            const double merit = std::max(h.fw, h.pen);
+            if (!(merit <= h.best_merit)) {
+                ASB_CUDA(cudaMemcpyAsync(w.p, w.best, (size_t)N * sizeof(T),
+                                         cudaMemcpyDeviceToDevice, s));
+                h.u_fresh = 0;
+                returned_best = true;
+            }
+        }
+        if (!h.u_fresh) {
+            apply(w.p, w.u, nullptr);
+            h.mv++;
+        }
+        h.halt = H_FINAL;
+        write_state();
+        k_eval1<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.u, g0, w.p, w.g, w.part, 1);
+        k_eval2<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.g, w.mask, w.part, nullptr, 1);
+        ASB_CUDA(cudaGetLastError());
+        read_state();
+        if (!h.finite && status != ST_NONFINITE) status = ST_NONFINITE;
+        if (status == ST_CONVERGED && !(h.load <= load_tol && h.fw <= tol && h.pen <= tol)) {
+            status = ST_VERIFICATION_FAILED;
+            reason = "final_check";
+        }
+        if (status == ST_CONVERGED && req_tol < tol && !o.allow_tolerance_relaxation) {
+            if (!(h.fw <= req_tol && h.pen <= req_tol)) {
+                status = ST_STAGNATED;
+                reason = "precision_limit";
+            }
+        }
+        double ob[3];
+        reduce(5, w.p, w.u, g0, nullptr, 0.0, ob);
+        k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, pressure, w.p);
+        if (!o.light) {
+            if (disp) k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, disp, w.u);
+            if (gap) k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, gap, w.g);
+        }
+        ASB_CUDA(cudaGetLastError());
+        int hl = 0;
+        if (o.record_history && hist_host && hist_cap > 0 && hist_len > 0) {
+            hl = std::min(h.it, hist_cap);
+            if (hl > 0)
+                ASB_CUDA(cudaMemcpyAsync(hist_host, w.hist, hl * sizeof(double),
+                                         cudaMemcpyDeviceToHost, s));
+        }
+        ASB_CUDA(cudaStreamSynchronize(s));
+
+        std::memset(&res, 0, sizeof(res));
+        res.status = status;
+        std::strncpy(res.status_reason, reason.c_str(), sizeof(res.status_reason) - 1);
+        res.iterations = h.it;
+        res.converged = status == ST_CONVERGED;
+        res.contact_fraction = (double)h.nc / (double)N;
+        res.mean_pressure = h.psum / (double)N;
+        res.approach = h.alpha_ref + datum;
+        res.objective = ob[0] + datum * P_total;
+        res.error = h.pk;
+        res.pk_error = h.pk;
+        res.fw_gap = h.G;
+        res.fw_error = h.fw;
+        res.load_error = h.load;
+        res.pressure_violation = 0.0;
+        res.penetration_error = h.pen;
+        res.requested_tol = req_tol;
+        res.effective_tol = tol;
+        res.p_ref = p_ref;
+        res.g_ref = g_ref;
+        res.matvec_count = h.mv;
+        res.precond_count = h.pc;
+        res.identification_steps = id_steps;
+        res.returned_best = returned_best;
+        res.history_len = hl;
+        const long long rb = sizeof(T);
+        res.mem_cg_state = 7LL * N * rb;
+        res.mem_best_iterate = o.keep_best ? N * rb : 0;
+        res.mem_contact_mask = N;
+        res.mem_output_arrays = (rb == 8 ? 0 : N * 8LL) + (o.light ? 0 : 2LL * N * 8);
+        res.mem_peak = res.mem_cg_state + res.mem_best_iterate + res.mem_contact_mask +
+                       res.mem_output_arrays;
+        res.time_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start)
+                             .count();
+    }
+};
+
+}  // namespace
+
+namespace {
+// w(dx, dy) of the |k| kernel on the Nw^2 grid: the c2r of |k| (DC zeroed) by
+// direct summation over the half spectrum (kx = 0 and Nw/2 counted once).
+long double kgrid_value(int Nw, int dx, int dy) {
+    const int nh = Nw / 2 + 1;
+    long double acc = 0.0L;
+    const long double tp = 2.0L * 3.14159265358979323846264338327950288L / Nw;
+    for (int ky = 0; ky < Nw; ++ky) {
+        const int kof = ky < Nw / 2 ? ky : ky - Nw;
+        for (int kx = 0; kx < nh; ++kx) {
+            if (kx == 0 && ky == 0) continue;
+            const long double mag = std::sqrt((long double)kx * kx + (long double)kof * kof);
+            const long double wt = (kx == 0 || 2 * kx == Nw) ? 1.0L : 2.0L;
+            acc += wt * mag * std::cos(tp * ((long double)kx * dx + (long double)ky * dy));
+        }
+    }
+    return acc;
+}
+std::mutex g_taps_mu;
+std::map<std::pair<int, int>, StencilTaps> g_taps_cache;
+}  // namespace
+
+StencilTaps make_stencil_taps(int Ns, int R) {
+    if (R < 1) throw Error(ASPHER_EINVAL, "stencil radius must be >= 1");
+    if (R > kMaxR) throw Error(ASPHER_EINVAL, "stencil radius must be <= 4");
+    if (2 * R + 1 > Ns) throw Error(ASPHER_EINVAL, "stencil radius too large for the grid");
+    // The kernel shape is taken on min(Ns, 512) (stencil_precond.cpp:199-220).
+    const int Nw = Ns < 512 ? Ns : 512;
+    {
+        std::lock_guard<std::mutex> lk(g_taps_mu);
+        auto it = g_taps_cache.find({Nw, R});
+        if (it != g_taps_cache.end()) return it->second;
+    }
+    StencilTaps t{};
+    t.R = R;
+    t.n = 0;
+    const long double c0 = kgrid_value(Nw, 0, 0);
+    std::map<std::pair<int, int>, double> uniq;  // w depends on (|dx|, |dy|) only
+    for (int dy = -R; dy <= R; ++dy)
+        for (int dx = -R; dx <= R; ++dx) {
+            if (dx * dx + dy * dy > R * R) continue;
+            const std::pair<int, int> key{std::abs(dx), std::abs(dy)};
+            auto u = uniq.find(key);
+            double v;
+            if (dx == 0 && dy == 0) v = 1.0;
+            else if (u != uniq.end()) v = u->second;
+            else v = uniq[key] = (double)(kgrid_value(Nw, key.first, key.second) / c0);
+            t.dx[t.n] = dx;
+            t.dy[t.n] = dy;
+            t.w[t.n] = v;
+            ++t.n;
+        }
+    std::lock_guard<std::mutex> lk(g_taps_mu);
+    g_taps_cache[{Nw, R}] = t;
+    return t;
+}
+
+template <typename T>
+void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
+                const void* p_init, double* pressure, double* disp, double* gap, double* hist,
+                int hist_cap, aspher_result& res, cudaStream_t s) {
+    Solver<T> S(op, s);
+    S.run(o, (const T*)g0, p_bar, (const T*)p_init, pressure, disp, gap, hist, hist_cap, res);
+}
+template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*, double,
+                                const void*, double*, double*, double*, double*, int,
+                                aspher_result&, cudaStream_t);
+template void solve_impl<double>(Operator&, const aspher_solve_opts&, const void*, double,
+                                 const void*, double*, double*, double*, double*, int,
+                                 aspher_result&, cudaStream_t);
+
+// Standalone preconditioner apply: z = M^-1 g on contact, contact-mean removed.
+template <typename T>
+void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
+                        const uint8_t* mask, T* z, cudaStream_t s) {
+    const long N = (long)op.Ns * op.Ns;
+    PkState* st = nullptr;
+    double* part = nullptr;
+    ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
+    ASB_CUDA(cudaMallocAsync((void**)&part, kMaxBlocks * 8 * sizeof(double), s));
+    ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));
+    PkParams P{};
+    P.N = N;
+    P.Ns = op.Ns;
+    P.precond = precond;
+    const int grid = red_grid(N);
+    k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
+    if (precond == 1) {
+        StencilTaps taps = make_stencil_taps(op.Ns, radius);
+        k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(P, st, taps, g, mask, z, part, 0);
+    } else {
+        fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
+    }
+    k_sub_zmean<T><<<grid, kRedThreads, 0, s>>>(N, z, mask, st);
+    ASB_CUDA(cudaGetLastError());
+    cudaFreeAsync(st, s);
+    cudaFreeAsync(part, s);
+    ASB_CUDA(cudaStreamSynchronize(s));
+}
+template void precond_apply_impl<float>(Operator&, int, int, const float*, const uint8_t*, float*,
+                                        cudaStream_t);
+template void precond_apply_impl<double>(Operator&, int, int, const double*, const uint8_t*,
+                                         double*, cudaStream_t);
+
+}  // namespace asb

@@ -1,0 +1,38 @@
+// Internal declarations of the solver translation unit.
+#pragma once
+
+#include "../../include/aspher_b200.h"
+#include "ops.hpp"
+#include "pk_state.hpp"
+
+namespace asb {
+
+// Stencil taps of the l2 disc |d| <= R (R <= 4: at most 49 taps).
+struct StencilTaps {
+    int n;
+    int R;
+    int dx[64];
+    int dy[64];
+    double w[64];
+};
+StencilTaps make_stencil_taps(int Ns, int R);
+
+// Full-grid |k| preconditioner inside a PK solve: centre g on the contact
+// mask by st->gcs / st->nc, transform, multiply by |k|/Ns^2 (FP32 table
+// values, fourier_precond.cpp:12-28), gather on contact into z and leave
+// T(contact mean of z) in st->zmean (st->pc incremented).  Kernels return at
+// entry when gate != nullptr and *gate != 0.  Defined in operators.cu.
+template <typename T>
+void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
+                        double* part, cudaStream_t s, const int* gate);
+
+template <typename T>
+void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
+                const void* p_init, double* pressure, double* disp, double* gap, double* hist,
+                int hist_cap, aspher_result& res, cudaStream_t s);
+
+template <typename T>
+void precond_apply_impl(Operator& op, int precond, int radius, const T* g, const uint8_t* mask,
+                        T* z, cudaStream_t s);
+
+}  // namespace asb

@@ -1,0 +1,194 @@
+/*
+ * aspher_b200 -- C ABI of the B200 (sm_100a) FFT-operator contact solve.
+ *
+ * This is the drop-in boundary for ASPHER's backend="fft" / "periodic"
+ * normal-contact path.  Each entry point names the reference interface it
+ * replaces (paths relative to the reference project).  Conventions:
+ *   - plain pointers and sizes only; every array argument named *_dev is a
+ *     device pointer on the current CUDA device, 16-byte aligned;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *   - every function returns ASPHER_OK (0) or a negative error code and
+ *     leaves a message readable through aspher_last_error() (thread-local);
+ *     no C++ exception crosses this boundary;
+ *   - numerical outcomes of a solve are NOT errors: they are reported in
+ *     aspher_result.status (the reference's SolveStatus taxonomy);
+ *   - handles are not thread-safe: one operator per host thread / stream,
+ *     as for the reference's operators (include/fft_operator.hpp:42-44).
+ */
+#ifndef ASPHER_B200_H
+#define ASPHER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ASPHER_B200_ABI_VERSION 1
+
+/* ---- error codes ------------------------------------------------------- */
+#define ASPHER_OK 0
+#define ASPHER_EINVAL (-1)   /* invalid argument (reference: std::invalid_argument) */
+#define ASPHER_ECUDA (-2)    /* CUDA runtime / launch failure */
+#define ASPHER_EBUILD (-3)   /* operator build check failed (fft_operator.cpp:57-60) */
+#define ASPHER_ETIMEOUT (-4) /* a bounded device wait gave up */
+
+/* ---- enums -------------------------------------------------------------- */
+enum aspher_backend { ASPHER_BACKEND_FFT = 0, ASPHER_BACKEND_PERIODIC = 1 };
+enum aspher_dtype { ASPHER_F32 = 0, ASPHER_F64 = 1 };
+/* precond: reference python/bindings.cpp:193-214 ("fourier" is the stencil) */
+enum aspher_precond {
+    ASPHER_PRECOND_NONE = 0,
+    ASPHER_PRECOND_STENCIL = 1, /* StencilPreconditioner (include/stencil_precond.hpp:50) */
+    ASPHER_PRECOND_FFT = 2      /* FourierPreconditioner (include/fourier_precond.hpp:33) */
+};
+/* SolveStatus, reference include/contact_solver.hpp:13-21 */
+enum aspher_status {
+    ASPHER_CONVERGED = 0,
+    ASPHER_STAGNATED = 1,
+    ASPHER_MAX_ITERATIONS = 2,
+    ASPHER_NONPOSITIVE_CURVATURE = 3,
+    ASPHER_NONFINITE = 4,
+    ASPHER_VERIFICATION_FAILED = 5,
+    ASPHER_RESOURCE_LIMIT = 6
+};
+/* SolveScales::DatumMode, reference include/contact_solver.hpp:138-144 */
+enum aspher_datum_mode { ASPHER_DATUM_AUTOMATIC = 0, ASPHER_DATUM_SOLVER = 1, ASPHER_DATUM_CALLER = 2 };
+
+int aspher_abi_version(void);
+const char* aspher_last_error(void);
+/* to_string(SolveStatus), reference src/contact_solver.cpp:12-23 */
+const char* aspher_status_string(int status);
+
+/* ---- operators ---------------------------------------------------------- */
+typedef struct aspher_op aspher_op;
+
+/* Replaces BoussinesqKernel(Ns, L, E*) + FFTOperator(kernel).build()
+ * (include/boussinesq_kernel.hpp:26, include/fft_operator.hpp:47-52) for
+ * backend FFT and PeriodicFFTOperator(Ns, L, E*)
+ * (include/periodic_fft_operator.hpp:26) for backend PERIODIC.  The Love
+ * table and its FP64 spectrum are built on the device; synchronous.
+ * grid_size must be a power of two in [16, 8192]. */
+int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
+                     aspher_op** out);
+int aspher_op_destroy(aspher_op* op);
+
+/* y = S x over Ns*Ns values of `dtype` (F64: FFTOperator::matvec_into,
+ * include/fft_operator.hpp:57; F32: matvec_single_into, :62; periodic:
+ * include/periodic_fft_operator.hpp:32,35).  x and y may alias.  Async on
+ * `stream`. */
+int aspher_op_matvec(aspher_op* op, int dtype, const void* x_dev, void* y_dev, void* stream);
+
+/* FFTInfo, reference include/fft_operator.hpp:13-25 */
+typedef struct {
+    int backend;
+    int grid_size;
+    int padded_side;
+    int64_t n;
+    int64_t bytes_spectrum;
+    int64_t bytes_scratch;
+    int64_t bytes_total;
+    double max_im_ratio; /* build-time max|Im|/max|Re| of the kernel spectrum */
+} aspher_op_info;
+int aspher_op_get_info(const aspher_op* op, aspher_op_info* info);
+
+/* Copies the Ns*Ns FP64 Love table T[dy*Ns+dx] (BoussinesqKernel::table_,
+ * src/boussinesq_kernel.cpp:97-106) to host memory.  FFT backend only. */
+int aspher_op_love_table(const aspher_op* op, double* host_out);
+
+/* z = M^-1 g on the contact set (contact_dev: Ns*Ns bytes, nonzero = in
+ * contact), centred and mean-zeroed on it: StencilPreconditioner::apply_into
+ * (include/stencil_precond.hpp:64, radius >= 1) or
+ * FourierPreconditioner::apply_into (include/fourier_precond.hpp:46).
+ * Synchronous. */
+int aspher_precond_apply(aspher_op* op, int precond, int radius, int dtype, const void* g_dev,
+                         const uint8_t* contact_dev, void* z_dev, void* stream);
+
+/* Stencil taps (StencilPreconditioner::tap_dx/tap_dy/tap_w,
+ * include/stencil_precond.hpp:57-60) for grid_size and radius; writes at
+ * most `cap` taps and returns their count in *ntaps. */
+int aspher_stencil_taps(int grid_size, int radius, int* dx, int* dy, double* w, int cap,
+                        int* ntaps);
+
+/* ---- solve -------------------------------------------------------------- */
+/* SolveOptions + SolveScales, reference include/contact_solver.hpp:134-191 */
+typedef struct {
+    double tol;
+    double requested_tol;   /* 0 -> tol */
+    int max_iter;
+    int use_pr;             /* Polak-Ribiere+ (1) or Fletcher-Reeves (0) */
+    int light;              /* skip displacement / gap outputs */
+    int record_history;
+    int keep_best;
+    double load_tol;        /* 0 -> 1e-12 (F64) / 5e-7 (F32) */
+    int stall_limit;        /* <= 0 -> 200 */
+    int allow_tolerance_relaxation;
+    int precond;            /* enum aspher_precond */
+    int precond_radius;     /* stencil radius (2 -> 13 taps) */
+    double p_ref;           /* <= 0 -> p_bar */
+    double g_ref;           /* <= 0 -> range(g0) */
+    int datum_mode;         /* enum aspher_datum_mode */
+    double datum;
+    int dtype;              /* working precision Real: ASPHER_F32 / ASPHER_F64 */
+} aspher_solve_opts;
+
+/* Fills the reference defaults (SolveOptions{} and solve_contact(...)'s
+ * arguments: tol 1e-8, max_iter 5000, use_pr, keep_best, F64). */
+void aspher_solve_opts_default(aspher_solve_opts* o);
+
+/* ContactResult, reference include/contact_solver.hpp:25-123 */
+typedef struct {
+    int status;              /* enum aspher_status */
+    char status_reason[32];  /* "", "stall", "precision_limit", "final_check" */
+    int iterations;
+    int converged;
+    double contact_fraction; /* Python `contact_area` */
+    double mean_pressure;
+    double approach;
+    double objective;
+    double error;            /* == pk_error */
+    double pk_error;
+    double fw_gap;
+    double fw_error;
+    double load_error;
+    double pressure_violation;
+    double penetration_error;
+    double requested_tol;
+    double effective_tol;
+    double p_ref;
+    double g_ref;
+    int64_t matvec_count;
+    int64_t precond_count;
+    int identification_steps;
+    int returned_best;
+    int history_len;         /* entries written to history_out */
+    double time_total;       /* seconds, host wall clock around the solve */
+    int64_t mem_cg_state;    /* Memory, contact_solver.hpp:75-81 */
+    int64_t mem_best_iterate;
+    int64_t mem_contact_mask;
+    int64_t mem_output_arrays;
+    int64_t mem_peak;
+} aspher_result;
+
+/* solve_contact_impl<Real> (include/contact_solver.hpp:244-249; reference
+ * src/contact_solver.cpp:150-587) with the operator of `op`, the
+ * preconditioner selected in opts, and Real = opts->dtype:
+ *   g0_dev        : Ns*Ns values of opts->dtype (read only)
+ *   p_init_dev    : NULL or Ns*Ns values of opts->dtype (warm start; read only)
+ *   pressure_dev  : Ns*Ns FP64 output (required)
+ *   displacement_dev, gap_dev : Ns*Ns FP64 outputs or NULL (skipped when light)
+ *   history_host  : NULL or host array of history_cap doubles (per-iteration
+ *                   pk error when opts->record_history)
+ * Invalid input returns ASPHER_EINVAL before any operator apply
+ * (contact_solver.cpp:159-168).  Synchronous with respect to the host. */
+int aspher_solve(aspher_op* op, const aspher_solve_opts* opts, const void* g0_dev, double p_bar,
+                 const void* p_init_dev, double* pressure_dev, double* displacement_dev,
+                 double* gap_dev, double* history_host, int history_cap, aspher_result* res,
+                 void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ASPHER_B200_H */
