@@ -9,9 +9,11 @@ Lower level: Operator (device matvec), solve_device (device tensors in / out).
 """
 
 from ._lib import AspherError, LIB_PATH  # noqa: F401
-from .api import ContactResult, ContactSolver, Operator, solve_device, stencil_taps  # noqa: F401
+from .api import (ContactResult, ContactSolver, Operator, solve_device,  # noqa: F401
+                  solve_device_mixed, stencil_taps)
 from .nested import solve_nested  # noqa: F401
 from .surfaces import self_affine_gap  # noqa: F401
 
-__all__ = ["ContactSolver", "ContactResult", "Operator", "solve_device", "solve_nested",
+__all__ = ["ContactSolver", "ContactResult", "Operator", "solve_device", "solve_device_mixed",
+           "solve_nested",
            "stencil_taps", "self_affine_gap", "AspherError"]

@@ -55,13 +55,34 @@ class Result(C.Structure):
                 ("history_len", C.c_int), ("time_total", C.c_double),
                 ("mem_cg_state", C.c_int64), ("mem_best_iterate", C.c_int64),
                 ("mem_contact_mask", C.c_int64), ("mem_output_arrays", C.c_int64),
-                ("mem_peak", C.c_int64)]
+                ("mem_peak", C.c_int64), ("time_build", C.c_double),
+                ("time_coarse", C.c_double)]
+
+
+class NestedOpts(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int), ("use_pr", C.c_int),
+                ("coarsest", C.c_int), ("q", C.c_int), ("leaf_side", C.c_int),
+                ("precond", C.c_int), ("precond_engine", C.c_int),
+                ("precond_radius", C.c_int), ("precond_occupancy_max", C.c_double),
+                ("coarse_tol", C.c_double), ("single_precision", C.c_int),
+                ("precision", C.c_int), ("float_floor", C.c_double),
+                ("allow_tolerance_relaxation", C.c_int), ("light_result", C.c_int),
+                ("record_error_history", C.c_int), ("active_set", C.c_int)]
+
+
+class Stage(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("precision", C.c_char * 8), ("q", C.c_int),
+                ("requested_tol", C.c_double), ("effective_tol", C.c_double),
+                ("iterations", C.c_int), ("matvec_count", C.c_int64), ("seconds", C.c_double),
+                ("status", C.c_int), ("fw_error", C.c_double),
+                ("penetration_error", C.c_double), ("precond_dropped", C.c_int)]
 
 
 # exported symbol -> (restype, argtypes)
 SIGNATURES = {
     "aspher_abi_version": (C.c_int, []),
     "aspher_last_error": (C.c_char_p, []),
+    "aspher_launch_count": (C.c_int64, []),
     "aspher_status_string": (C.c_char_p, [C.c_int]),
     "aspher_op_create": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double,
                                    C.POINTER(C.c_void_p)]),
@@ -78,6 +99,18 @@ SIGNATURES = {
     "aspher_solve": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_double,
                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                C.c_int, C.POINTER(Result), C.c_void_p]),
+    "aspher_solve_mixed": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_void_p, C.c_double,
+                                     C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.POINTER(Result), C.POINTER(Result),
+                                     C.c_void_p]),
+    "aspher_nested_opts_default": (None, [C.POINTER(NestedOpts)]),
+    "aspher_solve_nested": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                      C.c_double, C.POINTER(NestedOpts), C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.POINTER(Result), C.POINTER(Stage), C.c_int,
+                                      C.POINTER(C.c_int), C.c_void_p]),
+    "aspher_stencil_for_level": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double]),
+    "aspher_operator_cache_clear": (C.c_int, []),
 }
 
 _lib = None

@@ -32,6 +32,20 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
 
 
+def _to_device_f64(a, expected, dev):
+    """numpy array or torch tensor (host, pinned host or device) -> FP64
+    device vector of `expected` entries (host->device copy on the current
+    stream; non-blocking from pinned memory)."""
+    if isinstance(a, torch.Tensor):
+        if a.numel() != expected:
+            raise ValueError("array has %d entries, expected %d" % (a.numel(), expected))
+        t = a.reshape(-1)
+        if t.dtype != torch.float64:
+            t = t.to(torch.float64)
+        return t.to(dev, non_blocking=True)
+    return torch.from_numpy(_as_vector(a, expected)).to(dev)
+
+
 def _as_vector(a, expected, name="array"):
     a = np.ascontiguousarray(np.asarray(a, dtype=np.float64)).reshape(-1)
     if a.size != expected:
@@ -305,23 +319,19 @@ class ContactSolver:
         'float_then_double' (FP32 at tol, then an FP64 polish).
         """
         N = self.Ns * self.Ns
-        g0 = _as_vector(gap, N, "array")
         if precond not in ("none", "", "fourier", "fourier-fft"):
             raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
-        if not np.all(np.isfinite(g0)):
-            raise ValueError("solve_contact: g0 contains non-finite values")
         dev = _dev()
-        g0d = torch.from_numpy(g0).to(dev)
-        p0 = None
-        if p_init is not None:
-            p0 = torch.from_numpy(_as_vector(p_init, N)).to(dev)
+        g0d = _to_device_f64(gap, N, dev)
+        p0 = None if p_init is None else _to_device_f64(p_init, N, dev)
         t0 = time.perf_counter()
         if precision == "double":
             r = solve_device(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
                              torch.float64)
         elif precision in ("float", "float_then_double"):
-            r = _solve_float(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
-                             polish=(precision == "float_then_double"))
+            r, _ = solve_device_mixed(self.op, g0d, p_nominal, tol, None,
+                                      precision == "float_then_double", max_iter, use_pr,
+                                      precond, p0)
         else:
             raise ValueError("precision must be 'double', 'float' or 'float_then_double'")
         r.wall = time.perf_counter() - t0
@@ -340,28 +350,57 @@ class ContactSolver:
         return d
 
 
-def _solve_float(op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0, polish,
-                 float_floor=None):
-    """FP32 stage (datum removed inside the cast, nested_solve.cpp:871-917),
-    optionally followed by an FP64 polish warm-started from it (:931-974)."""
-    gmin, gmax = float(g0d.min()), float(g0d.max())
-    datum = gmin + 0.5 * (gmax - gmin)
-    g_ref = gmax - gmin
-    gf = (g0d - datum).to(torch.float32)
-    tol_f = tol if float_floor is None else max(tol, float_floor)
-    r = solve_device(op, gf, p_nominal, tol_f, max_iter, use_pr, precond,
-                     None if p0 is None else p0.to(torch.float32), torch.float32,
-                     g_ref=g_ref, datum_mode="caller", datum=datum,
-                     requested_tol=tol, allow_tolerance_relaxation=polish)
-    if not polish:
-        return r
-    before = r
-    r = solve_device(op, g0d, p_nominal, tol, max_iter, use_pr, precond,
-                     before.pressure_device, torch.float64, g_ref=g_ref,
-                     datum_mode="solver", datum=datum)
-    r.stage_stats = [dict(name="float", precision="float", iterations=before.iterations,
-                          status=before.status),
-                     dict(name="polish", precision="double", iterations=r.iterations,
-                          status=r.status)]
-    r.float_iterations = before.iterations
-    return r
+def solve_device_mixed(op, g0, p_nominal, tol=1e-6, float_tol=None, polish=True,
+                       max_iter=5000, use_pr=True, precond="fourier", p_init=None,
+                       light=False, keep_best=None, g_ref=0.0, datum_mode="automatic",
+                       datum=0.0, precond_radius=2, pressure_out=None):
+    """FP32 PK solve with FP64 reductions to ``float_tol`` (default: tol),
+    then (polish) an FP64 PK solve warm-started from it that certifies
+    ``tol``: the reference's float_then_double staging on one grid.
+    g0 / p_init: FP64 device tensors.  Returns (final, float_stage)."""
+    N = op.N
+    if g0.numel() != N:
+        raise ValueError("array has %d entries, expected %d" % (g0.numel(), N))
+    if precond not in L.PRECOND:
+        raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
+    dev = g0.device
+    g0 = g0.to(torch.float64).contiguous().reshape(-1)
+    if p_init is not None:
+        p_init = p_init.to(device=dev, dtype=torch.float64).contiguous().reshape(-1)
+        if p_init.numel() != N:
+            raise ValueError("solve_contact: p_init size mismatch")
+    o = L.SolveOpts()
+    L.lib().aspher_solve_opts_default(C.byref(o))
+    o.tol = float(tol)
+    o.max_iter = int(max_iter)
+    o.use_pr = int(bool(use_pr))
+    o.light = int(bool(light))
+    o.keep_best = int(not light) if keep_best is None else int(bool(keep_best))
+    o.precond = L.PRECOND[precond]
+    o.precond_radius = int(precond_radius)
+    o.g_ref = float(g_ref)
+    o.datum_mode = L.DATUM[datum_mode]
+    o.datum = float(datum)
+    p_out = pressure_out if pressure_out is not None else torch.empty(N, dtype=torch.float64,
+                                                                    device=dev)
+    u_out = g_out = None
+    if not light:
+        u_out = torch.empty(N, dtype=torch.float64, device=dev)
+        g_out = torch.empty(N, dtype=torch.float64, device=dev)
+    res, resf = L.Result(), L.Result()
+    ftol = float(tol if float_tol is None else float_tol)
+    L.check(L.lib().aspher_solve_mixed(
+        op.handle, C.byref(o), _ptr(g0), C.c_double(float(p_nominal)), _ptr(p_init),
+        C.c_double(ftol), int(bool(polish)), _ptr(p_out), _ptr(u_out), _ptr(g_out),
+        C.byref(res), C.byref(resf), _stream()))
+    r = ContactResult(res, op.Ns, p_out, u_out, g_out)
+    rf = ContactResult(resf, op.Ns, None)
+    r.stage_stats = [dict(name="float", precision="float", iterations=rf.iterations,
+                          matvec_count=rf.matvec_count, status=rf.status,
+                          fw_error=rf.fw_error, penetration_error=rf.penetration_error)]
+    if polish:
+        r.stage_stats.append(dict(name="polish", precision="double",
+                                  iterations=r.iterations - rf.iterations,
+                                  status=r.status, fw_error=r.fw_error,
+                                  penetration_error=r.penetration_error))
+    return r, rf

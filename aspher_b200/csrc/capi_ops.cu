@@ -38,6 +38,8 @@ int aspher_abi_version(void) { return ASPHER_B200_ABI_VERSION; }
 
 const char* aspher_last_error(void) { return asb::g_last_error.c_str(); }
 
+int64_t aspher_launch_count(void) { return (int64_t)asb::launch_count(); }
+
 int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
                      aspher_op** out) {
     ASB_API_BEGIN

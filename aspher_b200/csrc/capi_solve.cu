@@ -86,6 +86,23 @@ int aspher_solve(aspher_op* op, const aspher_solve_opts* opts, const void* g0_de
     ASB_API_END
 }
 
+int aspher_solve_mixed(aspher_op* op, const aspher_solve_opts* opts, const double* g0_dev,
+                       double p_bar, const double* p_init_dev, double float_tol, int polish,
+                       double* pressure_dev, double* displacement_dev, double* gap_dev,
+                       aspher_result* res, aspher_result* res_float, void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !opts || !g0_dev || !pressure_dev || !res)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_mixed: NULL argument");
+    if (!(float_tol > 0.0)) throw asb::Error(ASPHER_EINVAL, "aspher_solve_mixed: float_tol must be positive");
+    const uintptr_t a = (uintptr_t)g0_dev | (uintptr_t)pressure_dev | (uintptr_t)p_init_dev |
+                        (uintptr_t)displacement_dev | (uintptr_t)gap_dev;
+    if (a % 16) throw asb::Error(ASPHER_EINVAL, "aspher_solve_mixed: buffers must be 16-byte aligned");
+    asb::solve_mixed(*op->impl, *opts, g0_dev, p_bar, p_init_dev, float_tol, polish, pressure_dev,
+                     displacement_dev, gap_dev, *res, res_float, static_cast<cudaStream_t>(stream));
+    return ASPHER_OK;
+    ASB_API_END
+}
+
 int aspher_precond_apply(aspher_op* op, int precond, int radius, int dtype, const void* g_dev,
                          const uint8_t* contact_dev, void* z_dev, void* stream) {
     ASB_API_BEGIN
@@ -102,6 +119,62 @@ int aspher_precond_apply(aspher_op* op, int precond, int radius, int dtype, cons
                                        contact_dev, (float*)z_dev, s);
     else
         throw asb::Error(ASPHER_EINVAL, "aspher_precond_apply: dtype must be F32 or F64");
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+void aspher_nested_opts_default(aspher_nested_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->tol = 1e-8;
+    o->max_iter = 20000;
+    o->use_pr = 1;
+    o->coarsest = 64;
+    o->q = 6;
+    o->leaf_side = 8;
+    o->precond = 1;
+    o->precond_engine = 0;
+    o->precond_radius = 2;
+    o->precond_occupancy_max = 0.4;
+    o->coarse_tol = 1e-4;
+    o->single_precision = 0;
+    o->precision = 0;
+    o->float_floor = 2e-6;
+    o->allow_tolerance_relaxation = 0;
+    o->light_result = 0;
+    o->record_error_history = 0;
+    o->active_set = 0;
+}
+
+int aspher_solve_nested(int backend, int grid_size, double domain_size, double E_star,
+                        const double* g0_dev, double p_bar, const aspher_nested_opts* opts,
+                        double* pressure_dev, double* displacement_dev, double* gap_dev,
+                        double* history_host, int history_cap, aspher_result* res,
+                        aspher_stage* stages, int stage_cap, int* nstages, void* stream) {
+    ASB_API_BEGIN
+    if (!opts || !g0_dev || !pressure_dev || !res)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_nested: NULL argument");
+    if (backend != ASPHER_BACKEND_FFT && backend != ASPHER_BACKEND_PERIODIC)
+        throw asb::Error(ASPHER_EINVAL, "solve_contact_nested: backend must be 'fft' or "
+                                        "'periodic' on this build");
+    const uintptr_t a = (uintptr_t)g0_dev | (uintptr_t)pressure_dev |
+                        (uintptr_t)displacement_dev | (uintptr_t)gap_dev;
+    if (a % 16) throw asb::Error(ASPHER_EINVAL, "aspher_solve_nested: buffers must be 16-byte aligned");
+    asb::solve_nested(backend, grid_size, domain_size, E_star, g0_dev, p_bar, *opts, pressure_dev,
+                      displacement_dev, gap_dev, history_host, history_cap, *res, stages,
+                      stage_cap, nstages, static_cast<cudaStream_t>(stream));
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_stencil_for_level(int engine, int precond, double prev_occupancy,
+                             double occupancy_max) {
+    return asb::stencil_for_level(engine, precond != 0, prev_occupancy, occupancy_max) ? 1 : 0;
+}
+
+int aspher_operator_cache_clear(void) {
+    ASB_API_BEGIN
+    asb::clear_operator_cache();
     return ASPHER_OK;
     ASB_API_END
 }

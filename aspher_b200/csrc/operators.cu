@@ -19,6 +19,7 @@
 #include "pcg.hpp"
 #include "reduce.cuh"
 
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -69,6 +70,12 @@ const void* tw_table(bool dbl, int L) {
 }
 
 bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+namespace {
+std::atomic<long long> g_launches{0};
+}
+void count_launches(long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 void smem_optin(const void* func, int bytes) {
     if (bytes <= 48 * 1024) return;
@@ -258,6 +265,11 @@ struct FreeImpl {
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
                        const int* gate) {
+        if constexpr (col_smem<T>(LC, CT) > 227 * 1024) {
+            throw Error(-1, "free-space FP64 apply at grid_size 8192 is not supported (the "
+                            "16384-point FP64 column does not fit one CTA's shared memory); "
+                            "use FP32 or grid_size <= 4096");
+        } else {
         constexpr int rb = row_rb<T>(LR);
         constexpr int rthreads = rb * (LR / rpt_for(LR));
         constexpr int rsm = row_smem<T>(LR);
@@ -276,7 +288,9 @@ struct FreeImpl {
         smem_optin((const void*)ki, rsm);
         ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT}, StoreRealRows<T>{y, NS}, NS,
                                         tw<T>(LR), tw<T>(2 * LR), gate);
+        count_launches(3);
         ASB_CUDA(cudaGetLastError());
+        }
     }
 };
 
@@ -308,6 +322,7 @@ struct PeriodicImpl {
         smem_optin((const void*)ki, rsm);
         ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT}, StoreRealRows<T>{y, NS}, NS,
                                         tw<T>(LR), tw<T>(2 * LR), gate);
+        count_launches(3);
         ASB_CUDA(cudaGetLastError());
     }
 
@@ -402,6 +417,7 @@ struct FourierImpl {
         ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT},
                                         StoreGather<T>{z, mask, NS, st, part, 0.0}, NS, tw<T>(LR),
                                         tw<T>(2 * LR), gate);
+        count_launches(3);
         ASB_CUDA(cudaGetLastError());
     }
 };
@@ -501,6 +517,8 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
 }
 
 Operator::~Operator() {
+    ctx_f.reset();
+    ctx_d.reset();
     cudaFree(kh_d);
     cudaFree(kh_f);
     cudaFree(spec_d);

@@ -7,6 +7,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <memory>
 #include <stdexcept>
 #include <string>
 
@@ -26,6 +27,16 @@ struct Error : std::runtime_error {
     } while (0)
 
 void set_last_error(const std::string& m);
+
+// Kernel launches issued by this library (aspher_launch_count()).
+void count_launches(long n);
+long long launch_count();
+
+// Cached solver state attached to an operator (see pcg.cu).
+struct SolverCtxBase {
+    virtual ~SolverCtxBase() = default;
+    virtual size_t bytes() const = 0;
+};
 
 // exp(-2 pi i k / L), k < L, for every power of two L <= kMaxTw, on the
 // current device; tw_f(L)/tw_d(L) return the length-L table.
@@ -63,6 +74,8 @@ struct Operator {
     size_t spec_d_bytes = 0, spec_f_bytes = 0;
     // Love table (free space only), kept for tests/diagnostics
     double* table = nullptr;
+    // solver contexts per precision (workspace + loop graph), built lazily
+    std::shared_ptr<SolverCtxBase> ctx_f, ctx_d;
 
     Operator(int kind, int Ns, double L, double E_star);
     ~Operator();

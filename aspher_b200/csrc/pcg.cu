@@ -23,6 +23,7 @@
 #include <cstring>
 #include <limits>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <vector>
 
@@ -81,9 +82,10 @@ __device__ __forceinline__ void set_halt(PkState* st, int h) {
 // ---- evaluate() -----------------------------------------------------------------
 // pass 1: v = u + (g0 - gshift) -> g; sum of v over p>0, count, min v.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_eval1(PkParams P, PkState* st, const T* u,
+__global__ void __launch_bounds__(kRedThreads) k_eval1(const PkParams* __restrict__ Pp, PkState* st, const T* u,
                                                        const T* g0, const T* p, T* g,
                                                        double* part, int final_mode) {
+    const PkParams& P = *Pp;
     if (!final_mode && st->halt) return;
     const T gs = (T)P.gshift;
     double acc[3] = {0.0, 0.0, (double)INFINITY};
@@ -121,9 +123,10 @@ __global__ void __launch_bounds__(kRedThreads) k_eval1(PkParams P, PkState* st, 
 // pass 2: centre g, certificate sums, contact mask; last block runs the
 // convergence test and the best/stall bookkeeping (contact_solver.cpp:379-412).
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_eval2(PkParams P, PkState* st, const T* p, T* g,
+__global__ void __launch_bounds__(kRedThreads) k_eval2(const PkParams* __restrict__ Pp, PkState* st, const T* p, T* g,
                                                        uint8_t* mask, double* part, double* hist,
                                                        int final_mode) {
+    const PkParams& P = *Pp;
     if (!final_mode && st->halt) return;
     const T aT = (T)st->alpha, gmT = (T)st->gmin;
     double acc[5] = {0, 0, 0, 0, 0};  // pv, gcs, e, Gc, psum
@@ -206,9 +209,10 @@ __global__ void __launch_bounds__(kRedThreads) k_eval2(PkParams P, PkState* st, 
 constexpr int kStX = 64, kStY = 16, kMaxR = 4;
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_stencil(PkParams P, PkState* st, StencilTaps taps,
+__global__ void __launch_bounds__(256) k_stencil(const PkParams* __restrict__ Pp, PkState* st, StencilTaps taps,
                                                  const T* g, const uint8_t* mask, T* z,
                                                  double* part, int gated) {
+    const PkParams& P = *Pp;
     if (gated && st->halt) return;
     __shared__ double tile[(kStY + 2 * kMaxR) * (kStX + 2 * kMaxR)];
     const int Ns = P.Ns, R = taps.R;
@@ -260,9 +264,10 @@ __device__ __forceinline__ T zfinal(const PkParams& P, T z, T g, T zm) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_dots(PkParams P, PkState* st, const T* z,
+__global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, const T* gprev,
                                                       const uint8_t* mask, double* part) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     const T zm = (T)st->zmean;
     double acc[3] = {0, 0, 0};  // G, G_pr, gg
@@ -295,9 +300,10 @@ __global__ void __launch_bounds__(kRedThreads) k_dots(PkParams P, PkState* st, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_tupd(PkParams P, PkState* st, const T* z,
+__global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, T* gprev, T* t,
                                                       const uint8_t* mask, const T* p, T* best) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     const T zm = (T)st->zmean, beta = (T)st->beta;
     const int cb = st->copy_best;
@@ -322,9 +328,10 @@ __global__ void __launch_bounds__(kRedThreads) k_tupd(PkParams P, PkState* st, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_rsum(PkParams P, PkState* st, const T* r,
+__global__ void __launch_bounds__(kRedThreads) k_rsum(const PkParams* __restrict__ Pp, PkState* st, const T* r,
                                                       const T* g, const T* t,
                                                       const uint8_t* mask, double* part) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     double acc[2] = {0, 0};
     GRID_LOOP4(P.N) {
@@ -355,9 +362,10 @@ __global__ void __launch_bounds__(kRedThreads) k_rsum(PkParams P, PkState* st, c
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_den(PkParams P, PkState* st, const T* r,
+__global__ void __launch_bounds__(kRedThreads) k_den(const PkParams* __restrict__ Pp, PkState* st, const T* r,
                                                      const T* t, const uint8_t* mask,
                                                      double* part) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     const T rm = (T)st->rmean;
     double acc[1] = {0};
@@ -386,8 +394,9 @@ __global__ void __launch_bounds__(kRedThreads) k_den(PkParams P, PkState* st, co
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_pupd(PkParams P, PkState* st, T* p, const T* t,
+__global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict__ Pp, PkState* st, T* p, const T* t,
                                                       const T* g, double* part) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     const T tau = (T)st->tau, tov = (T)st->tau_ov;
     double acc[2] = {0, 0};  // changed (max), total
@@ -425,8 +434,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pupd(PkParams P, PkState* st, T
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_rescale(PkParams P, PkState* st, T* p,
+__global__ void __launch_bounds__(kRedThreads) k_rescale(const PkParams* __restrict__ Pp, PkState* st, T* p,
                                                          double* part) {
+    const PkParams& P = *Pp;
     if (st->halt) return;
     const int fill = st->fill;
     const T f = (T)st->scale, pb = (T)P.p_bar;
@@ -453,10 +463,11 @@ __global__ void __launch_bounds__(kRedThreads) k_rescale(PkParams P, PkState* st
 //                    4: count/sum of x > theta
 //                    5: objective = sum p(0.5u + g0s)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_reduce(PkParams P, PkState* st, int mode,
+__global__ void __launch_bounds__(kRedThreads) k_reduce(const PkParams* __restrict__ Pp, PkState* st, int mode,
                                                         const T* a, const T* b, const T* c,
                                                         const T* d, double theta,
                                                         double* part) {
+    const PkParams& P = *Pp;
     const T gs = (T)P.gshift;
     double acc[3] = {0, 0, 0};
     if (mode == 0) { acc[0] = (double)INFINITY; acc[1] = -(double)INFINITY; }
@@ -502,8 +513,9 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(PkParams P, PkState* st,
 
 // gd = sum double(g) * double(z - p)  (contact_solver.cpp:345-346)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_gd(PkParams P, PkState* st, const T* g,
+__global__ void __launch_bounds__(kRedThreads) k_gd(const PkParams* __restrict__ Pp, PkState* st, const T* g,
                                                     const T* z, const T* p, double* part) {
+    const PkParams& P = *Pp;
     double acc[1] = {0};
     GRID_LOOP4(P.N) {
         T G[4], Z[4], Pp[4];
@@ -577,6 +589,17 @@ __global__ void k_to_f64(long N, double* out, const T* x) {
         out[i] = (double)x[i];
 }
 
+// out = float(x - datum): the FP32 stage's gap, centred before the cast so a
+// large datum is not rounded into the field (nested_solve.cpp:871-917)
+__global__ void k_center_cast(long N, float* out, const double* x, double datum) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        out[i] = (float)(x[i] - datum);
+}
+__global__ void k_cast_f32(long N, float* out, const double* x) {
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        out[i] = (float)x[i];
+}
+
 // z[C] -= T(zmean) (the standalone preconditioner entry point)
 template <typename T>
 __global__ void k_sub_zmean(long N, T* z, const uint8_t* mask, const PkState* st) {
@@ -599,6 +622,12 @@ __global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, cons
     }
 }
 
+// ---- device-side loop control -------------------------------------------------------
+// Last kernel of the graph body: keep looping while no pass has set `halt`.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st) {
+    cudaGraphSetConditional(h, st->halt == H_RUN ? 1u : 0u);
+}
+
 // ---- host driver -----------------------------------------------------------------
 namespace {
 
@@ -609,65 +638,178 @@ int red_grid(long N) {
     return (int)g;
 }
 
+// Per-operator, per-precision solver context: the CG workspace, the device
+// parameter block and the instantiated loop graph (a while-conditional node
+// whose body is one CG iteration), reused by every solve with the same
+// preconditioner configuration.
 template <typename T>
-struct Workspace {
+struct SolverCtx : SolverCtxBase {
+    Operator& op;
     long N = 0;
     T *p = nullptr, *t = nullptr, *u = nullptr, *g = nullptr, *gprev = nullptr, *z = nullptr,
       *r = nullptr, *best = nullptr;
+    T* g0c = nullptr;  // the solve's gap, copied in so the loop graph is reusable
     uint8_t* mask = nullptr;
     double* part = nullptr;
     double* hist = nullptr;
+    int hist_cap = 0;
     PkState* st = nullptr;
-    cudaStream_t s = nullptr;
-    void alloc(long n, bool keep_best, int hist_len, cudaStream_t stream) {
-        N = n;
-        s = stream;
-        const size_t b = (size_t)n * sizeof(T);
-        T** vecs[] = {&p, &t, &u, &g, &gprev, &z, &r};
-        for (T** v : vecs) ASB_CUDA(cudaMallocAsync((void**)v, b, s));
-        if (keep_best) ASB_CUDA(cudaMallocAsync((void**)&best, b, s));
-        ASB_CUDA(cudaMallocAsync((void**)&mask, (size_t)n, s));
-        ASB_CUDA(cudaMallocAsync((void**)&part, kMaxBlocks * 8 * sizeof(double), s));
-        ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
-        if (hist_len > 0) ASB_CUDA(cudaMallocAsync((void**)&hist, hist_len * sizeof(double), s));
-        ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));
+    PkParams* Pd = nullptr;
+    StencilTaps taps{};
+    int precond = -1, radius = -1;
+    int grid = 1;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph = nullptr;
+
+    explicit SolverCtx(Operator& o) : op(o) {
+        N = (long)o.Ns * o.Ns;
+        const size_t b = (size_t)N * sizeof(T);
+        T** vecs[] = {&p, &t, &u, &g, &gprev, &z, &r, &best, &g0c};
+        for (T** v : vecs) ASB_CUDA(cudaMalloc((void**)v, b));
+        ASB_CUDA(cudaMalloc((void**)&mask, (size_t)N));
+        ASB_CUDA(cudaMalloc((void**)&part, kMaxBlocks * 8 * sizeof(double)));
+        ASB_CUDA(cudaMalloc((void**)&st, sizeof(PkState)));
+        ASB_CUDA(cudaMalloc((void**)&Pd, sizeof(PkParams)));
+        ASB_CUDA(cudaMemset(st, 0, sizeof(PkState)));
+        grid = red_grid(N);
+        (void)o.spectrum(sizeof(T) == 8, nullptr);  // allocate before any capture
     }
-    ~Workspace() {
-        void* all[] = {p, t, u, g, gprev, z, r, best, mask, part, hist, st};
+    ~SolverCtx() override {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd};
         for (void* v : all)
-            if (v) cudaFreeAsync(v, s);
+            if (v) cudaFree(v);
+    }
+    size_t bytes() const override {
+        return (9 * sizeof(T) + 1) * (size_t)N + hist_cap * sizeof(double) +
+               kMaxBlocks * 8 * sizeof(double);
+    }
+    void ensure_hist(int cap) {
+        if (cap <= hist_cap) return;
+        if (hist) ASB_CUDA(cudaFree(hist));
+        ASB_CUDA(cudaMalloc((void**)&hist, (size_t)cap * sizeof(double)));
+        hist_cap = cap;
+        drop_graph();  // the graph bakes the history pointer
+    }
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    void configure(int pc, int R) {
+        if (pc == precond && (pc != 1 || R == radius)) return;
+        if (pc == 1) taps = make_stencil_taps(op.Ns, R);
+        precond = pc;
+        radius = R;
+        drop_graph();
+    }
+
+    void apply(const T* x, T* y, const int* gate, cudaStream_t s) {
+        op.matvec(sizeof(T) == 8, x, y, s, gate);
+    }
+    void precond_apply(const int* gate, cudaStream_t s) {
+        if (precond == 1) {
+            k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, g, mask, z, part,
+                                                            gate != nullptr);
+            count_launches(1);
+            ASB_CUDA(cudaGetLastError());
+        } else if (precond == 2) {
+            fourier_precond_pk<T>(op, g, mask, st, z, part, s, gate);
+        }
+    }
+    // one CG iteration (the common path), every pass gated on the device
+    void enqueue_iteration(const T* g0, cudaStream_t s) {
+        apply(p, u, &st->skip_mv1, s);
+        k_eval1<T><<<grid, kRedThreads, 0, s>>>(Pd, st, u, g0, p, g, part, 0);
+        k_eval2<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, g, mask, part, hist, 0);
+        if (precond > 0) precond_apply(&st->halt, s);
+        k_dots<T><<<grid, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
+        k_tupd<T><<<grid, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
+        apply(t, r, &st->halt, s);
+        k_rsum<T><<<grid, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
+        k_den<T><<<grid, kRedThreads, 0, s>>>(Pd, st, r, t, mask, part);
+        k_pupd<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
+        k_rescale<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, part);
+        count_launches(8);
+        ASB_CUDA(cudaGetLastError());
+    }
+    // Graph: while (halt == H_RUN) { iteration }.  The g0 pointer is baked
+    // in, so the graph is rebuilt when a solve passes another gap buffer.
+    const T* graph_g0 = nullptr;
+    void build_graph(const T* g0, cudaStream_t s) {
+        drop_graph();
+        ASB_CUDA(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle h;
+        ASB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        ASB_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        ASB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                               cudaStreamCaptureModeRelaxed));
+        enqueue_iteration(g0, s);
+        k_loop_cond<<<1, 1, 0, s>>>(h, st);
+        cudaGraph_t captured = nullptr;
+        ASB_CUDA(cudaStreamEndCapture(s, &captured));
+        ASB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+        graph_g0 = g0;
+    }
+    // (Re)build the loop graph if needed.  Before capturing, one fully gated
+    // iteration runs eagerly (every kernel returns at entry) so that all
+    // function attributes are set outside the capture.  Clobbers st; the
+    // caller writes the initial state afterwards.
+    void ensure_graph(const T* g0, cudaStream_t s) {
+        if (exec && graph_g0 == g0) return;
+        PkState gated;
+        std::memset(&gated, 0, sizeof(gated));
+        gated.halt = H_FINAL;
+        gated.skip_mv1 = 1;
+        ASB_CUDA(cudaMemcpyAsync(st, &gated, sizeof(PkState), cudaMemcpyHostToDevice, s));
+        enqueue_iteration(g0, s);
+        ASB_CUDA(cudaStreamSynchronize(s));
+        build_graph(g0, s);
+    }
+    void launch_graph(cudaStream_t s) {
+        ASB_CUDA(cudaGraphLaunch(exec, s));
+        count_launches(1);
     }
 };
 
 template <typename T>
 struct Solver {
-    Operator& op;
+    SolverCtx<T>& c;
     PkParams P{};
-    Workspace<T> w;
-    StencilTaps taps{};
     cudaStream_t s;
-    int grid;
     PkState h{};  // host mirror
+    const T* g0 = nullptr;
+    long long mv_host = 0;
 
-    Solver(Operator& o, cudaStream_t st) : op(o), s(st) {}
+    Solver(SolverCtx<T>& ctx, cudaStream_t st) : c(ctx), s(st) {}
 
     void read_state() {
-        ASB_CUDA(cudaMemcpyAsync(&h, w.st, sizeof(PkState), cudaMemcpyDeviceToHost, s));
+        ASB_CUDA(cudaMemcpyAsync(&h, c.st, sizeof(PkState), cudaMemcpyDeviceToHost, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
     void write_state() {
-        ASB_CUDA(cudaMemcpyAsync(w.st, &h, sizeof(PkState), cudaMemcpyHostToDevice, s));
+        ASB_CUDA(cudaMemcpyAsync(c.st, &h, sizeof(PkState), cudaMemcpyHostToDevice, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
     // results of the helper reductions live in st->red; only that slice is
     // read back so the host mirror `h` is never clobbered mid-update
     void read_red(double (&r)[8]) {
-        ASB_CUDA(cudaMemcpyAsync(r, w.st->red, sizeof(r), cudaMemcpyDeviceToHost, s));
+        ASB_CUDA(cudaMemcpyAsync(r, c.st->red, sizeof(r), cudaMemcpyDeviceToHost, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
-    double reduce(int mode, const T* a, const T* b, const T* c, const T* d, double theta,
+    double reduce(int mode, const T* a, const T* b, const T* cc, const T* d, double theta,
                   double* out3 = nullptr) {
-        k_reduce<T><<<grid, kRedThreads, 0, s>>>(P, w.st, mode, a, b, c, d, theta, w.part);
+        k_reduce<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, mode, a, b, cc, d, theta, c.part);
+        count_launches(1);
         ASB_CUDA(cudaGetLastError());
         double r[8];
         read_red(r);
@@ -675,46 +817,15 @@ struct Solver {
         return r[0];
     }
 
-    void apply(const T* x, T* y, const int* gate) {
-        op.matvec(sizeof(T) == 8, x, y, s, gate);
-    }
-
-    void precond_apply(const int* gate) {
-        if (P.precond == 1) {
-            k_stencil<T><<<stencil_grid(P.Ns), 256, 0, s>>>(P, w.st, taps, w.g, w.mask, w.z, w.part,
-                                                           gate != nullptr);
-            ASB_CUDA(cudaGetLastError());
-        } else if (P.precond == 2) {
-            fourier_precond_pk<T>(op, w.g, w.mask, w.st, w.z, w.part, s, gate);
-        }
-    }
-
-    // one CG iteration (common path), all gated on the device
-    void enqueue_iteration() {
-        apply(w.p, w.u, &w.st->skip_mv1);
-        k_eval1<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.u, g0, w.p, w.g, w.part, 0);
-        k_eval2<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.g, w.mask, w.part, w.hist, 0);
-        if (P.precond) precond_apply(&w.st->halt);
-        k_dots<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.z, w.g, w.gprev, w.mask, w.part);
-        k_tupd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.z, w.g, w.gprev, w.t, w.mask, w.p,
-                                               w.best);
-        apply(w.t, w.r, &w.st->halt);
-        k_rsum<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.r, w.g, w.t, w.mask, w.part);
-        k_den<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.r, w.t, w.mask, w.part);
-        k_pupd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.t, w.g, w.part);
-        k_rescale<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.part);
-        ASB_CUDA(cudaGetLastError());
-    }
-
-    // project_load_simplex on w.z (contact_solver.cpp:31-60)
+    // project_load_simplex on c.z (contact_solver.cpp:31-60)
     void project_simplex(double P_total) {
         const long N = P.N;
-        double ssum = reduce(1, w.z, nullptr, nullptr, nullptr, 0.0);
+        double ssum = reduce(1, c.z, nullptr, nullptr, nullptr, 0.0);
         long nact = N;
         double theta = (ssum - P_total) / (double)nact;
         for (int pass = 0; pass < 64; ++pass) {
             double o[3];
-            reduce(4, w.z, nullptr, nullptr, nullptr, theta, o);
+            reduce(4, c.z, nullptr, nullptr, nullptr, theta, o);
             const long n2 = (long)o[1];
             if (n2 == 0) break;
             if (n2 == nact) break;
@@ -722,36 +833,39 @@ struct Solver {
             ssum = o[0];
             theta = (ssum - P_total) / (double)nact;
         }
-        k_threshold<T><<<grid, kRedThreads, 0, s>>>(N, w.z, (T)theta);
+        k_threshold<T><<<c.grid, kRedThreads, 0, s>>>(N, c.z, (T)theta);
+        count_launches(1);
         ASB_CUDA(cudaGetLastError());
     }
 
-    // identification step (contact_solver.cpp:314-364); state h is current
+    // identification step (contact_solver.cpp:314-364); host mirror h is current
     bool identification_step(double& s_id, int& id_steps) {
         double o[3];
-        reduce(2, w.p, w.u, g0, nullptr, 0.0, o);
+        reduce(2, c.p, c.u, g0, nullptr, 0.0, o);
         const double f_cur = o[0];
         if (!(s_id > 0.0)) {
             const double pp = o[1], pu = o[2];
             s_id = (pu > 0.0 && pp > 0.0) ? pp / pu : 1.0;
         }
         for (int trial = 0; trial < 12; ++trial) {
-            k_axpy_trial<T><<<grid, kRedThreads, 0, s>>>(P.N, w.z, w.p, w.g, (T)s_id);
+            k_axpy_trial<T><<<c.grid, kRedThreads, 0, s>>>(P.N, c.z, c.p, c.g, (T)s_id);
+            count_launches(1);
             project_simplex(P.P_total);
-            apply(w.z, w.r, nullptr);
+            c.apply(c.z, c.r, nullptr, s);
             mv_host++;
-            reduce(3, w.z, w.r, g0, nullptr, 0.0, o);
+            reduce(3, c.z, c.r, g0, nullptr, 0.0, o);
             const double f_try = o[0];
-            k_gd<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.g, w.z, w.p, w.part);
+            k_gd<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.g, c.z, c.p, c.part);
+            count_launches(1);
             double rr[8];
             read_red(rr);
             const double gd = rr[3];
             if (std::isfinite(f_try) && gd < 0.0 && f_try <= f_cur + 1e-4 * gd) {
                 const size_t b = (size_t)P.N * sizeof(T);
-                ASB_CUDA(cudaMemcpyAsync(w.p, w.z, b, cudaMemcpyDeviceToDevice, s));
-                ASB_CUDA(cudaMemcpyAsync(w.u, w.r, b, cudaMemcpyDeviceToDevice, s));
-                ASB_CUDA(cudaMemsetAsync(w.t, 0, b, s));
-                ASB_CUDA(cudaMemsetAsync(w.gprev, 0, b, s));
+                ASB_CUDA(cudaMemcpyAsync(c.p, c.z, b, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemcpyAsync(c.u, c.r, b, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemsetAsync(c.t, 0, b, s));
+                ASB_CUDA(cudaMemsetAsync(c.gprev, 0, b, s));
                 h.u_fresh = 1;
                 h.delta = 0.0;
                 h.G_old = 1.0;
@@ -764,30 +878,31 @@ struct Solver {
         return false;
     }
 
-    const T* g0 = nullptr;
-    long long mv_host = 0;
-
     void run(const aspher_solve_opts& o, const T* g0_, double p_bar, const T* p_init,
              double* pressure, double* disp, double* gap, double* hist_host, int hist_cap,
              aspher_result& res) {
         const auto t_start = std::chrono::steady_clock::now();
-        g0 = g0_;
-        const int Ns = op.Ns;
+        const int Ns = c.op.Ns;
         const long N = (long)Ns * Ns;
+        // the caller's gap is read once into the context (zero-copy is not
+        // needed on a 180 GB device, and a fixed address keeps the graph valid)
+        if (g0_ != c.g0c)
+            ASB_CUDA(cudaMemcpyAsync(c.g0c, g0_, (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice,
+                                     s));
+        g0 = c.g0c;
         constexpr bool is_double = sizeof(T) == 8;
         if (!(p_bar > 0.0) || !std::isfinite(p_bar))
             throw Error(ASPHER_EINVAL, "solve_contact: empty gap or p_bar <= 0");
         if (!(o.tol > 0.0)) throw Error(ASPHER_EINVAL, "solve_contact: tol must be positive");
         if (o.max_iter < 0) throw Error(ASPHER_EINVAL, "solve_contact: max_iter must be >= 0");
         if (o.precond < 0 || o.precond > 2) throw Error(ASPHER_EINVAL, "solve_contact: bad precond");
-        if (o.precond == 1) taps = make_stencil_taps(Ns, o.precond_radius);
-        grid = red_grid(N);
-        const int hist_len = o.record_history ? o.max_iter + 1 : 0;
-        w.alloc(N, o.keep_best != 0, hist_len, s);
+        c.configure(o.precond, o.precond_radius);
+        if (o.record_history) c.ensure_hist(o.max_iter + 1);
         P.N = N;
         P.Ns = Ns;
         // validation before any operator apply (contact_solver.cpp:159-168)
         double mm[3];
+        ASB_CUDA(cudaMemcpyAsync(c.Pd, &P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
         reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
         if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
         const double P_total = (double)(T)p_bar * (double)N;
@@ -813,7 +928,7 @@ struct Solver {
         P.max_iter = o.max_iter;
         P.stall_limit = o.stall_limit > 0 ? o.stall_limit : 200;
         P.keep_best = o.keep_best;
-        P.record_history = o.record_history && hist_len > 0;
+        P.record_history = o.record_history && c.hist_cap > 0;
         P.use_pr = o.use_pr;
         P.precond = o.precond;
         P.P_total = P_total;
@@ -822,20 +937,23 @@ struct Solver {
         P.load_tol = load_tol;
         P.p_bar = (double)(T)p_bar;
         P.gshift = subtract ? (double)(T)datum : 0.0;
+        ASB_CUDA(cudaMemcpyAsync(c.Pd, &P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
 
         // initial pressure (contact_solver.cpp:204-223)
         const T pb = (T)p_bar;
         if (p_init) {
-            k_clamp_pos<T><<<grid, kRedThreads, 0, s>>>(N, w.p, p_init);
-            const double ssum = reduce(1, w.p, nullptr, nullptr, nullptr, 0.0);
-            if (ssum > 0.0) k_scale<T><<<grid, kRedThreads, 0, s>>>(N, w.p, (T)(P_total / ssum));
-            else k_fill<T><<<grid, kRedThreads, 0, s>>>(N, w.p, pb);
+            k_clamp_pos<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, p_init);
+            count_launches(1);
+            const double ssum = reduce(1, c.p, nullptr, nullptr, nullptr, 0.0);
+            if (ssum > 0.0) k_scale<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, (T)(P_total / ssum));
+            else k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, pb);
         } else {
-            k_fill<T><<<grid, kRedThreads, 0, s>>>(N, w.p, pb);
+            k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, pb);
         }
-        ASB_CUDA(cudaMemsetAsync(w.t, 0, (size_t)N * sizeof(T), s));
-        ASB_CUDA(cudaMemsetAsync(w.gprev, 0, (size_t)N * sizeof(T), s));
-        ASB_CUDA(cudaMemsetAsync(w.z, 0, (size_t)N * sizeof(T), s));
+        count_launches(1);
+        ASB_CUDA(cudaMemsetAsync(c.t, 0, (size_t)N * sizeof(T), s));
+        ASB_CUDA(cudaMemsetAsync(c.gprev, 0, (size_t)N * sizeof(T), s));
+        ASB_CUDA(cudaMemsetAsync(c.z, 0, (size_t)N * sizeof(T), s));
         std::memset(&h, 0, sizeof(h));
         h.G_old = 1.0;
         h.delta = 0.0;
@@ -844,20 +962,18 @@ struct Solver {
         h.status = ST_MAX_ITERATIONS;
         h.halt = o.max_iter > 0 ? H_RUN : H_FINAL;
         h.skip_mv1 = h.halt ? 1 : 0;
+        c.ensure_graph(g0, s);
         write_state();
 
         double s_id = 0.0;
         int forced_id = 0, id_steps = 0;
         std::string reason;
-        int batch = 2;
         while (h.halt == H_RUN) {
-            for (int k = 0; k < batch; ++k) enqueue_iteration();
+            c.launch_graph(s);
             read_state();
-            if (batch < 16) batch *= 2;
-            if (h.halt == H_RUN) continue;
-            if (h.halt == H_FINAL) break;
+            if (h.halt == H_RUN || h.halt == H_FINAL) break;
             if (h.copy_best) {
-                ASB_CUDA(cudaMemcpyAsync(w.best, w.p, (size_t)N * sizeof(T),
+                ASB_CUDA(cudaMemcpyAsync(c.best, c.p, (size_t)N * sizeof(T),
                                          cudaMemcpyDeviceToDevice, s));
                 h.copy_best = 0;
                 h.have_best = 1;
@@ -890,7 +1006,6 @@ struct Solver {
             h.halt = H_RUN;
             h.skip_mv1 = h.u_fresh ? 1 : 0;
             write_state();
-            batch = 2;
         }
         h.mv += mv_host;
         mv_host = 0;
@@ -900,20 +1015,21 @@ struct Solver {
         if (status != ST_CONVERGED && o.keep_best && h.have_best) {
             const double merit = std::max(h.fw, h.pen);
             if (!(merit <= h.best_merit)) {
-                ASB_CUDA(cudaMemcpyAsync(w.p, w.best, (size_t)N * sizeof(T),
+                ASB_CUDA(cudaMemcpyAsync(c.p, c.best, (size_t)N * sizeof(T),
                                          cudaMemcpyDeviceToDevice, s));
                 h.u_fresh = 0;
                 returned_best = true;
             }
         }
         if (!h.u_fresh) {
-            apply(w.p, w.u, nullptr);
+            c.apply(c.p, c.u, nullptr, s);
             h.mv++;
         }
         h.halt = H_FINAL;
         write_state();
-        k_eval1<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.u, g0, w.p, w.g, w.part, 1);
-        k_eval2<T><<<grid, kRedThreads, 0, s>>>(P, w.st, w.p, w.g, w.mask, w.part, nullptr, 1);
+        k_eval1<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.u, g0, c.p, c.g, c.part, 1);
+        k_eval2<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.p, c.g, c.mask, c.part, nullptr, 1);
+        count_launches(2);
         ASB_CUDA(cudaGetLastError());
         read_state();
         if (!h.finite && status != ST_NONFINITE) status = ST_NONFINITE;
@@ -928,18 +1044,19 @@ struct Solver {
             }
         }
         double ob[3];
-        reduce(5, w.p, w.u, g0, nullptr, 0.0, ob);
-        k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, pressure, w.p);
+        reduce(5, c.p, c.u, g0, nullptr, 0.0, ob);
+        k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, pressure, c.p);
+        count_launches(1);
         if (!o.light) {
-            if (disp) k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, disp, w.u);
-            if (gap) k_to_f64<T><<<grid, kRedThreads, 0, s>>>(N, gap, w.g);
+            if (disp) { k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, disp, c.u); count_launches(1); }
+            if (gap) { k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, gap, c.g); count_launches(1); }
         }
         ASB_CUDA(cudaGetLastError());
         int hl = 0;
-        if (o.record_history && hist_host && hist_cap > 0 && hist_len > 0) {
+        if (o.record_history && hist_host && hist_cap > 0 && c.hist_cap > 0) {
             hl = std::min(h.it, hist_cap);
             if (hl > 0)
-                ASB_CUDA(cudaMemcpyAsync(hist_host, w.hist, hl * sizeof(double),
+                ASB_CUDA(cudaMemcpyAsync(hist_host, c.hist, hl * sizeof(double),
                                          cudaMemcpyDeviceToHost, s));
         }
         ASB_CUDA(cudaStreamSynchronize(s));
@@ -980,6 +1097,13 @@ struct Solver {
                              .count();
     }
 };
+
+template <typename T>
+SolverCtx<T>& get_ctx(Operator& op) {
+    std::shared_ptr<SolverCtxBase>& slot = sizeof(T) == 8 ? op.ctx_d : op.ctx_f;
+    if (!slot) slot = std::make_shared<SolverCtx<T>>(op);
+    return static_cast<SolverCtx<T>&>(*slot);
+}
 
 }  // namespace
 
@@ -1044,7 +1168,7 @@ template <typename T>
 void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
                 int hist_cap, aspher_result& res, cudaStream_t s) {
-    Solver<T> S(op, s);
+    Solver<T> S(get_ctx<T>(op), s);
     S.run(o, (const T*)g0, p_bar, (const T*)p_init, pressure, disp, gap, hist, hist_cap, res);
 }
 template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*, double,
@@ -1053,6 +1177,79 @@ template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*
 template void solve_impl<double>(Operator&, const aspher_solve_opts&, const void*, double,
                                  const void*, double*, double*, double*, double*, int,
                                  aspher_result&, cudaStream_t);
+
+
+// FP32 stage + FP64 polish (the reference's float_then_double staging,
+// nested_solve.cpp:871-974, on one level): the gap is centred by its
+// midpoint datum and cast to FP32 on the device, the FP32 PK solve runs to
+// float_tol with FP64 reductions, and -- when polish -- an FP64 PK solve
+// warm-started from that pressure certifies the requested tol.
+void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
+                 const double* p_init, double float_tol, int polish, double* pressure,
+                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
+                 cudaStream_t s) {
+    SolverCtx<double>& cd = get_ctx<double>(op);
+    SolverCtx<float>& cf = get_ctx<float>(op);
+    const long N = (long)op.Ns * op.Ns;
+    // FP64 statistics of the gap (validation before any apply)
+    Solver<double> probe(cd, s);
+    probe.P.N = N;
+    probe.P.Ns = op.Ns;
+    ASB_CUDA(cudaMemcpyAsync(cd.Pd, &probe.P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
+    double mm[3];
+    probe.reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
+    if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
+    const double datum = o.datum_mode == ASPHER_DATUM_AUTOMATIC ? mm[0] + 0.5 * (mm[1] - mm[0])
+                                                                 : o.datum;
+    double g_ref = o.g_ref;
+    if (!(g_ref > 0.0)) g_ref = mm[1] - mm[0];
+    if (!(g_ref > 0.0)) g_ref = 1.0;
+    const int grid = red_grid(N);
+    k_center_cast<<<grid, kRedThreads, 0, s>>>(N, cf.g0c, g0, o.datum_mode == ASPHER_DATUM_CALLER ? 0.0 : datum);
+    count_launches(1);
+    float* pinit_f = nullptr;
+    if (p_init) {
+        pinit_f = cf.r;  // scratch: read by the FP32 solve before r is first written
+        k_cast_f32<<<grid, kRedThreads, 0, s>>>(N, pinit_f, p_init);
+        count_launches(1);
+    }
+    ASB_CUDA(cudaGetLastError());
+    aspher_solve_opts of = o;
+    of.dtype = ASPHER_F32;
+    of.tol = float_tol;
+    of.requested_tol = polish ? float_tol : (o.requested_tol > 0.0 ? o.requested_tol : o.tol);
+    of.allow_tolerance_relaxation = polish ? 1 : o.allow_tolerance_relaxation;
+    of.datum_mode = ASPHER_DATUM_CALLER;
+    of.datum = datum;
+    of.g_ref = g_ref;
+    of.light = polish ? 1 : o.light;
+    aspher_result rf;
+    {
+        Solver<float> S(cf, s);
+        S.run(of, cf.g0c, p_bar, pinit_f, pressure, polish ? nullptr : disp,
+              polish ? nullptr : gap, nullptr, 0, rf);
+    }
+    if (res_float) *res_float = rf;
+    if (!polish) {
+        res = rf;
+        return;
+    }
+    aspher_solve_opts od = o;
+    od.dtype = ASPHER_F64;
+    od.datum_mode = ASPHER_DATUM_SOLVER;
+    od.datum = datum;
+    od.g_ref = g_ref;
+    {
+        Solver<double> S(cd, s);
+        S.run(od, g0, p_bar, pressure, pressure, disp, gap, nullptr, 0, res);
+    }
+    // the reported work is the sum of both stages (nested_solve.cpp:445-450)
+    res.iterations += rf.iterations;
+    res.matvec_count += rf.matvec_count;
+    res.precond_count += rf.precond_count;
+    res.identification_steps += rf.identification_steps;
+    res.time_total += rf.time_total;
+}
 
 // Standalone preconditioner apply: z = M^-1 g on contact, contact-mean removed.
 template <typename T>
@@ -1068,18 +1265,25 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     P.N = N;
     P.Ns = op.Ns;
     P.precond = precond;
+    PkParams* Pd = nullptr;
+    ASB_CUDA(cudaMallocAsync((void**)&Pd, sizeof(PkParams), s));
+    ASB_CUDA(cudaMemcpyAsync(Pd, &P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
     const int grid = red_grid(N);
     k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
     if (precond == 1) {
         StencilTaps taps = make_stencil_taps(op.Ns, radius);
-        k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(P, st, taps, g, mask, z, part, 0);
+        k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, g, mask, z, part, 0);
+        count_launches(1);
     } else {
         fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
     }
     k_sub_zmean<T><<<grid, kRedThreads, 0, s>>>(N, z, mask, st);
+    count_launches(2);
     ASB_CUDA(cudaGetLastError());
+    ASB_CUDA(cudaStreamSynchronize(s));
     cudaFreeAsync(st, s);
     cudaFreeAsync(part, s);
+    cudaFreeAsync(Pd, s);
     ASB_CUDA(cudaStreamSynchronize(s));
 }
 template void precond_apply_impl<float>(Operator&, int, int, const float*, const uint8_t*, float*,

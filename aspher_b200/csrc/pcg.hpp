@@ -31,6 +31,18 @@ void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
                 int hist_cap, aspher_result& res, cudaStream_t s);
 
+void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
+                 const double* p_init, double float_tol, int polish, double* pressure,
+                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
+                 cudaStream_t s);
+
+void solve_nested(int kind, int Ns, double L, double E, const double* g0, double p_bar,
+                  const aspher_nested_opts& np, double* pressure, double* disp, double* gap,
+                  double* hist_host, int hist_cap, aspher_result& res, aspher_stage* stages,
+                  int stage_cap, int* nstages, cudaStream_t s);
+bool stencil_for_level(int engine, bool precond, double prev_occupancy, double occupancy_max);
+void clear_operator_cache();
+
 template <typename T>
 void precond_apply_impl(Operator& op, int precond, int radius, const T* g, const uint8_t* mask,
                         T* z, cudaStream_t s);

@@ -58,6 +58,10 @@ enum aspher_datum_mode { ASPHER_DATUM_AUTOMATIC = 0, ASPHER_DATUM_SOLVER = 1, AS
 
 int aspher_abi_version(void);
 const char* aspher_last_error(void);
+/* Number of CUDA kernel launches this library has issued in this process
+ * (a CUDA-graph launch counts once); for launch accounting in benchmarks.
+ * No reference counterpart. */
+int64_t aspher_launch_count(void);
 /* to_string(SolveStatus), reference src/contact_solver.cpp:12-23 */
 const char* aspher_status_string(int status);
 
@@ -169,6 +173,8 @@ typedef struct {
     int64_t mem_contact_mask;
     int64_t mem_output_arrays;
     int64_t mem_peak;
+    double time_build;       /* nested driver: operator construction, seconds */
+    double time_coarse;      /* nested driver: coarse-level solves, seconds */
 } aspher_result;
 
 /* solve_contact_impl<Real> (include/contact_solver.hpp:244-249; reference
@@ -186,6 +192,84 @@ int aspher_solve(aspher_op* op, const aspher_solve_opts* opts, const void* g0_de
                  const void* p_init_dev, double* pressure_dev, double* displacement_dev,
                  double* gap_dev, double* history_host, int history_cap, aspher_result* res,
                  void* stream);
+
+/* Mixed-precision solve: FP32 operator/CG with FP64-accumulated reductions
+ * to float_tol, then (polish != 0) an FP64 PK solve warm-started from it that
+ * certifies opts->tol on the FP64 operator.  This is the reference's
+ * float_then_double staging (src/nested_solve.cpp:871-974,
+ * include/nested_solve.hpp:53-68) applied to one grid.  g0_dev and
+ * p_init_dev are FP64 (opts->dtype is ignored); the gap is centred by its
+ * datum and cast to FP32 on the device.  *res holds the final stage with
+ * iterations / matvec / precond counts summed over both stages;
+ * res_float (nullable) receives the FP32 stage alone.  Synchronous. */
+int aspher_solve_mixed(aspher_op* op, const aspher_solve_opts* opts, const double* g0_dev,
+                       double p_bar, const double* p_init_dev, double float_tol, int polish,
+                       double* pressure_dev, double* displacement_dev, double* gap_dev,
+                       aspher_result* res, aspher_result* res_float, void* stream);
+
+/* ---- nested-grid driver ---------------------------------------------------- */
+/* NestedParams, reference include/nested_solve.hpp:11-119 (the fields that
+ * apply to the fft / periodic backends; the H2 q / leaf_side are kept for
+ * signature compatibility, leaf_side still clamps the stencil radius). */
+typedef struct {
+    double tol;
+    int max_iter;
+    int use_pr;
+    int coarsest;
+    int q;
+    int leaf_side;
+    int precond;               /* bool */
+    int precond_engine;        /* 0 auto, 1 stencil, 2 fft */
+    int precond_radius;
+    double precond_occupancy_max;
+    double coarse_tol;
+    int single_precision;      /* legacy spelling of precision = float */
+    int precision;             /* 0 defer to single_precision, 1 double, 2 float, 3 float_then_double */
+    double float_floor;
+    int allow_tolerance_relaxation;
+    int light_result;
+    int record_error_history;
+    int active_set;            /* rejected for fft/periodic, as in the reference */
+} aspher_nested_opts;
+
+/* ContactResult::Stage, reference include/contact_solver.hpp:100-113 */
+typedef struct {
+    char name[32];             /* "coarse:128", "finest:2048", "polish:2048" */
+    char precision[8];         /* "float" | "double" */
+    int q;
+    double requested_tol;
+    double effective_tol;
+    int iterations;
+    int64_t matvec_count;
+    double seconds;
+    int status;
+    double fw_error;
+    double penetration_error;
+    int precond_dropped;
+} aspher_stage;
+
+/* Fills the reference defaults (python/bindings.cpp:836-853). */
+void aspher_nested_opts_default(aspher_nested_opts* o);
+
+/* solve_contact_nested for backend FFT / PERIODIC (include/nested_solve.hpp:146-151,
+ * reference src/nested_solve.cpp:518-990).  g0_dev: Ns*Ns FP64 gap on the
+ * device (read only); outputs as for aspher_solve.  Operators of every
+ * level come from a per-process cache keyed by (backend, Ns, L, E*, device).
+ * stages (nullable) receives up to stage_cap entries, *nstages their count.
+ * Synchronous. */
+int aspher_solve_nested(int backend, int grid_size, double domain_size, double E_star,
+                        const double* g0_dev, double p_bar, const aspher_nested_opts* opts,
+                        double* pressure_dev, double* displacement_dev, double* gap_dev,
+                        double* history_host, int history_cap, aspher_result* res,
+                        aspher_stage* stages, int stage_cap, int* nstages, void* stream);
+
+/* stencil_for_level (include/nested_solve.hpp:132-133): which preconditioner
+ * engine a level uses; engine 0 auto, 1 stencil, 2 fft.  Returns 0 / 1. */
+int aspher_stencil_for_level(int engine, int precond, double prev_occupancy,
+                             double occupancy_max);
+
+/* Drops the cached per-level operators of aspher_solve_nested. */
+int aspher_operator_cache_clear(void);
 
 #ifdef __cplusplus
 }

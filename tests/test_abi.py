@@ -67,3 +67,21 @@ def test_invalid_arguments_raise_before_any_device_work():
         stencil_taps(4, 2)  # 2R+1 > Ns
     with pytest.raises(ValueError):
         stencil_taps(64, 0)
+
+
+def test_stencil_for_level_decision_table():
+    """tests/test_precond.cpp:68-101 (exhaustive table)."""
+    from aspher_b200.nested import stencil_for_level as f
+    omax = 0.4
+    assert not f("stencil", False, -1.0, omax)
+    assert not f("fft", False, 0.1, omax)
+    assert not f("auto", False, 0.9, omax)
+    assert f("stencil", True, -1.0, omax) and f("stencil", True, 0.0, omax)
+    assert f("stencil", True, 0.9, omax)
+    assert not f("fft", True, -1.0, omax) and not f("fft", True, 0.0, omax)
+    assert not f("fft", True, 0.9, omax)
+    assert f("auto", True, -1.0, omax) and f("auto", True, 0.0, omax)
+    assert f("auto", True, 0.39, omax)
+    assert not f("auto", True, 0.4, omax) and not f("auto", True, 0.41, omax)
+    assert not f("auto", True, 1.0, omax)
+    assert f("auto", True, 0.55, 0.6) and not f("auto", True, 0.65, 0.6)
