@@ -90,6 +90,11 @@ SIGNATURES = {
     "aspher_op_matvec": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_op_get_info": (C.c_int, [C.c_void_p, C.POINTER(OpInfo)]),
     "aspher_op_love_table": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "aspher_op_set_variants": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "aspher_op_get_variants": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "aspher_op_autotune": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "aspher_precond_apply": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
                                        C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_stencil_taps": (C.c_int, [C.c_int, C.c_int, C.POINTER(C.c_int),

@@ -101,6 +101,27 @@ class Operator:
         L.check(L.lib().aspher_op_get_info(self._h, C.byref(inf)))
         return inf
 
+    def variants(self, dtype=torch.float32):
+        """(row variant, column variant, column tile width) of this precision."""
+        rv, cv, ct = C.c_int(), C.c_int(), C.c_int()
+        L.check(L.lib().aspher_op_get_variants(self._h, L.F64 if dtype == torch.float64 else L.F32,
+                                               C.byref(rv), C.byref(cv), C.byref(ct)))
+        return rv.value, cv.value, ct.value
+
+    def set_variants(self, row_variant, col_variant, dtype=torch.float32):
+        L.check(L.lib().aspher_op_set_variants(
+            self._h, L.F64 if dtype == torch.float64 else L.F32, int(row_variant),
+            int(col_variant)))
+
+    def autotune(self, dtype=torch.float32, reps=5):
+        """Time every launch-variant pair of the three FFT passes, keep the
+        fastest (also for later operators of this shape); returns
+        (row variant, column variant, ms per apply)."""
+        rv, cv, ms = C.c_int(), C.c_int(), C.c_double()
+        L.check(L.lib().aspher_op_autotune(self._h, L.F64 if dtype == torch.float64 else L.F32,
+                                           int(reps), C.byref(rv), C.byref(cv), C.byref(ms)))
+        return rv.value, cv.value, ms.value
+
     def love_table(self):
         out = np.empty((self.Ns, self.Ns), dtype=np.float64)
         L.check(L.lib().aspher_op_love_table(self._h, out.ctypes.data_as(C.c_void_p)))

@@ -91,13 +91,45 @@ int aspher_op_get_info(const aspher_op* op, aspher_op_info* info) {
     info->grid_size = o.Ns;
     info->padded_side = o.kind == asb::OP_FFT ? 2 * o.Ns : o.Ns;
     info->n = (int64_t)o.Ns * o.Ns;
-    if (o.kind == asb::OP_FFT) {
-        info->bytes_spectrum = (int64_t)(o.Ns / o.ct_d + 1) * (o.Ns + 1) * o.ct_d * 8 +
-                               (int64_t)(o.Ns / o.ct_f + 1) * (o.Ns + 1) * o.ct_f * 4;
-    }
+    if (o.kind == asb::OP_FFT)
+        info->bytes_spectrum = (int64_t)(o.Ns + 16) * (o.Ns + 1) * 12 + (int64_t)(o.Ns + 1) * (o.Ns + 1) * 8;
     info->bytes_scratch = (int64_t)(o.spec_d_bytes + o.spec_f_bytes);
     info->bytes_total = (int64_t)o.resident_bytes();
     info->max_im_ratio = o.max_im_ratio;
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_set_variants(aspher_op* op, int dtype, int row_variant, int col_variant) {
+    ASB_API_BEGIN
+    if (!op || !op->impl) throw asb::Error(ASPHER_EINVAL, "aspher_op_set_variants: NULL operator");
+    op->impl->set_variants(dtype == ASPHER_F64, row_variant, col_variant);
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_get_variants(const aspher_op* op, int dtype, int* row_variant, int* col_variant,
+                           int* col_tile) {
+    ASB_API_BEGIN
+    if (!op || !op->impl) throw asb::Error(ASPHER_EINVAL, "aspher_op_get_variants: NULL operator");
+    const int d = dtype == ASPHER_F64;
+    if (row_variant) *row_variant = op->impl->rowv[d];
+    if (col_variant) *col_variant = op->impl->colv[d];
+    if (col_tile) *col_tile = op->impl->ct[d];
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_op_autotune(aspher_op* op, int dtype, int reps, int* row_variant, int* col_variant,
+                       double* best_ms) {
+    ASB_API_BEGIN
+    if (!op || !op->impl) throw asb::Error(ASPHER_EINVAL, "aspher_op_autotune: NULL operator");
+    if (reps < 1) throw asb::Error(ASPHER_EINVAL, "aspher_op_autotune: reps must be >= 1");
+    int rv = 0, cv = 0;
+    const double ms = op->impl->autotune(dtype == ASPHER_F64, reps, rv, cv);
+    if (row_variant) *row_variant = rv;
+    if (col_variant) *col_variant = cv;
+    if (best_ms) *best_ms = ms;
     return ASPHER_OK;
     ASB_API_END
 }

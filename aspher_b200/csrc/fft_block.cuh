@@ -100,6 +100,12 @@ __host__ __device__ constexpr int num_stages(int L, int RMAX) {
 
 __device__ __forceinline__ int smaddr(int i, int S, int off) { return (i + (i >> 4)) * S + off; }
 
+// a * w (forward) or a * conj(w) (inverse), w from the exp(-2 pi i k/L) table
+template <int DIR, typename V>
+__device__ __forceinline__ V tw_apply(V a, V w) {
+    return DIR < 0 ? cmul(a, w) : cmulc(a, w);
+}
+
 // Shared-memory elements needed by one transform of length L (padded).
 __host__ __device__ constexpr int sm_len(int L) { return L + L / 16 + 1; }
 
@@ -121,12 +127,37 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
 #pragma unroll
             for (int r = 0; r < R; ++r) a[r] = v[q + r * Q];
             if constexpr (SPAN > 1) {
+                // w^r for r = 1..R-1 from the loaded powers w, w^2, w^4, w^8
+                // (products at most three deep), applied as each is formed
                 const int jm = j % SPAN;
                 constexpr int TS = L / (SPAN * R);
-#pragma unroll
-                for (int r = 1; r < R; ++r) {
-                    const cplx<T> w = __ldg(&tw[r * jm * TS]);
-                    a[r] = DIR < 0 ? cmul(a[r], w) : cmulc(a[r], w);
+                const int b = jm * TS;
+                const cplx<T> w1 = __ldg(&tw[b]);
+                a[1] = tw_apply<DIR>(a[1], w1);
+                if constexpr (R >= 4) {
+                    const cplx<T> w2 = __ldg(&tw[2 * b]);
+                    a[2] = tw_apply<DIR>(a[2], w2);
+                    const cplx<T> w3 = cmul(w2, w1);
+                    a[3] = tw_apply<DIR>(a[3], w3);
+                    if constexpr (R >= 8) {
+                        const cplx<T> w4 = __ldg(&tw[4 * b]);
+                        a[4] = tw_apply<DIR>(a[4], w4);
+                        a[5] = tw_apply<DIR>(a[5], cmul(w4, w1));
+                        a[6] = tw_apply<DIR>(a[6], cmul(w4, w2));
+                        a[7] = tw_apply<DIR>(a[7], cmul(w4, w3));
+                        if constexpr (R >= 16) {
+                            const cplx<T> w8 = __ldg(&tw[8 * b]);
+                            a[8] = tw_apply<DIR>(a[8], w8);
+                            a[9] = tw_apply<DIR>(a[9], cmul(w8, w1));
+                            a[10] = tw_apply<DIR>(a[10], cmul(w8, w2));
+                            a[11] = tw_apply<DIR>(a[11], cmul(w8, w3));
+                            const cplx<T> w12 = cmul(w8, w4);
+                            a[12] = tw_apply<DIR>(a[12], w12);
+                            a[13] = tw_apply<DIR>(a[13], cmul(w12, w1));
+                            a[14] = tw_apply<DIR>(a[14], cmul(w12, w2));
+                            a[15] = tw_apply<DIR>(a[15], cmul(w12, w3));
+                        }
+                    }
                 }
             }
             dft<R, DIR, T>(a);

@@ -13,14 +13,22 @@
 // of which only the first Ns outputs are kept.
 //
 // The half spectrum lives in HBM in a column-tiled layout:
-//   elem(row, k) = base[(k / CT) * nrows * CT + row * CT + (k % CT)]
+//   elem(row, k) = base[(k / ct) * nrows * ct + row * ct + (k % ct)]
 // so a column CTA streams one contiguous tile and a row CTA of RB rows
-// touches RB*CT contiguous elements per tile.
+// touches RB*ct contiguous elements per tile.
+//
+// Launch shapes are variants (V = 0..kVariants-1) trading registers per
+// thread (RPT elements, radix <= RPT), CTA size and CTAs per SM; the
+// operator picks one row variant and one column variant per size and
+// precision (a default table, or the autotuner in operators.cu).
 #pragma once
 
 #include "fft_block.cuh"
 
 namespace asb {
+
+constexpr int kVariants = 4;
+constexpr int kSmemPerSM = 227 * 1024;
 
 template <typename T>
 struct TiledSpec {
@@ -32,29 +40,75 @@ struct TiledSpec {
     }
 };
 
-// ---- launch shapes ----------------------------------------------------------
-__host__ __device__ constexpr int rpt_for(int L) { return L >= 16 ? 16 : L; }
-
+// ---- variant tables -----------------------------------------------------------------
+// Row kernels.  FP32: V0 RPT16/512 thr/1 CTA, V1 RPT16/256/2, V2 RPT8/256/3,
+// V3 RPT8/512/2.  FP64: V0 RPT16/512/1, V1 RPT8/256/2, V2 RPT8/256/3,
+// V3 RPT8/512/1.
 template <typename T>
-__host__ __device__ constexpr int row_rb(int LR) {
-    const int tt = LR / rpt_for(LR);
-    int rb = 512 / tt;
+__host__ __device__ constexpr int row_rpt(int LR, int v) {
+    int want = sizeof(T) == 4 ? ((v <= 1) ? 16 : 8) : (v == 0 ? 16 : 8);
+    if (want < LR / 1024) want = LR / 1024;  // at most 1024 threads per transform
+    return LR < want ? LR : want;
+}
+template <typename T>
+__host__ __device__ constexpr int row_target_threads(int v) {
+    return (v == 0 || v == 3) ? 512 : 256;
+}
+template <typename T>
+__host__ __device__ constexpr int row_minb_req(int v) {
+    return sizeof(T) == 4 ? (v == 0 ? 1 : (v == 2 ? 3 : 2)) : (v == 1 ? 2 : (v == 2 ? 3 : 1));
+}
+template <typename T>
+__host__ __device__ constexpr int row_rb_v(int LR, int v) {
+    const int tt = LR / row_rpt<T>(LR, v);
+    int rb = row_target_threads<T>(v) / tt;
     if (rb < 1) rb = 1;
     if (rb > 16) rb = 16;
     const int per_row = sm_len(LR + 1) * (int)sizeof(cplx<T>);
-    while (rb > 1 && rb * per_row > 100 * 1024) rb >>= 1;
+    const int mb = row_minb_req<T>(v);
+    while (rb > 1 && rb * per_row * mb > kSmemPerSM) rb >>= 1;
     return rb;
 }
 template <typename T>
-__host__ __device__ constexpr int row_smem(int LR) {
-    return row_rb<T>(LR) * sm_len(LR + 1) * (int)sizeof(cplx<T>);
+__host__ __device__ constexpr int row_threads(int LR, int v) {
+    return row_rb_v<T>(LR, v) * (LR / row_rpt<T>(LR, v));
 }
 template <typename T>
-__host__ __device__ constexpr int col_ct(int LC, int ncols_minus1) {
-    const int tt = LC / rpt_for(LC);
+__host__ __device__ constexpr int row_smem_v(int LR, int v) {
+    return row_rb_v<T>(LR, v) * sm_len(LR + 1) * (int)sizeof(cplx<T>);
+}
+template <typename T>
+__host__ __device__ constexpr int row_minb(int LR, int v) {
+    int mb = row_minb_req<T>(v);
+    while (mb > 1 && mb * row_smem_v<T>(LR, v) > kSmemPerSM) --mb;
+    while (mb > 1 && mb * row_threads<T>(LR, v) > 2048) --mb;
+    return mb;
+}
+
+// Column kernel.  FP32: V0 RPT16/<=512 thr/1, V1 RPT16/<=256/2, V2 RPT8/<=512/2,
+// V3 RPT8/<=256/3.  FP64: V0 RPT16/<=512/1, V1 RPT8/<=256/2, V2 RPT8/<=512/1,
+// V3 RPT8/<=256/3.
+template <typename T>
+__host__ __device__ constexpr int col_rpt(int LC, int v) {
+    int want = sizeof(T) == 4 ? (v <= 1 ? 16 : 8) : (v == 0 ? 16 : 8);
+    if (want < LC / 1024) want = LC / 1024;  // at most 1024 threads per transform
+    return LC < want ? LC : want;
+}
+template <typename T>
+__host__ __device__ constexpr int col_max_threads(int v) {
+    return (v == 0 || v == 2) ? 512 : 256;
+}
+template <typename T>
+__host__ __device__ constexpr int col_minb_req(int v) {
+    return sizeof(T) == 4 ? (v == 0 ? 1 : (v == 3 ? 3 : 2)) : (v == 1 ? 2 : (v == 3 ? 3 : 1));
+}
+template <typename T>
+__host__ __device__ constexpr int col_ct_v(int LC, int ncols_minus1, int v) {
+    const int tt = LC / col_rpt<T>(LC, v);
+    const int mb = col_minb_req<T>(v);
     int ct = 16;
-    while (ct > 1 && (ct * tt > 512 ||
-                      ct * (sm_len(LC) + 1) * (int)sizeof(cplx<T>) > 200 * 1024 ||
+    while (ct > 1 && (ct * tt > col_max_threads<T>(v) ||
+                      (ct * sm_len(LC) + ct) * (int)sizeof(cplx<T>) * mb > kSmemPerSM ||
                       ct > ncols_minus1))
         ct >>= 1;
     return ct;
@@ -63,23 +117,40 @@ template <typename T>
 __host__ __device__ constexpr int col_smem(int LC, int ct) {
     return (ct * sm_len(LC) + ct) * (int)sizeof(cplx<T>);
 }
+template <typename T>
+__host__ __device__ constexpr int col_threads(int LC, int ncm1, int v) {
+    return col_ct_v<T>(LC, ncm1, v) * (LC / col_rpt<T>(LC, v));
+}
+template <typename T>
+__host__ __device__ constexpr int col_minb(int LC, int ncm1, int v) {
+    int mb = col_minb_req<T>(v);
+    const int sm = col_smem<T>(LC, col_ct_v<T>(LC, ncm1, v));
+    while (mb > 1 && mb * sm > kSmemPerSM) --mb;
+    while (mb > 1 && mb * col_threads<T>(LC, ncm1, v) > 2048) --mb;
+    return mb;
+}
+// does a column of length LC fit one CTA at all (variant-independent floor)
+template <typename T>
+__host__ __device__ constexpr bool col_fits(int LC) {
+    return col_smem<T>(LC, 1) <= kSmemPerSM;
+}
 
 // ---- row forward ---------------------------------------------------------------
 // Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1])
 // Store: void operator()(int row, int k, cplx<T> X), k in [0, LR]
 //        static constexpr bool kFinish; when true, every thread calls
 //        finish(double* scratch) after a __syncthreads() at the end
-template <typename T, int LR, bool PAD, class Load, class Store>
-__global__ void __launch_bounds__(row_rb<T>(LR) * (LR / rpt_for(LR)), 1)
+template <typename T, int LR, bool PAD, int V, class Load, class Store>
+__global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
                const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
     if (gate && *gate) return;
-    constexpr int RPT = rpt_for(LR);
+    constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
     const int r = threadIdx.x / TT, t = threadIdx.x % TT;
-    const int row = blockIdx.x * row_rb<T>(LR) + r;
+    const int row = blockIdx.x * row_rb_v<T>(LR, V) + r;
     const bool valid = row < nrows;
     const int off = r * sm_len(LR + 1);
     cplx<T> v[RPT];
@@ -119,17 +190,17 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 // Load:  cplx<T> operator()(int row, int k), k in [0, LR]
 // Store: void operator()(int row, int n, cplx<T> z) -> (x[2n], x[2n+1]);
 //        static constexpr bool kFinish (see row_fwd_kernel)
-template <typename T, int LR, bool PAD, class Load, class Store>
-__global__ void __launch_bounds__(row_rb<T>(LR) * (LR / rpt_for(LR)), 1)
+template <typename T, int LR, bool PAD, int V, class Load, class Store>
+__global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
                const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
     if (gate && *gate) return;
-    constexpr int RPT = rpt_for(LR);
+    constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
     const int r = threadIdx.x / TT, t = threadIdx.x % TT;
-    const int row = blockIdx.x * row_rb<T>(LR) + r;
+    const int row = blockIdx.x * row_rb_v<T>(LR, V) + r;
     const bool valid = row < nrows;
     const int off = r * sm_len(LR + 1);
     for (int k = t; k <= LR; k += TT)
@@ -161,12 +232,13 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 
 // ---- column forward * multiplier * inverse --------------------------------------
 // Mult: cplx<T> operator()(cplx<T> X, int kx, int ky)
-template <typename T, int LC, int CT, bool PAD, class Mult>
-__global__ void __launch_bounds__(CT * (LC / rpt_for(LC)), 1)
+template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
+__global__ void __launch_bounds__(col_threads<T>(LC, NCM1, V), col_minb<T>(LC, NCM1, V))
 col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
            const cplx<T>* __restrict__ tw_lc, const int* __restrict__ gate) {
     if (gate && *gate) return;
-    constexpr int RPT = rpt_for(LC);
+    constexpr int RPT = col_rpt<T>(LC, V);
+    constexpr int CT = col_ct_v<T>(LC, NCM1, V);
     constexpr int TT = LC / RPT;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);

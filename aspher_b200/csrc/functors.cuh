@@ -1,0 +1,77 @@
+// Load / store / multiplier functors of the row and column kernels shared by
+// the operators (operators.cu) and the allocation-free entry point.
+#pragma once
+
+#include "fft_kernels.cuh"
+
+namespace asb {
+
+template <typename T>
+struct LoadRealRows {  // z[n] = (x[row*pitch + 2n], x[row*pitch + 2n + 1])
+    const T* x;
+    int pitch;
+    __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
+        return *reinterpret_cast<const cplx<T>*>(x + (size_t)row * pitch + 2 * n);
+    }
+};
+
+template <typename T>
+struct StoreRealRows {
+    T* y;
+    int pitch;
+    static constexpr bool kFinish = false;
+    __device__ __forceinline__ void operator()(int row, int n, cplx<T> z) const {
+        *reinterpret_cast<cplx<T>*>(y + (size_t)row * pitch + 2 * n) = z;
+    }
+    __device__ void finish(double*) const {}
+};
+
+template <typename T>
+struct StoreTiled {
+    cplx<T>* base;
+    int nrows, ct;
+    static constexpr bool kFinish = false;
+    __device__ __forceinline__ void operator()(int row, int k, cplx<T> X) const {
+        base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)] = X;
+    }
+    __device__ void finish(double*) const {}
+};
+
+template <typename T>
+struct LoadTiled {
+    const cplx<T>* base;
+    int nrows, ct;
+    __device__ __forceinline__ cplx<T> operator()(int row, int k) const {
+        return base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)];
+    }
+};
+
+// Free-space multiplier: real Kh, even-folded in ky, tiled like the spectrum
+// with ct columns per tile and Ns+1 rows.
+template <typename T>
+struct KhMult {
+    const T* kh;
+    int nk;  // Ns + 1 rows
+    int M;   // padded length 2 Ns
+    int ct;
+    __device__ __forceinline__ cplx<T> operator()(cplx<T> X, int kx, int ky) const {
+        const int kf = ky <= (M >> 1) ? ky : M - ky;
+        const T w = __ldg(&kh[(size_t)(kx / ct) * nk * ct + (size_t)kf * ct + (kx % ct)]);
+        return cscale(X, w);
+    }
+};
+
+// Periodic multiplier: scale / |m| in FP64, cast to T (periodic_fft_operator.cpp:34-47).
+template <typename T>
+struct PeriodicMult {
+    double scale;
+    int Ns;
+    __device__ __forceinline__ cplx<T> operator()(cplx<T> X, int kx, int ky) const {
+        const int my = ky < (Ns + 1) / 2 ? ky : ky - Ns;
+        const double m2 = (double)kx * kx + (double)my * my;
+        const T w = m2 > 0.0 ? (T)(scale / sqrt(m2)) : T(0);
+        return cscale(X, w);
+    }
+};
+
+}  // namespace asb

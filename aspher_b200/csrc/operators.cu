@@ -15,6 +15,7 @@
 // scale/|m| (scale = L/(pi E* Ns^2), m = (kx, signed ky), zero mode 0) is
 // evaluated in FP64 inside the column kernel and cast to the working type.
 #include "fft_kernels.cuh"
+#include "functors.cuh"
 #include "ops.hpp"
 #include "pcg.hpp"
 #include "reduce.cuh"
@@ -22,7 +23,9 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace asb {
@@ -130,74 +133,6 @@ __global__ void love_table_kernel(double* __restrict__ tab, int Ns, double h, do
 // ----------------------------------------------------------------------------
 // functors
 // ----------------------------------------------------------------------------
-template <typename T>
-struct LoadRealRows {  // z[n] = (x[row*pitch + 2n], x[row*pitch + 2n + 1])
-    const T* x;
-    int pitch;
-    __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
-        return *reinterpret_cast<const cplx<T>*>(x + (size_t)row * pitch + 2 * n);
-    }
-};
-
-template <typename T>
-struct StoreRealRows {
-    T* y;
-    int pitch;
-    static constexpr bool kFinish = false;
-    __device__ __forceinline__ void operator()(int row, int n, cplx<T> z) const {
-        *reinterpret_cast<cplx<T>*>(y + (size_t)row * pitch + 2 * n) = z;
-    }
-    __device__ void finish(double*) const {}
-};
-
-template <typename T>
-struct StoreTiled {
-    cplx<T>* base;
-    int nrows, ct;
-    static constexpr bool kFinish = false;
-    __device__ __forceinline__ void operator()(int row, int k, cplx<T> X) const {
-        base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)] = X;
-    }
-    __device__ void finish(double*) const {}
-};
-
-template <typename T>
-struct LoadTiled {
-    const cplx<T>* base;
-    int nrows, ct;
-    __device__ __forceinline__ cplx<T> operator()(int row, int k) const {
-        return base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)];
-    }
-};
-
-// Free-space multiplier: real Kh, even-folded in ky, tiled like the spectrum
-// with ct columns per tile and Ns+1 rows.
-template <typename T>
-struct KhMult {
-    const T* kh;
-    int nk;  // Ns + 1 rows
-    int M;   // padded length 2 Ns
-    int ct;
-    __device__ __forceinline__ cplx<T> operator()(cplx<T> X, int kx, int ky) const {
-        const int kf = ky <= (M >> 1) ? ky : M - ky;
-        const T w = __ldg(&kh[(size_t)(kx / ct) * nk * ct + (size_t)kf * ct + (kx % ct)]);
-        return cscale(X, w);
-    }
-};
-
-// Periodic multiplier: scale / |m| in FP64, cast to T (periodic_fft_operator.cpp:34-47).
-template <typename T>
-struct PeriodicMult {
-    double scale;
-    int Ns;
-    __device__ __forceinline__ cplx<T> operator()(cplx<T> X, int kx, int ky) const {
-        const int my = ky < (Ns + 1) / 2 ? ky : ky - Ns;
-        const double m2 = (double)kx * kx + (double)my * my;
-        const T w = m2 > 0.0 ? (T)(scale / sqrt(m2)) : T(0);
-        return cscale(X, w);
-    }
-};
-
 // ---- Kh build functors (FP64) -------------------------------------------------
 // Embedded table K(iy, ix) = T(|d(iy)|, |d(ix)|), d(i) = i (i < Ns) or i - M,
 // with row/column Ns zero (fft_operator.cpp:31-44), generated on the fly.
@@ -216,7 +151,7 @@ struct LoadEmbedded {
 };
 
 // Pass A: Yt[k][row] = Re X (real by evenness in ix); tracks max|Im|, max|Re|.
-// Pass B: Kh[(row/ct)][k][row%ct] = Re X / M^2 in FP64 and FP32 copies.
+// Pass B: canonical Kh[k * nk + row] = Re X / M^2 (ky = k, kx = row).
 struct StoreRealTracked {
     double* out_t;  // pass A: transposed real, (Ns+1) x M
     int M;
@@ -231,9 +166,7 @@ struct StoreRealTracked {
         if (out_t) {
             out_t[(size_t)k * M + row] = X.x;
         } else {
-            const double v = X.x * norm;
-            kh_d[(size_t)(row / ct_d) * nk * ct_d + (size_t)k * ct_d + (row % ct_d)] = v;
-            kh_f[(size_t)(row / ct_f) * nk * ct_f + (size_t)k * ct_f + (row % ct_f)] = (float)v;
+            kh_d[(size_t)k * nk + row] = X.x * norm;
         }
         mi = fmax(mi, fabs(X.y));
         mr = fmax(mr, fabs(X.x));
@@ -253,43 +186,145 @@ struct StoreRealTracked {
 // in mutable members initialised to zero by the host copy.
 
 // ----------------------------------------------------------------------------
+// launch-variant selection: a default per (backend, precision, Ns), overridden
+// process-wide by the autotuner (Operator::autotune) or set per operator
+// ----------------------------------------------------------------------------
+namespace {
+std::mutex g_tuned_mu;
+std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
+}  // namespace
+
+void default_variants(int kind, int dbl, int Ns, int& rv, int& cv) {
+    (void)kind;
+    (void)dbl;
+    (void)Ns;
+    rv = 0;
+    cv = 0;
+}
+
+void tuned_variants(int kind, int dbl, int Ns, int& rv, int& cv) {
+    {
+        std::lock_guard<std::mutex> lk(g_tuned_mu);
+        auto it = g_tuned.find(std::make_tuple(kind, dbl, Ns));
+        if (it != g_tuned.end()) {
+            rv = it->second.first;
+            cv = it->second.second;
+            return;
+        }
+    }
+    default_variants(kind, dbl, Ns, rv, cv);
+}
+
+void record_tuned(int kind, int dbl, int Ns, int rv, int cv) {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[std::make_tuple(kind, dbl, Ns)] = std::make_pair(rv, cv);
+}
+
+// ----------------------------------------------------------------------------
+// launchers (variant V compile-time; small sizes collapse to variant 0)
+// ----------------------------------------------------------------------------
+__host__ __device__ constexpr int vclamp(int L, int V) { return L >= 128 ? V : 0; }
+
+namespace {
+std::mutex g_attr_mu;
+std::map<std::pair<const void*, int>, int> g_attr_done;
+}  // namespace
+
+// max dynamic shared memory + max-shared carveout, once per kernel per device
+void fft_attrs(const void* func, int bytes) {
+    int dev = 0;
+    ASB_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    auto key = std::make_pair(func, dev);
+    auto it = g_attr_done.find(key);
+    if (it != g_attr_done.end() && it->second >= bytes) return;
+    if (bytes > 48 * 1024)
+        ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  cudaSharedmemCarveoutMaxShared));
+    g_attr_done[key] = bytes;
+}
+
+template <typename T, int LR, bool PAD, int V, class Load, class Store>
+void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
+    auto k = row_fwd_kernel<T, LR, PAD, V, Load, Store>;
+    fft_attrs((const void*)k, sm);
+    k<<<(nrows + rb - 1) / rb, thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
+}
+template <typename T, int LR, bool PAD, int V, class Load, class Store>
+void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
+    auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
+    fft_attrs((const void*)k, sm);
+    k<<<(nrows + rb - 1) / rb, thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
+}
+template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
+void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate) {
+    constexpr int ct = col_ct_v<T>(LC, NCM1, V), thr = col_threads<T>(LC, NCM1, V);
+    constexpr int sm = col_smem<T>(LC, ct);
+    auto k = col_kernel<T, LC, NCM1, PAD, V, Mult>;
+    fft_attrs((const void*)k, sm);
+    k<<<NCM1 / ct + 1, thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
+}
+
+#define ASB_V_SWITCH(VV, L, ...)                                                   \
+    switch (VV) {                                                                  \
+        case 0: { constexpr int V = vclamp(L, 0); __VA_ARGS__; } break;            \
+        case 1: { constexpr int V = vclamp(L, 1); __VA_ARGS__; } break;            \
+        case 2: { constexpr int V = vclamp(L, 2); __VA_ARGS__; } break;            \
+        case 3: { constexpr int V = vclamp(L, 3); __VA_ARGS__; } break;            \
+        default: throw Error(-1, "FFT launch variant out of range");              \
+    }
+
+template <typename T, int LR, bool PAD, class Load, class Store>
+void row_fwd_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+    ASB_V_SWITCH(v, LR, (launch_row_fwd<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate)));
+}
+template <typename T, int LR, bool PAD, class Load, class Store>
+void row_inv_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+    ASB_V_SWITCH(v, LR, (launch_row_inv<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate)));
+}
+template <typename T, int LC, int NCM1, bool PAD, class Mult>
+void col_v(int v, cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate) {
+    ASB_V_SWITCH(v, LC, (launch_col<T, LC, NCM1, PAD, V, Mult>(spec, nrows, m, s, gate)));
+}
+// tile width of column variant v (runtime view of the constexpr table)
+template <typename T, int LC, int NCM1>
+int col_ct_rt(int v) {
+    int ct = 1;
+    ASB_V_SWITCH(v, LC, ct = col_ct_v<T>(LC, NCM1, V));
+    return ct;
+}
+
+// ----------------------------------------------------------------------------
 // per-size implementation
 // ----------------------------------------------------------------------------
 template <typename T, int NS>
 struct FreeImpl {
     static constexpr int LR = NS, LC = 2 * NS;
-    static constexpr int CT = col_ct<T>(LC, LR);
-    static constexpr int NT = LR / CT + 1;  // tiles over Ns+1 columns
-
-    static size_t spec_elems() { return (size_t)NT * NS * CT; }
+    static constexpr bool kFits = col_fits<T>(LC);
+    // spectrum sized for the widest tile (16 columns)
+    static size_t spec_elems() { return (size_t)(LR + 16) * NS; }
+    static int ct(int cv) { return col_ct_rt<T, LC, LR>(cv); }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
                        const int* gate) {
-        if constexpr (col_smem<T>(LC, CT) > 227 * 1024) {
+        if constexpr (!kFits) {
             throw Error(-1, "free-space FP64 apply at grid_size 8192 is not supported (the "
                             "16384-point FP64 column does not fit one CTA's shared memory); "
                             "use FP32 or grid_size <= 4096");
         } else {
-        constexpr int rb = row_rb<T>(LR);
-        constexpr int rthreads = rb * (LR / rpt_for(LR));
-        constexpr int rsm = row_smem<T>(LR);
-        const int rgrid = (NS + rb - 1) / rb;
-        auto kf = row_fwd_kernel<T, LR, true, LoadRealRows<T>, StoreTiled<T>>;
-        smem_optin((const void*)kf, rsm);
-        kf<<<rgrid, rthreads, rsm, s>>>(LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, CT}, NS,
-                                        tw<T>(LR), tw<T>(2 * LR), gate);
-        constexpr int cthreads = CT * (LC / rpt_for(LC));
-        constexpr int csm = col_smem<T>(LC, CT);
-        auto kc = col_kernel<T, LC, CT, true, KhMult<T>>;
-        smem_optin((const void*)kc, csm);
-        const T* kh = sizeof(T) == 8 ? (const T*)op.kh_d : (const T*)op.kh_f;
-        kc<<<NT, cthreads, csm, s>>>(spec, NS, KhMult<T>{kh, NS + 1, LC, CT}, tw<T>(LC), gate);
-        auto ki = row_inv_kernel<T, LR, true, LoadTiled<T>, StoreRealRows<T>>;
-        smem_optin((const void*)ki, rsm);
-        ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT}, StoreRealRows<T>{y, NS}, NS,
-                                        tw<T>(LR), tw<T>(2 * LR), gate);
-        count_launches(3);
-        ASB_CUDA(cudaGetLastError());
+            const int dbl = sizeof(T) == 8;
+            const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
+            const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
+            row_fwd_v<T, LR, true>(rv, LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, c}, NS, s,
+                                   gate);
+            col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate);
+            row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c}, StoreRealRows<T>{y, NS}, NS, s,
+                                   gate);
+            count_launches(3);
+            ASB_CUDA(cudaGetLastError());
         }
     }
 };
@@ -297,41 +332,28 @@ struct FreeImpl {
 template <typename T, int NS>
 struct PeriodicImpl {
     static constexpr int LR = NS / 2, LC = NS;
-    static constexpr int CT = col_ct<T>(LC, LR);
-    static constexpr int NT = LR / CT + 1;
+    static size_t spec_elems() { return (size_t)(LR + 16) * NS; }
+    static int ct(int cv) { return col_ct_rt<T, LC, LR>(cv); }
 
-    static size_t spec_elems() { return (size_t)NT * NS * CT; }
-
-    template <class Mult>
-    static void apply_mult(const T* x, T* y, cplx<T>* spec, Mult mult, cudaStream_t s,
-                           const int* gate) {
-        constexpr int rb = row_rb<T>(LR);
-        constexpr int rthreads = rb * (LR / rpt_for(LR));
-        constexpr int rsm = row_smem<T>(LR);
-        const int rgrid = (NS + rb - 1) / rb;
-        auto kf = row_fwd_kernel<T, LR, false, LoadRealRows<T>, StoreTiled<T>>;
-        smem_optin((const void*)kf, rsm);
-        kf<<<rgrid, rthreads, rsm, s>>>(LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, CT}, NS,
-                                        tw<T>(LR), tw<T>(2 * LR), gate);
-        constexpr int cthreads = CT * (LC / rpt_for(LC));
-        constexpr int csm = col_smem<T>(LC, CT);
-        auto kc = col_kernel<T, LC, CT, false, Mult>;
-        smem_optin((const void*)kc, csm);
-        kc<<<NT, cthreads, csm, s>>>(spec, NS, mult, tw<T>(LC), gate);
-        auto ki = row_inv_kernel<T, LR, false, LoadTiled<T>, StoreRealRows<T>>;
-        smem_optin((const void*)ki, rsm);
-        ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT}, StoreRealRows<T>{y, NS}, NS,
-                                        tw<T>(LR), tw<T>(2 * LR), gate);
+    template <class Load, class Mult, class Store>
+    static void apply(int rv, int cv, Load ld, Mult mult, Store st, cplx<T>* spec, cudaStream_t s,
+                      const int* gate) {
+        const int c = ct(cv);
+        StoreTiled<T> sto{spec, NS, c};
+        row_fwd_v<T, LR, false>(rv, ld, sto, NS, s, gate);
+        col_v<T, LC, LR, false>(cv, spec, NS, mult, s, gate);
+        row_inv_v<T, LR, false>(rv, LoadTiled<T>{spec, NS, c}, st, NS, s, gate);
         count_launches(3);
         ASB_CUDA(cudaGetLastError());
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
                        const int* gate) {
-        apply_mult(x, y, spec, PeriodicMult<T>{op.scale, NS}, s, gate);
+        const int dbl = sizeof(T) == 8;
+        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS}, PeriodicMult<T>{op.scale, NS},
+              StoreRealRows<T>{y, NS}, spec, s, gate);
     }
 };
-
 
 // ----------------------------------------------------------------------------
 // full-grid |k| preconditioner (reference: src/fourier_precond.cpp:12-116)
@@ -395,70 +417,38 @@ struct FourierImpl {
     using PI = PeriodicImpl<T, NS>;
     static void run(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
                     double* part, cudaStream_t s, const int* gate) {
-        constexpr int LR = PI::LR, LC = PI::LC, CT = PI::CT, NT = PI::NT;
         cplx<T>* spec = static_cast<cplx<T>*>(op.spectrum(sizeof(T) == 8, s));
-        constexpr int rb = row_rb<T>(LR);
-        constexpr int rthreads = rb * (LR / rpt_for(LR));
-        constexpr int rsm = row_smem<T>(LR);
-        const int rgrid = (NS + rb - 1) / rb;
-        auto kf = row_fwd_kernel<T, LR, false, LoadMaskCentered<T>, StoreTiled<T>>;
-        smem_optin((const void*)kf, rsm);
-        kf<<<rgrid, rthreads, rsm, s>>>(LoadMaskCentered<T>{g, mask, st, NS},
-                                        StoreTiled<T>{spec, NS, CT}, NS, tw<T>(LR),
-                                        tw<T>(2 * LR), gate);
-        constexpr int cthreads = CT * (LC / rpt_for(LC));
-        constexpr int csm = col_smem<T>(LC, CT);
-        auto kc = col_kernel<T, LC, CT, false, FourierMult<T>>;
-        smem_optin((const void*)kc, csm);
+        int rv = 0, cv = 0;
+        tuned_variants(OP_PERIODIC, sizeof(T) == 8, NS, rv, cv);
         const float norm = 1.0f / ((float)NS * (float)NS);
-        kc<<<NT, cthreads, csm, s>>>(spec, NS, FourierMult<T>{NS, norm}, tw<T>(LC), gate);
-        auto ki = row_inv_kernel<T, LR, false, LoadTiled<T>, StoreGather<T>>;
-        smem_optin((const void*)ki, rsm);
-        ki<<<rgrid, rthreads, rsm, s>>>(LoadTiled<T>{spec, NS, CT},
-                                        StoreGather<T>{z, mask, NS, st, part, 0.0}, NS, tw<T>(LR),
-                                        tw<T>(2 * LR), gate);
-        count_launches(3);
-        ASB_CUDA(cudaGetLastError());
+        PI::apply(rv, cv, LoadMaskCentered<T>{g, mask, st, NS}, FourierMult<T>{NS, norm},
+                  StoreGather<T>{z, mask, NS, st, part, 0.0}, spec, s, gate);
     }
 };
 
-// Kh build for the free-space operator of size NS (FP64).
+// Kh build for the free-space operator of size NS (FP64): canonical real
+// spectrum kh_canon[ky * (Ns+1) + kx], ky, kx in [0, Ns].
 template <int NS>
 struct KhBuild {
     static void run(Operator& op) {
         constexpr int LR = NS, M = 2 * NS;
-        constexpr int CTD = FreeImpl<double, NS>::CT, CTF = FreeImpl<float, NS>::CT;
-        op.ct_d = CTD;
-        op.ct_f = CTF;
-        const size_t nkd = (size_t)(NS / CTD + 1) * (NS + 1) * CTD;
-        const size_t nkf = (size_t)(NS / CTF + 1) * (NS + 1) * CTF;
-        ASB_CUDA(cudaMalloc(&op.kh_d, nkd * sizeof(double)));
-        ASB_CUDA(cudaMalloc(&op.kh_f, nkf * sizeof(float)));
-        ASB_CUDA(cudaMemset(op.kh_d, 0, nkd * sizeof(double)));
-        ASB_CUDA(cudaMemset(op.kh_f, 0, nkf * sizeof(float)));
+        const size_t nk = (size_t)(NS + 1) * (NS + 1);
+        ASB_CUDA(cudaMalloc(&op.kh_canon, nk * sizeof(double)));
         double* yt = nullptr;
         unsigned long long* mx = nullptr;
         ASB_CUDA(cudaMalloc(&yt, (size_t)(NS + 1) * M * sizeof(double)));
         ASB_CUDA(cudaMalloc(&mx, 4 * sizeof(unsigned long long)));
         ASB_CUDA(cudaMemset(mx, 0, 4 * sizeof(unsigned long long)));
-        constexpr int rb = row_rb<double>(LR);
-        constexpr int rthreads = rb * (LR / rpt_for(LR));
-        constexpr int rsm = row_smem<double>(LR);
-        auto k = row_fwd_kernel<double, LR, false, LoadEmbedded, StoreRealTracked>;
-        smem_optin((const void*)k, rsm);
-        // pass A over the M rows of the embedded table
+        // pass A over the M rows of the embedded table (real by evenness in ix)
         StoreRealTracked sa{yt, M, nullptr, nullptr, 0, 0, 0, 0.0, mx, 0.0, 0.0};
-        k<<<(M + rb - 1) / rb, rthreads, rsm>>>(LoadEmbedded{op.table, NS, M}, sa, M,
-                                                tw<double>(LR), tw<double>(2 * LR), nullptr);
+        launch_row_fwd<double, LR, false, 0>(LoadEmbedded{op.table, NS, M}, sa, M, nullptr,
+                                             nullptr);
         ASB_CUDA(cudaGetLastError());
         // pass B over the Ns+1 rows of the transposed buffer (each M long)
-        auto k2 = row_fwd_kernel<double, LR, false, LoadRealRows<double>, StoreRealTracked>;
-        smem_optin((const void*)k2, rsm);
-        StoreRealTracked sb{nullptr, M, op.kh_d, op.kh_f, NS + 1, CTD, CTF,
+        StoreRealTracked sb{nullptr, M, op.kh_canon, nullptr, NS + 1, 0, 0,
                             1.0 / ((double)M * (double)M), mx + 2, 0.0, 0.0};
-        k2<<<(NS + 1 + rb - 1) / rb, rthreads, rsm>>>(LoadRealRows<double>{yt, M}, sb, NS + 1,
-                                                      tw<double>(LR), tw<double>(2 * LR),
-                                                      nullptr);
+        launch_row_fwd<double, LR, false, 0>(LoadRealRows<double>{yt, M}, sb, NS + 1, nullptr,
+                                             nullptr);
         ASB_CUDA(cudaGetLastError());
         unsigned long long h[4];
         ASB_CUDA(cudaMemcpy(h, mx, sizeof(h), cudaMemcpyDeviceToHost));
@@ -475,6 +465,20 @@ struct KhBuild {
                             "part; wrap-around embedding is broken");
     }
 };
+
+// tiled copy of the canonical Kh for column tile width ct (both precisions)
+__global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
+                            double* __restrict__ kd, int ct_f, float* __restrict__ kf) {
+    const int nk = Ns + 1;
+    const long n = (long)nk * nk;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        const int ky = (int)(i / nk), kx = (int)(i % nk);
+        const double v = canon[i];
+        if (kd) kd[(size_t)(kx / ct_d) * nk * ct_d + (size_t)ky * ct_d + (kx % ct_d)] = v;
+        if (kf) kf[(size_t)(kx / ct_f) * nk * ct_f + (size_t)ky * ct_f + (kx % ct_f)] = (float)v;
+    }
+}
 
 // ----------------------------------------------------------------------------
 // size dispatch
@@ -505,14 +509,25 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
     (void)tw_table(false, 2);
     if (kind == OP_PERIODIC) {
         scale = L / (M_PI * E_star * (double)Ns * Ns);
-        return;
+    } else {
+        // Love table on the device (boussinesq_kernel.cpp:97-106)
+        ASB_CUDA(cudaMalloc(&table, (size_t)Ns * Ns * sizeof(double)));
+        const double h = L / Ns;
+        love_table_kernel<<<592, 256>>>(table, Ns, h, 1.0 / (M_PI * E_star));
+        ASB_CUDA(cudaGetLastError());
+        ASB_SIZE_SWITCH(Ns, KhBuild<NS>::run(*this));
+        const size_t nt = (size_t)(Ns + 16) * (Ns + 1);  // widest tiling
+        ASB_CUDA(cudaMalloc(&kh_d, nt * sizeof(double)));
+        ASB_CUDA(cudaMalloc(&kh_f, nt * sizeof(float)));
+        ASB_CUDA(cudaMemset(kh_d, 0, nt * sizeof(double)));
+        ASB_CUDA(cudaMemset(kh_f, 0, nt * sizeof(float)));
     }
-    // Love table on the device (boussinesq_kernel.cpp:97-106)
-    ASB_CUDA(cudaMalloc(&table, (size_t)Ns * Ns * sizeof(double)));
-    const double h = L / Ns;
-    love_table_kernel<<<592, 256>>>(table, Ns, h, 1.0 / (M_PI * E_star));
-    ASB_CUDA(cudaGetLastError());
-    ASB_SIZE_SWITCH(Ns, KhBuild<NS>::run(*this));
+    for (int dbl = 0; dbl < 2; ++dbl) {
+        int rv = 0, cv = 0;
+        tuned_variants(kind, dbl, Ns, rv, cv);
+        ct[dbl] = 0;  // force the first tiling
+        set_variants(dbl != 0, rv, cv);
+    }
     ASB_CUDA(cudaDeviceSynchronize());
 }
 
@@ -521,9 +536,98 @@ Operator::~Operator() {
     ctx_d.reset();
     cudaFree(kh_d);
     cudaFree(kh_f);
+    cudaFree(kh_canon);
     cudaFree(spec_d);
     cudaFree(spec_f);
     cudaFree(table);
+}
+
+int Operator::col_tile(bool dbl, int cv) const {
+    int c = 1;
+    if (kind == OP_FFT) {
+        if (dbl) { ASB_SIZE_SWITCH(Ns, c = FreeImpl<double, NS>::ct(cv)); }
+        else { ASB_SIZE_SWITCH(Ns, c = FreeImpl<float, NS>::ct(cv)); }
+    } else {
+        if (dbl) { ASB_SIZE_SWITCH(Ns, c = PeriodicImpl<double, NS>::ct(cv)); }
+        else { ASB_SIZE_SWITCH(Ns, c = PeriodicImpl<float, NS>::ct(cv)); }
+    }
+    return c;
+}
+
+void Operator::set_variants(bool dbl, int rv, int cv) {
+    if (rv < 0 || rv >= kVariants || cv < 0 || cv >= kVariants)
+        throw Error(-1, "launch variant out of range");
+    const int c = col_tile(dbl, cv);
+    if (kind == OP_FFT && c != ct[dbl]) {
+        // re-tile Kh of this precision for the new column tile width
+        k_retile_kh<<<1184, 256>>>(Ns, kh_canon, c, dbl ? kh_d : nullptr, c,
+                                   dbl ? nullptr : kh_f);
+        ASB_CUDA(cudaGetLastError());
+        ASB_CUDA(cudaDeviceSynchronize());
+    }
+    rowv[dbl] = rv;
+    colv[dbl] = cv;
+    ct[dbl] = c;
+    if (ctx_f) ctx_f->invalidate();
+    if (ctx_d) ctx_d->invalidate();
+}
+
+double Operator::autotune(bool dbl, int reps, int& best_rv, int& best_cv) {
+    const long N = (long)Ns * Ns;
+    const size_t eb = dbl ? 8 : 4;
+    void *x = nullptr, *y = nullptr, *flush = nullptr;
+    const size_t fb = 256u << 20;  // > 126 MB L2
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    ASB_CUDA(cudaMalloc(&x, N * eb));
+    ASB_CUDA(cudaMalloc(&y, N * eb));
+    ASB_CUDA(cudaMalloc(&flush, fb));
+    ASB_CUDA(cudaMemset(x, 0, N * eb));
+    ASB_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    ASB_CUDA(cudaEventCreate(&e0));
+    ASB_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    best_rv = rowv[dbl];
+    best_cv = colv[dbl];
+    try {
+        for (int cv = 0; cv < kVariants; ++cv) {
+            for (int rv = 0; rv < kVariants; ++rv) {
+                set_variants(dbl, rv, cv);
+                matvec(dbl, x, y, s, nullptr);
+                matvec(dbl, x, y, s, nullptr);
+                double tot = 0.0;
+                for (int r = 0; r < reps; ++r) {
+                    ASB_CUDA(cudaMemsetAsync(flush, r & 0xff, fb, s));
+                    ASB_CUDA(cudaEventRecord(e0, s));
+                    matvec(dbl, x, y, s, nullptr);
+                    ASB_CUDA(cudaEventRecord(e1, s));
+                    ASB_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    ASB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    tot += ms;
+                }
+                const double mean = tot / reps;
+                if (mean < best) {
+                    best = mean;
+                    best_rv = rv;
+                    best_cv = cv;
+                }
+            }
+        }
+    } catch (...) {
+        cudaFree(x); cudaFree(y); cudaFree(flush);
+        cudaStreamDestroy(s); cudaEventDestroy(e0); cudaEventDestroy(e1);
+        throw;
+    }
+    cudaFree(x);
+    cudaFree(y);
+    cudaFree(flush);
+    cudaStreamDestroy(s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    set_variants(dbl, best_rv, best_cv);
+    record_tuned(kind, dbl, Ns, best_rv, best_cv);
+    return best;
 }
 
 size_t Operator::spectrum_bytes(bool dbl) const {
@@ -553,9 +657,10 @@ void* Operator::spectrum(bool dbl, cudaStream_t) {
 size_t Operator::resident_bytes() const {
     size_t n = spec_d_bytes + spec_f_bytes;
     if (kind == OP_FFT) {
-        n += (size_t)(Ns / ct_d + 1) * (Ns + 1) * ct_d * sizeof(double);
-        n += (size_t)(Ns / ct_f + 1) * (Ns + 1) * ct_f * sizeof(float);
-        n += (size_t)Ns * Ns * sizeof(double);
+        const size_t nt = (size_t)(Ns + 16) * (Ns + 1);
+        n += nt * (sizeof(double) + sizeof(float));
+        n += (size_t)(Ns + 1) * (Ns + 1) * sizeof(double);  // canonical Kh
+        n += (size_t)Ns * Ns * sizeof(double);              // Love table
     }
     return n;
 }

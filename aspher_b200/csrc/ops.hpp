@@ -36,6 +36,8 @@ long long launch_count();
 struct SolverCtxBase {
     virtual ~SolverCtxBase() = default;
     virtual size_t bytes() const = 0;
+    // drop captured graphs (they bake in launch variants and layouts)
+    virtual void invalidate() = 0;
 };
 
 // exp(-2 pi i k / L), k < L, for every power of two L <= kMaxTw, on the
@@ -52,6 +54,10 @@ enum OpKind : int { OP_FFT = 0, OP_PERIODIC = 1 };
 
 bool is_pow2(long v);
 
+// launch variants chosen for (kind, precision, Ns): the autotuned entry of
+// this process if any, else the built-in default
+void tuned_variants(int kind, int dbl, int Ns, int& rv, int& cv);
+
 // Opt into >48 KB dynamic shared memory once per kernel per device.
 void smem_optin(const void* func, int bytes);
 
@@ -60,12 +66,16 @@ struct Operator {
     int Ns = 0;
     double L = 1.0, E_star = 1.0;
     int device = 0;
-    // free space: tiled real half spectrum Kh (1/M^2 folded in), rows
-    // ky in [0, Ns] only (Kh is even in ky), tile widths per precision
+    // free space: real half spectrum Kh (1/M^2 folded in), rows ky in [0, Ns]
+    // only (Kh is even in ky): canonical [ky][kx] FP64, plus FP64 / FP32
+    // copies tiled for the active column tile width of each precision
+    double* kh_canon = nullptr;
     double* kh_d = nullptr;
     float* kh_f = nullptr;
-    int ct_d = 1, ct_f = 1;
     double max_im_ratio = 0.0;
+    // launch variants per precision [F32, F64] and the column tile width
+    // (half-spectrum layout) they imply
+    int rowv[2] = {0, 0}, colv[2] = {0, 0}, ct[2] = {0, 0};
     // periodic: symbol scale L / (pi E* Ns^2)
     double scale = 0.0;
     // scratch half spectra per precision (lazily sized)
@@ -86,6 +96,11 @@ struct Operator {
     // gate: optional device int; when nonzero at kernel start, kernels return.
     void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr);
     void* spectrum(bool dbl, cudaStream_t s);
+    int col_tile(bool dbl, int cv) const;
+    void set_variants(bool dbl, int rv, int cv);
+    // times every (row, column) variant pair (reps applies each, L2 flushed),
+    // keeps and records (process-wide) the fastest; returns its mean ms
+    double autotune(bool dbl, int reps, int& best_rv, int& best_cv);
     size_t spectrum_bytes(bool dbl) const;
     size_t resident_bytes() const;
 };

@@ -660,8 +660,16 @@ struct SolverCtx : SolverCtxBase {
     int grid = 1;
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
+    // Private non-blocking stream: the loop graph is captured and launched
+    // here (the legacy NULL stream a caller may pass cannot be captured);
+    // entry and exit are fenced to the caller's stream with events.
+    cudaStream_t ws = nullptr;
+    cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 
     explicit SolverCtx(Operator& o) : op(o) {
+        ASB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
+        ASB_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
+        ASB_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
         N = (long)o.Ns * o.Ns;
         const size_t b = (size_t)N * sizeof(T);
         T** vecs[] = {&p, &t, &u, &g, &gprev, &z, &r, &best, &g0c};
@@ -680,6 +688,9 @@ struct SolverCtx : SolverCtxBase {
         void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd};
         for (void* v : all)
             if (v) cudaFree(v);
+        if (ev_in) cudaEventDestroy(ev_in);
+        if (ev_out) cudaEventDestroy(ev_out);
+        if (ws) cudaStreamDestroy(ws);
     }
     size_t bytes() const override {
         return (9 * sizeof(T) + 1) * (size_t)N + hist_cap * sizeof(double) +
@@ -692,6 +703,7 @@ struct SolverCtx : SolverCtxBase {
         hist_cap = cap;
         drop_graph();  // the graph bakes the history pointer
     }
+    void invalidate() override { drop_graph(); }
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -790,7 +802,16 @@ struct Solver {
     const T* g0 = nullptr;
     long long mv_host = 0;
 
-    Solver(SolverCtx<T>& ctx, cudaStream_t st) : c(ctx), s(st) {}
+    cudaStream_t caller;
+    // All work runs on the context's private stream, ordered after the
+    // caller's pending work and before the caller's later work.
+    Solver(SolverCtx<T>& ctx, cudaStream_t st) : c(ctx), s(ctx.ws), caller(st) {
+        ASB_CUDA(cudaEventRecord(c.ev_in, caller));
+        ASB_CUDA(cudaStreamWaitEvent(s, c.ev_in, 0));
+    }
+    ~Solver() {
+        if (cudaEventRecord(c.ev_out, s) == cudaSuccess) cudaStreamWaitEvent(caller, c.ev_out, 0);
+    }
 
     void read_state() {
         ASB_CUDA(cudaMemcpyAsync(&h, c.st, sizeof(PkState), cudaMemcpyDeviceToHost, s));
@@ -1192,12 +1213,15 @@ void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, dou
     SolverCtx<float>& cf = get_ctx<float>(op);
     const long N = (long)op.Ns * op.Ns;
     // FP64 statistics of the gap (validation before any apply)
-    Solver<double> probe(cd, s);
-    probe.P.N = N;
-    probe.P.Ns = op.Ns;
-    ASB_CUDA(cudaMemcpyAsync(cd.Pd, &probe.P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
     double mm[3];
-    probe.reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
+    {
+        Solver<double> probe(cd, s);
+        probe.P.N = N;
+        probe.P.Ns = op.Ns;
+        ASB_CUDA(cudaMemcpyAsync(cd.Pd, &probe.P, sizeof(PkParams), cudaMemcpyHostToDevice,
+                                 probe.s));
+        probe.reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
+    }
     if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
     const double datum = o.datum_mode == ASPHER_DATUM_AUTOMATIC ? mm[0] + 0.5 * (mm[1] - mm[0])
                                                                  : o.datum;

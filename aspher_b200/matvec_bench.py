@@ -18,10 +18,12 @@ import torch
 from .api import Operator
 
 
-def run(backend, ns, dtype, iters, warmup=3, flush=True):
+def run(backend, ns, dtype, iters, warmup=3, flush=True, variants=None, op=None):
     dt = torch.float32 if dtype == "f32" else torch.float64
     b = 4 if dtype == "f32" else 8
-    op = Operator(backend, ns)
+    op = op if op is not None else Operator(backend, ns)
+    if variants is not None:
+        op.set_variants(variants[0], variants[1], dt)
     N = ns * ns
     xs = [torch.randn(N, dtype=dt, device="cuda") for _ in range(2)]
     y = torch.empty(N, dtype=dt, device="cuda")
@@ -42,7 +44,9 @@ def run(backend, ns, dtype, iters, warmup=3, flush=True):
         ts.append(a.elapsed_time(c) / 1e3)
     model = (12 if backend == "fft" else 6) * b * N
     t = statistics.mean(ts)
-    return dict(backend=backend, ns=ns, dtype=dtype, iters=iters, ms_mean=t * 1e3,
+    rv, cv, ct = op.variants(dt)
+    return dict(backend=backend, ns=ns, dtype=dtype, iters=iters, variants=[rv, cv, ct],
+                ms_mean=t * 1e3,
                 ms_min=min(ts) * 1e3, alg_bytes=model, gbs=model / t / 1e9,
                 gbs_best=model / min(ts) / 1e9)
 
@@ -56,7 +60,27 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--sweep", action="store_true",
                     help="all backends x dtypes x Ns in {512..8192}")
+    ap.add_argument("--variants", action="store_true",
+                    help="with --sweep: time every (row, column) launch-variant pair")
     a = ap.parse_args()
+    if a.sweep and a.variants:
+        for backend in ("fft", "periodic"):
+            for dtype in ("f32", "f64"):
+                for ns in (256, 512, 1024, 2048, 4096, 8192):
+                    if backend == "fft" and dtype == "f64" and ns == 8192:
+                        continue
+                    op = Operator(backend, ns)
+                    best = None
+                    for cv in range(4):
+                        for rv in range(4):
+                            r = run(backend, ns, dtype, a.iters, a.warmup, variants=(rv, cv),
+                                    op=op)
+                            print(json.dumps(r), flush=True)
+                            if best is None or r["ms_mean"] < best["ms_mean"]:
+                                best = r
+                    print(json.dumps(dict(best=best)), flush=True)
+                    del op
+        return
     if a.sweep:
         for backend in ("fft", "periodic"):
             for dtype in ("f32", "f64"):

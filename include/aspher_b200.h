@@ -97,6 +97,22 @@ typedef struct {
 } aspher_op_info;
 int aspher_op_get_info(const aspher_op* op, aspher_op_info* info);
 
+/* Launch variants of the three FFT passes (row variant: registers per thread
+ * and rows per CTA of the two row passes; column variant: registers per
+ * thread, columns per CTA and CTAs per SM of the column pass).  Variants
+ * 0..3; the half-spectrum layout follows the column variant's tile width.
+ * No reference counterpart (the reference's FFT engine has no launch shape). */
+int aspher_op_set_variants(aspher_op* op, int dtype, int row_variant, int col_variant);
+int aspher_op_get_variants(const aspher_op* op, int dtype, int* row_variant, int* col_variant,
+                           int* col_tile);
+/* Autotuner: times every variant pair (reps applies each, L2 flushed between
+ * applies) on this operator, keeps the fastest and records it for every
+ * operator of the same backend / precision / grid_size created later in the
+ * process.  Synchronous; allocates temporary device buffers.  No reference
+ * counterpart. */
+int aspher_op_autotune(aspher_op* op, int dtype, int reps, int* row_variant, int* col_variant,
+                       double* best_ms);
+
 /* Copies the Ns*Ns FP64 Love table T[dy*Ns+dx] (BoussinesqKernel::table_,
  * src/boussinesq_kernel.cpp:97-106) to host memory.  FFT backend only. */
 int aspher_op_love_table(const aspher_op* op, double* host_out);
