@@ -108,6 +108,8 @@ SIGNATURES = {
                                      C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.POINTER(Result), C.POINTER(Result),
                                      C.c_void_p]),
+    "aspher_periodic_matvec_noalloc": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_nested_opts_default": (None, [C.POINTER(NestedOpts)]),
     "aspher_solve_nested": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
                                       C.c_double, C.POINTER(NestedOpts), C.c_void_p,

@@ -223,6 +223,20 @@ int aspher_solve_mixed(aspher_op* op, const aspher_solve_opts* opts, const doubl
                        double* pressure_dev, double* displacement_dev, double* gap_dev,
                        aspher_result* res, aspher_result* res_float, void* stream);
 
+/* Allocation-free doubly periodic apply, y = S x (no counterpart in the
+ * reference).  For callers that cannot allocate device memory: real-time
+ * loops that must not block in the allocator, and applications whose own
+ * allocator owns all GPU memory.  Same
+ * result as aspher_op_matvec on a PERIODIC operator of the same grid_size,
+ * domain_size and E_star, without an operator handle: the scratch is a
+ * static 8.65 MB device array (held by every GPU that loads the library)
+ * and grid_size must be a power of two in [16, 1024]; larger sizes return
+ * ASPHER_EINVAL.  The first call on a device sets it up (make it before any
+ * stream capture).  All calls share the scratch: calls that overlap on the
+ * GPU race.  x_dev and y_dev must not alias.  Async on `stream`. */
+int aspher_periodic_matvec_noalloc(int grid_size, double domain_size, double E_star, int dtype,
+                                   const void* x_dev, void* y_dev, void* stream);
+
 /* ---- nested-grid driver ---------------------------------------------------- */
 /* NestedParams, reference include/nested_solve.hpp:11-119 (the fields that
  * apply to the fft / periodic backends; the H2 q / leaf_side are kept for
