@@ -78,6 +78,12 @@ class Stage(C.Structure):
                 ("penetration_error", C.c_double), ("precond_dropped", C.c_int)]
 
 
+class AdjointInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("iterations", C.c_int), ("contact_count", C.c_int),
+                ("reserved", C.c_int), ("residual", C.c_double), ("mu", C.c_double),
+                ("time", C.c_double)]
+
+
 # exported symbol -> (restype, argtypes)
 SIGNATURES = {
     "aspher_abi_version": (C.c_int, []),
@@ -108,6 +114,17 @@ SIGNATURES = {
                                      C.c_void_p, C.c_double, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.POINTER(Result), C.POINTER(Result),
                                      C.c_void_p]),
+    "aspher_solve_batch": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_int,
+                                     C.POINTER(C.c_void_p), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                     C.POINTER(Result), C.c_void_p]),
+    "aspher_solve_batch_mixed": (C.c_int, [C.c_void_p, C.POINTER(SolveOpts), C.c_int,
+                                           C.POINTER(C.c_void_p), C.POINTER(C.c_double),
+                                           C.c_double, C.c_int, C.POINTER(C.c_void_p),
+                                           C.POINTER(Result), C.POINTER(Result), C.c_void_p]),
+    "aspher_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
+                                 C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double),
+                                 C.POINTER(AdjointInfo), C.c_void_p]),
     "aspher_periodic_matvec_noalloc": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_int,
                                                  C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_nested_opts_default": (None, [C.POINTER(NestedOpts)]),

@@ -296,6 +296,85 @@ def solve_device(op, g0, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precon
     return ContactResult(res, op.Ns, p_out, u_out, g_out, h)
 
 
+def _opts(tol, max_iter, use_pr, precond, keep_best, dtype, precond_radius=2, light=True):
+    o = L.SolveOpts()
+    L.lib().aspher_solve_opts_default(C.byref(o))
+    o.tol = float(tol)
+    o.max_iter = int(max_iter)
+    o.use_pr = int(bool(use_pr))
+    o.light = int(bool(light))
+    o.keep_best = int(bool(keep_best))
+    if precond not in L.PRECOND:
+        raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
+    o.precond = L.PRECOND[precond]
+    o.precond_radius = int(precond_radius)
+    o.dtype = L.F64 if dtype == torch.float64 else L.F32
+    return o
+
+
+def solve_device_batch(op, g0s, p_nominals, tol=1e-8, max_iter=5000, use_pr=True,
+                       precond="none", p_inits=None, dtype=torch.float64, keep_best=True,
+                       pressures_out=None):
+    """Batched solve_contact_impl<Real>: the problems g0s[b] (device fields
+    of ``dtype``) with loads p_nominals[b] on one operator, solved together
+    in one loop graph.  Returns one ContactResult per problem (pressure on
+    the device; no displacement / gap fields)."""
+    B = len(g0s)
+    if B < 1 or len(p_nominals) != B:
+        raise ValueError("solve_device_batch: need one p_nominal per gap")
+    N = op.N
+    g0s = [g.to(dtype).contiguous().reshape(-1) for g in g0s]
+    for g in g0s:
+        if g.numel() != N:
+            raise ValueError("array has %d entries, expected %d" % (g.numel(), N))
+    pis = None
+    if p_inits is not None:
+        pis = [None if p is None else p.to(dtype).contiguous().reshape(-1) for p in p_inits]
+    outs = pressures_out or [torch.empty(N, dtype=torch.float64, device=g0s[0].device)
+                             for _ in range(B)]
+    o = _opts(tol, max_iter, use_pr, precond, keep_best, dtype)
+    arr = C.c_void_p * B
+    res = (L.Result * B)()
+    L.check(L.lib().aspher_solve_batch(
+        op.handle, C.byref(o), B, arr(*[g.data_ptr() for g in g0s]),
+        (C.c_double * B)(*[float(p) for p in p_nominals]),
+        arr(*[0 if p is None else p.data_ptr() for p in pis]) if pis else None,
+        arr(*[p.data_ptr() for p in outs]), res, _stream()))
+    return [ContactResult(res[b], op.Ns, outs[b]) for b in range(B)]
+
+
+def solve_device_batch_mixed(op, g0s, p_nominals, tol=1e-6, float_tol=None, polish=True,
+                             max_iter=5000, use_pr=True, precond="fourier", keep_best=True,
+                             pressures_out=None, polish_tol=None):
+    """Batched FP32 stage (FP64 reductions) + FP64 polish: the batched form
+    of solve_device_mixed (same float_tol / polish_tol meaning).  g0s: FP64
+    device fields.  Returns (final results, FP32-stage results)."""
+    B = len(g0s)
+    if B < 1 or len(p_nominals) != B:
+        raise ValueError("solve_device_batch_mixed: need one p_nominal per gap")
+    if polish_tol is not None and not (0.0 < polish_tol <= tol):
+        raise ValueError("polish_tol must be in (0, tol]")
+    N = op.N
+    g0s = [g.to(torch.float64).contiguous().reshape(-1) for g in g0s]
+    for g in g0s:
+        if g.numel() != N:
+            raise ValueError("array has %d entries, expected %d" % (g.numel(), N))
+    outs = pressures_out or [torch.empty(N, dtype=torch.float64, device=g0s[0].device)
+                             for _ in range(B)]
+    o = _opts(tol if polish_tol is None or not polish else polish_tol, max_iter, use_pr,
+              precond, keep_best, torch.float64)
+    o.requested_tol = float(tol)
+    arr = C.c_void_p * B
+    res, resf = (L.Result * B)(), (L.Result * B)()
+    L.check(L.lib().aspher_solve_batch_mixed(
+        op.handle, C.byref(o), B, arr(*[g.data_ptr() for g in g0s]),
+        (C.c_double * B)(*[float(p) for p in p_nominals]),
+        C.c_double(float(tol if float_tol is None else float_tol)), int(bool(polish)),
+        arr(*[p.data_ptr() for p in outs]), res, resf, _stream()))
+    return ([ContactResult(res[b], op.Ns, outs[b]) for b in range(B)],
+            [ContactResult(resf[b], op.Ns, None) for b in range(B)])
+
+
 class ContactSolver:
     """``aspher.ContactSolver`` for backend='fft' / 'periodic' (bindings.cpp:805-834).
 
@@ -332,12 +411,14 @@ class ContactSolver:
         return y.cpu().numpy()
 
     def solve(self, gap, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precond="none",
-              p_init=None, *, precision="double"):
+              p_init=None, *, precision="double", float_tol=None, polish_tol=None):
         """Normal contact solve (bindings.cpp:186-234); always FP64 by default.
 
         ``precision`` (keyword-only extension): 'double' (reference),
         'float' (FP32 vectors and transforms, FP64 reductions) or
-        'float_then_double' (FP32 at tol, then an FP64 polish).
+        'float_then_double' (FP32 to float_tol (default tol), then an FP64
+        polish that certifies polish_tol (default tol); see
+        solve_device_mixed).
         """
         N = self.Ns * self.Ns
         if precond not in ("none", "", "fourier", "fourier-fft"):
@@ -350,9 +431,9 @@ class ContactSolver:
             r = solve_device(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
                              torch.float64)
         elif precision in ("float", "float_then_double"):
-            r, _ = solve_device_mixed(self.op, g0d, p_nominal, tol, None,
+            r, _ = solve_device_mixed(self.op, g0d, p_nominal, tol, float_tol,
                                       precision == "float_then_double", max_iter, use_pr,
-                                      precond, p0)
+                                      precond, p0, polish_tol=polish_tol)
         else:
             raise ValueError("precision must be 'double', 'float' or 'float_then_double'")
         r.wall = time.perf_counter() - t0
@@ -374,10 +455,15 @@ class ContactSolver:
 def solve_device_mixed(op, g0, p_nominal, tol=1e-6, float_tol=None, polish=True,
                        max_iter=5000, use_pr=True, precond="fourier", p_init=None,
                        light=False, keep_best=None, g_ref=0.0, datum_mode="automatic",
-                       datum=0.0, precond_radius=2, pressure_out=None):
+                       datum=0.0, precond_radius=2, pressure_out=None, polish_tol=None):
     """FP32 PK solve with FP64 reductions to ``float_tol`` (default: tol),
     then (polish) an FP64 PK solve warm-started from it that certifies
-    ``tol``: the reference's float_then_double staging on one grid.
+    ``polish_tol`` (default: tol; must be <= tol): the reference's
+    float_then_double staging on one grid.  A polish_tol below tol buys
+    pressure accuracy the certificate does not measure: FP32 rounding leaves
+    a high-frequency pressure error (1e-5 .. 3e-5 relative at Ns=2048) that
+    barely moves the Frank-Wolfe gap, and a few FP64 iterations past tol
+    remove it.  ``requested_tol`` of the result stays tol.
     g0 / p_init: FP64 device tensors.  Returns (final, float_stage)."""
     N = op.N
     if g0.numel() != N:
@@ -390,9 +476,12 @@ def solve_device_mixed(op, g0, p_nominal, tol=1e-6, float_tol=None, polish=True,
         p_init = p_init.to(device=dev, dtype=torch.float64).contiguous().reshape(-1)
         if p_init.numel() != N:
             raise ValueError("solve_contact: p_init size mismatch")
+    if polish_tol is not None and not (0.0 < polish_tol <= tol):
+        raise ValueError("polish_tol must be in (0, tol]")
     o = L.SolveOpts()
     L.lib().aspher_solve_opts_default(C.byref(o))
-    o.tol = float(tol)
+    o.tol = float(tol if polish_tol is None or not polish else polish_tol)
+    o.requested_tol = float(tol)
     o.max_iter = int(max_iter)
     o.use_pr = int(bool(use_pr))
     o.light = int(bool(light))

@@ -103,6 +103,79 @@ int aspher_solve_mixed(aspher_op* op, const aspher_solve_opts* opts, const doubl
     ASB_API_END
 }
 
+int aspher_solve_batch(aspher_op* op, const aspher_solve_opts* opts, int batch,
+                       const void* const* g0_devs, const double* p_bars,
+                       const void* const* p_init_devs, double* const* pressure_devs,
+                       aspher_result* res, void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !opts || !g0_devs || !p_bars || !pressure_devs || !res)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch: NULL argument");
+    if (batch < 1) throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch: batch must be >= 1");
+    for (int b = 0; b < batch; ++b) {
+        if (!g0_devs[b] || !pressure_devs[b])
+            throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch: NULL field");
+        const uintptr_t a = (uintptr_t)g0_devs[b] | (uintptr_t)pressure_devs[b] |
+                            (uintptr_t)(p_init_devs ? p_init_devs[b] : nullptr);
+        if (a % 16) throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch: buffers must be 16-byte aligned");
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (opts->dtype == ASPHER_F64)
+        asb::solve_batch_impl<double>(*op->impl, *opts, batch, g0_devs, p_bars, p_init_devs,
+                                      pressure_devs, res, s);
+    else if (opts->dtype == ASPHER_F32)
+        asb::solve_batch_impl<float>(*op->impl, *opts, batch, g0_devs, p_bars, p_init_devs,
+                                     pressure_devs, res, s);
+    else
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch: dtype must be F32 or F64");
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_solve_batch_mixed(aspher_op* op, const aspher_solve_opts* opts, int batch,
+                             const double* const* g0_devs, const double* p_bars, double float_tol,
+                             int polish, double* const* pressure_devs, aspher_result* res,
+                             aspher_result* res_float, void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !opts || !g0_devs || !p_bars || !pressure_devs || !res)
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch_mixed: NULL argument");
+    if (batch < 1) throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch_mixed: batch must be >= 1");
+    if (!(float_tol > 0.0))
+        throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch_mixed: float_tol must be positive");
+    for (int b = 0; b < batch; ++b) {
+        if (!g0_devs[b] || !pressure_devs[b])
+            throw asb::Error(ASPHER_EINVAL, "aspher_solve_batch_mixed: NULL field");
+        if (((uintptr_t)g0_devs[b] | (uintptr_t)pressure_devs[b]) % 16)
+            throw asb::Error(ASPHER_EINVAL,
+                             "aspher_solve_batch_mixed: buffers must be 16-byte aligned");
+    }
+    asb::solve_batch_mixed(*op->impl, *opts, batch, g0_devs, p_bars, float_tol, polish,
+                           pressure_devs, res, res_float, static_cast<cudaStream_t>(stream));
+    return ASPHER_OK;
+    ASB_API_END
+}
+
+int aspher_adjoint(aspher_op* op, int dtype, const double* p_dev, const double* w_dev,
+                   double tol, int max_iter, int precond, int precond_radius,
+                   double* grad_g0_dev, double* grad_pbar, aspher_adjoint_info* info,
+                   void* stream) {
+    ASB_API_BEGIN
+    if (!op || !op->impl || !p_dev || !w_dev || !grad_g0_dev)
+        throw asb::Error(ASPHER_EINVAL, "aspher_adjoint: NULL argument");
+    if (((uintptr_t)p_dev | (uintptr_t)w_dev | (uintptr_t)grad_g0_dev) % 16)
+        throw asb::Error(ASPHER_EINVAL, "aspher_adjoint: buffers must be 16-byte aligned");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (dtype == ASPHER_F64)
+        asb::adjoint_impl<double>(*op->impl, p_dev, w_dev, tol, max_iter, precond,
+                                  precond_radius, grad_g0_dev, grad_pbar, info, s);
+    else if (dtype == ASPHER_F32)
+        asb::adjoint_impl<float>(*op->impl, p_dev, w_dev, tol, max_iter, precond,
+                                 precond_radius, grad_g0_dev, grad_pbar, info, s);
+    else
+        throw asb::Error(ASPHER_EINVAL, "aspher_adjoint: dtype must be F32 or F64");
+    return ASPHER_OK;
+    ASB_API_END
+}
+
 int aspher_precond_apply(aspher_op* op, int precond, int radius, int dtype, const void* g_dev,
                          const uint8_t* contact_dev, void* z_dev, void* stream) {
     ASB_API_BEGIN

@@ -128,25 +128,27 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
             for (int r = 0; r < R; ++r) a[r] = v[q + r * Q];
             if constexpr (SPAN > 1) {
                 // w^r for r = 1..R-1 from the loaded powers w, w^2, w^4, w^8
-                // (products at most three deep), applied as each is formed
+                // (products at most three deep), applied as each is formed.
+                // w^(2^e) = exp(-2 pi i jm / (SPAN R / 2^e)) is entry jm of the
+                // length-(SPAN R / 2^e) table, so consecutive threads (jm)
+                // read consecutive entries instead of a stride of L/(SPAN R).
                 const int jm = j % SPAN;
-                constexpr int TS = L / (SPAN * R);
-                const int b = jm * TS;
-                const cplx<T> w1 = __ldg(&tw[b]);
+                const cplx<T>* __restrict__ tb = tw - L;  // tables at offset = length
+                const cplx<T> w1 = __ldg(&tb[SPAN * R + jm]);
                 a[1] = tw_apply<DIR>(a[1], w1);
                 if constexpr (R >= 4) {
-                    const cplx<T> w2 = __ldg(&tw[2 * b]);
+                    const cplx<T> w2 = __ldg(&tb[SPAN * R / 2 + jm]);
                     a[2] = tw_apply<DIR>(a[2], w2);
                     const cplx<T> w3 = cmul(w2, w1);
                     a[3] = tw_apply<DIR>(a[3], w3);
                     if constexpr (R >= 8) {
-                        const cplx<T> w4 = __ldg(&tw[4 * b]);
+                        const cplx<T> w4 = __ldg(&tb[SPAN * R / 4 + jm]);
                         a[4] = tw_apply<DIR>(a[4], w4);
                         a[5] = tw_apply<DIR>(a[5], cmul(w4, w1));
                         a[6] = tw_apply<DIR>(a[6], cmul(w4, w2));
                         a[7] = tw_apply<DIR>(a[7], cmul(w4, w3));
                         if constexpr (R >= 16) {
-                            const cplx<T> w8 = __ldg(&tw[8 * b]);
+                            const cplx<T> w8 = __ldg(&tb[SPAN * R / 8 + jm]);
                             a[8] = tw_apply<DIR>(a[8], w8);
                             a[9] = tw_apply<DIR>(a[9], cmul(w8, w1));
                             a[10] = tw_apply<DIR>(a[10], cmul(w8, w2));
@@ -182,7 +184,9 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
 
 // Length-L transform of the strided register pattern; DIR = -1 forward
 // (exp(-2 pi i jk/L)), +1 inverse, both unnormalised.  tw points at the
-// length-L table exp(-2 pi i k / L), k < L.  Every thread of the CTA must
+// length-L table exp(-2 pi i k / L), k < L, inside one array that holds the
+// table of every power-of-two length M <= L at offset M (so tw - L is the
+// array base and the stages read the shorter tables).  Every thread of the CTA must
 // call this (it contains __syncthreads), including threads whose transform
 // is a dummy.
 template <typename T, int L, int RPT, int DIR, int S>

@@ -17,6 +17,10 @@
 // so a column CTA streams one contiguous tile and a row CTA of RB rows
 // touches RB*ct contiguous elements per tile.
 //
+// Batched solves launch every kernel with gridDim.y = instances; the load /
+// store functors offset their pointers by blockIdx.y times a batch stride,
+// and instance b's spectrum is the b-th block of gridDim.x column tiles.
+//
 // Launch shapes are variants (V = 0..kVariants-1) trading registers per
 // thread (RPT elements, radix <= RPT), CTA size and CTAs per SM; the
 // operator picks one row variant and one column variant per size and
@@ -24,10 +28,15 @@
 #pragma once
 
 #include "fft_block.cuh"
+#include "pk_state.hpp"
 
 namespace asb {
 
 constexpr int kVariants = 4;
+// Batched launches (gridDim.y = instances) read instance b's gate at
+// gate[b * kGateStride]: the gates live in consecutive PkState records.
+constexpr int kGateStride = (int)(sizeof(PkState) / sizeof(int));
+static_assert(sizeof(PkState) % sizeof(int) == 0, "PkState must be a whole number of ints");
 constexpr int kSmemPerSM = 227 * 1024;
 
 template <typename T>
@@ -138,13 +147,15 @@ __host__ __device__ constexpr bool col_fits(int LC) {
 // ---- row forward ---------------------------------------------------------------
 // Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1])
 // Store: void operator()(int row, int k, cplx<T> X), k in [0, LR]
-//        static constexpr bool kFinish; when true, every thread calls
-//        finish(double* scratch) after a __syncthreads() at the end
+//        static constexpr bool kTiled: true for the tiled half-spectrum store
+//        (then the kernel writes whole tile chunks through base / nrows / ct /
+//        bs itself); static constexpr bool kFinish: when true, every thread
+//        calls finish(double* scratch) after a __syncthreads() at the end
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 __global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
                const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
-    if (gate && *gate) return;
+    if (gate && gate[blockIdx.y * kGateStride]) return;
     constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -160,25 +171,57 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
     }
     block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
-#pragma unroll
-    for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        const int k = t + m * TT;
-        const cplx<T> zk = v[m];
-        const cplx<T> zn = sm[smaddr((LR - k) & (LR - 1), 1, off)];
-        // E = (Zk + conj Zn)/2, O = (Zk - conj Zn)/(2i), X = E + w^k O
+    // split step of the real transform: X[k] = E + w^k O with
+    // E = (Z[k] + conj Z[-k])/2, O = (Z[k] - conj Z[-k])/(2i), k in [0, LR]
+    auto split = [&](cplx<T> zk, cplx<T> zn, int k) {
         const cplx<T> A = mk<T>(zk.x + zn.x, zk.y - zn.y);
         const cplx<T> B = mk<T>(zk.x - zn.x, zk.y + zn.y);
         const cplx<T> O = mk<T>(B.y * T(0.5), -B.x * T(0.5));
         const cplx<T> w = __ldg(&tw_2lr[k]);
-        const cplx<T> X = cadd(cscale(A, T(0.5)), cmul(w, O));
-        if (valid) st(row, k, X);
-    }
-    if (t == 0 && valid) {
+        return cadd(cscale(A, T(0.5)), cmul(w, O));
+    };
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
+    __syncthreads();
+    if constexpr (Store::kTiled) {
+        // each output reads Z[k] and Z[-k] from shared memory and goes straight
+        // to its tile chunk (RB rows x ct columns, contiguous in HBM)
+        constexpr int RB = row_rb_v<T>(LR, V);
+        const int row0 = blockIdx.x * RB;
+        const int nr = nrows - row0 < RB ? nrows - row0 : RB;
+        const int ct = st.ct;
+        const int chunk = nr * ct;
+        const int ntiles = LR / ct + 1;
+        const int lct = __ffs(ct) - 1;  // ct is a power of two
+        const bool full = nr == RB;
+        const int lchunk = lct + ilog2c(RB);
+        cplx<T>* base = st.base + blockIdx.y * st.bs + (size_t)row0 * ct;
+        for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
+            const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+            const int rr = e >> lct, c = e & (ct - 1);
+            const int k = j * ct + c;
+            if (k > LR) continue;
+            const int o = rr * sm_len(LR + 1);
+            const cplx<T> zk = sm[smaddr(k & (LR - 1), 1, o)];
+            cplx<T> X;
+            if (k == LR) {
+                X = mk<T>(zk.x - zk.y, T(0));  // zk = Z[0]
+            } else {
+                X = split(zk, sm[smaddr((LR - k) & (LR - 1), 1, o)], k);
+            }
+            base[(size_t)j * st.nrows * ct + e] = X;
+        }
+    } else {
         const cplx<T> z0 = v[0];
-        st(row, LR, mk<T>(z0.x - z0.y, T(0)));
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            const int k = t + m * TT;
+            v[m] = split(v[m], sm[smaddr((LR - k) & (LR - 1), 1, off)], k);
+        }
+#pragma unroll
+        for (int m = 0; m < RPT; ++m)
+            if (valid) st(row, t + m * TT, v[m]);
+        if (t == 0 && valid) st(row, LR, mk<T>(z0.x - z0.y, T(0)));
     }
     if constexpr (Store::kFinish) {
         __syncthreads();
@@ -187,14 +230,15 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 }
 
 // ---- row inverse ----------------------------------------------------------------
-// Load:  cplx<T> operator()(int row, int k), k in [0, LR]
+// Load:  cplx<T> operator()(int row, int k), k in [0, LR]; kTiled as for the
+//        forward store (whole tile chunks into shared memory)
 // Store: void operator()(int row, int n, cplx<T> z) -> (x[2n], x[2n+1]);
 //        static constexpr bool kFinish (see row_fwd_kernel)
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 __global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
                const cplx<T>* __restrict__ tw_2lr, const int* __restrict__ gate) {
-    if (gate && *gate) return;
+    if (gate && gate[blockIdx.y * kGateStride]) return;
     constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -203,8 +247,28 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
     const int row = blockIdx.x * row_rb_v<T>(LR, V) + r;
     const bool valid = row < nrows;
     const int off = r * sm_len(LR + 1);
-    for (int k = t; k <= LR; k += TT)
-        sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
+    if constexpr (Load::kTiled) {
+        // whole tile chunks (RB rows x ct columns, contiguous) per access
+        constexpr int RB = row_rb_v<T>(LR, V);
+        const int row0 = blockIdx.x * RB;
+        const int nr = nrows - row0 < RB ? nrows - row0 : RB;
+        const int ct = ld.ct;
+        const int chunk = nr * ct;
+        const int ntiles = LR / ct + 1;
+        const int lct = __ffs(ct) - 1;  // ct is a power of two
+        const bool full = nr == RB;
+        const int lchunk = lct + ilog2c(RB);
+        const cplx<T>* base = ld.base + blockIdx.y * ld.bs + (size_t)row0 * ct;
+        for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
+            const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+            const int rr = e >> lct, c = e & (ct - 1);
+            const int k = j * ct + c;
+            if (k <= LR) sm[smaddr(k, 1, rr * sm_len(LR + 1))] = base[(size_t)j * ld.nrows * ct + e];
+        }
+    } else {
+        for (int k = t; k <= LR; k += TT)
+            sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
+    }
     __syncthreads();
     cplx<T> v[RPT];
 #pragma unroll
@@ -236,7 +300,7 @@ template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
 __global__ void __launch_bounds__(col_threads<T>(LC, NCM1, V), col_minb<T>(LC, NCM1, V))
 col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
            const cplx<T>* __restrict__ tw_lc, const int* __restrict__ gate) {
-    if (gate && *gate) return;
+    if (gate && gate[blockIdx.y * kGateStride]) return;
     constexpr int RPT = col_rpt<T>(LC, V);
     constexpr int CT = col_ct_v<T>(LC, NCM1, V);
     constexpr int TT = LC / RPT;
@@ -244,7 +308,8 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
     const int c = threadIdx.x % CT, t = threadIdx.x / CT;
     const int tile = blockIdx.x;
-    cplx<T>* base = spec + (size_t)tile * nrows * CT;
+    // instance blockIdx.y owns gridDim.x contiguous tiles
+    cplx<T>* base = spec + ((size_t)blockIdx.y * gridDim.x + tile) * nrows * CT;
     cplx<T> v[RPT];
 #pragma unroll
     for (int m = 0; m < RPT; ++m) {

@@ -6,12 +6,17 @@
 
 namespace asb {
 
+// Every functor offsets by blockIdx.y * bs (elements): instance blockIdx.y
+// of a batched launch (bs = 0 or gridDim.y = 1 for a single field).
 template <typename T>
 struct LoadRealRows {  // z[n] = (x[row*pitch + 2n], x[row*pitch + 2n + 1])
     const T* x;
     int pitch;
+    long bs;
+    static constexpr bool kTiled = false;
     __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
-        return *reinterpret_cast<const cplx<T>*>(x + (size_t)row * pitch + 2 * n);
+        return *reinterpret_cast<const cplx<T>*>(x + blockIdx.y * bs + (size_t)row * pitch +
+                                                  2 * n);
     }
 };
 
@@ -19,9 +24,11 @@ template <typename T>
 struct StoreRealRows {
     T* y;
     int pitch;
+    long bs;
     static constexpr bool kFinish = false;
+    static constexpr bool kTiled = false;
     __device__ __forceinline__ void operator()(int row, int n, cplx<T> z) const {
-        *reinterpret_cast<cplx<T>*>(y + (size_t)row * pitch + 2 * n) = z;
+        *reinterpret_cast<cplx<T>*>(y + blockIdx.y * bs + (size_t)row * pitch + 2 * n) = z;
     }
     __device__ void finish(double*) const {}
 };
@@ -30,9 +37,11 @@ template <typename T>
 struct StoreTiled {
     cplx<T>* base;
     int nrows, ct;
+    long bs;
     static constexpr bool kFinish = false;
+    static constexpr bool kTiled = true;  // row kernels store whole tile chunks
     __device__ __forceinline__ void operator()(int row, int k, cplx<T> X) const {
-        base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)] = X;
+        base[blockIdx.y * bs + (size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)] = X;
     }
     __device__ void finish(double*) const {}
 };
@@ -41,8 +50,11 @@ template <typename T>
 struct LoadTiled {
     const cplx<T>* base;
     int nrows, ct;
+    long bs;
+    static constexpr bool kTiled = true;  // row kernels load whole tile chunks
     __device__ __forceinline__ cplx<T> operator()(int row, int k) const {
-        return base[(size_t)(k / ct) * nrows * ct + (size_t)row * ct + (k % ct)];
+        return base[blockIdx.y * bs + (size_t)(k / ct) * nrows * ct + (size_t)row * ct +
+                    (k % ct)];
     }
 };
 

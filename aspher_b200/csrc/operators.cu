@@ -18,6 +18,7 @@
 #include "functors.cuh"
 #include "ops.hpp"
 #include "pcg.hpp"
+#include "pk_fused.cuh"
 #include "reduce.cuh"
 
 #include <atomic>
@@ -137,6 +138,7 @@ __global__ void love_table_kernel(double* __restrict__ tab, int Ns, double h, do
 // Embedded table K(iy, ix) = T(|d(iy)|, |d(ix)|), d(i) = i (i < Ns) or i - M,
 // with row/column Ns zero (fft_operator.cpp:31-44), generated on the fly.
 struct LoadEmbedded {
+    static constexpr bool kTiled = false;
     const double* tab;
     int Ns, M;
     __device__ __forceinline__ double at(int iy, int ix) const {
@@ -161,6 +163,7 @@ struct StoreRealTracked {
     double norm;
     unsigned long long* maxbits;  // [0] = max|Im|, [1] = max|Re| (as bit patterns)
     static constexpr bool kFinish = true;
+    static constexpr bool kTiled = false;
     mutable double mi, mr;
     __device__ __forceinline__ void operator()(int row, int k, double2 X) const {
         if (out_t) {
@@ -194,12 +197,27 @@ std::mutex g_tuned_mu;
 std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
 }  // namespace
 
+// Fastest (row, column) variant pairs measured on B200 with
+// `python -m aspher_b200.matvec_bench --sweep --variants` (L2 flushed
+// between applies); sizes not listed use variant 0.
 void default_variants(int kind, int dbl, int Ns, int& rv, int& cv) {
-    (void)kind;
-    (void)dbl;
-    (void)Ns;
+    static const int table[][5] = {
+        // kind, dbl, Ns, row variant, column variant
+        {0, 0, 256, 2, 3},  {0, 0, 512, 2, 1},  {0, 0, 1024, 2, 1}, {0, 0, 2048, 3, 0},
+        {0, 0, 4096, 2, 0}, {0, 0, 8192, 1, 2}, {0, 1, 256, 2, 1},  {0, 1, 512, 2, 1},
+        {0, 1, 1024, 0, 0}, {0, 1, 2048, 2, 0}, {0, 1, 4096, 0, 0}, {1, 0, 256, 3, 3},
+        {1, 0, 512, 2, 3},  {1, 0, 1024, 2, 2}, {1, 0, 2048, 2, 1}, {1, 0, 4096, 3, 0},
+        {1, 0, 8192, 2, 1}, {1, 1, 256, 1, 1},  {1, 1, 512, 1, 1},  {1, 1, 1024, 2, 1},
+        {1, 1, 2048, 2, 0}, {1, 1, 4096, 2, 0}, {1, 1, 8192, 0, 0},
+    };
     rv = 0;
     cv = 0;
+    for (const auto& e : table)
+        if (e[0] == kind && e[1] == dbl && e[2] == Ns) {
+            rv = e[3];
+            cv = e[4];
+            return;
+        }
 }
 
 void tuned_variants(int kind, int dbl, int Ns, int& rv, int& cv) {
@@ -245,27 +263,30 @@ void fft_attrs(const void* func, int bytes) {
     g_attr_done[key] = bytes;
 }
 
+// B > 1: gridDim.y = B instances (functors / gates / spectrum per instance)
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
-void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
     constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
     auto k = row_fwd_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    k<<<(nrows + rb - 1) / rb, thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
+    k<<<dim3((nrows + rb - 1) / rb, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR),
+                                                      gate);
 }
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
-void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
+void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
     constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
     auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    k<<<(nrows + rb - 1) / rb, thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
+    k<<<dim3((nrows + rb - 1) / rb, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR),
+                                                      gate);
 }
 template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
-void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate) {
+void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate, int B = 1) {
     constexpr int ct = col_ct_v<T>(LC, NCM1, V), thr = col_threads<T>(LC, NCM1, V);
     constexpr int sm = col_smem<T>(LC, ct);
     auto k = col_kernel<T, LC, NCM1, PAD, V, Mult>;
     fft_attrs((const void*)k, sm);
-    k<<<NCM1 / ct + 1, thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
+    k<<<dim3(NCM1 / ct + 1, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
 }
 
 #define ASB_V_SWITCH(VV, L, ...)                                                   \
@@ -278,16 +299,16 @@ void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gat
     }
 
 template <typename T, int LR, bool PAD, class Load, class Store>
-void row_fwd_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
-    ASB_V_SWITCH(v, LR, (launch_row_fwd<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate)));
+void row_fwd_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B) {
+    ASB_V_SWITCH(v, LR, (launch_row_fwd<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
 }
 template <typename T, int LR, bool PAD, class Load, class Store>
-void row_inv_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate) {
-    ASB_V_SWITCH(v, LR, (launch_row_inv<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate)));
+void row_inv_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B) {
+    ASB_V_SWITCH(v, LR, (launch_row_inv<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
 }
 template <typename T, int LC, int NCM1, bool PAD, class Mult>
-void col_v(int v, cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate) {
-    ASB_V_SWITCH(v, LC, (launch_col<T, LC, NCM1, PAD, V, Mult>(spec, nrows, m, s, gate)));
+void col_v(int v, cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate, int B) {
+    ASB_V_SWITCH(v, LC, (launch_col<T, LC, NCM1, PAD, V, Mult>(spec, nrows, m, s, gate, B)));
 }
 // tile width of column variant v (runtime view of the constexpr table)
 template <typename T, int LC, int NCM1>
@@ -308,8 +329,10 @@ struct FreeImpl {
     static size_t spec_elems() { return (size_t)(LR + 16) * NS; }
     static int ct(int cv) { return col_ct_rt<T, LC, LR>(cv); }
 
-    static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
-                       const int* gate) {
+    // row_fwd(ld) -> col(x Kh) -> row_inv(st); ld / st see the Ns x Ns field(s)
+    template <class Load, class Store>
+    static void apply(const Operator& op, Load ld, Store st, cplx<T>* spec, cudaStream_t s,
+                      const int* gate, int B) {
         if constexpr (!kFits) {
             throw Error(-1, "free-space FP64 apply at grid_size 8192 is not supported (the "
                             "16384-point FP64 column does not fit one CTA's shared memory); "
@@ -318,14 +341,19 @@ struct FreeImpl {
             const int dbl = sizeof(T) == 8;
             const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
             const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
-            row_fwd_v<T, LR, true>(rv, LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, c}, NS, s,
-                                   gate);
-            col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate);
-            row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c}, StoreRealRows<T>{y, NS}, NS, s,
-                                   gate);
+            const long bsp = (long)(LR / c + 1) * NS * c;
+            row_fwd_v<T, LR, true>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
+            col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
+            row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
             count_launches(3);
             ASB_CUDA(cudaGetLastError());
         }
+    }
+
+    static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
+                       const int* gate, int B) {
+        const long bx = (long)NS * NS;
+        apply(op, LoadRealRows<T>{x, NS, bx}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
     }
 };
 
@@ -337,21 +365,22 @@ struct PeriodicImpl {
 
     template <class Load, class Mult, class Store>
     static void apply(int rv, int cv, Load ld, Mult mult, Store st, cplx<T>* spec, cudaStream_t s,
-                      const int* gate) {
+                      const int* gate, int B) {
         const int c = ct(cv);
-        StoreTiled<T> sto{spec, NS, c};
-        row_fwd_v<T, LR, false>(rv, ld, sto, NS, s, gate);
-        col_v<T, LC, LR, false>(cv, spec, NS, mult, s, gate);
-        row_inv_v<T, LR, false>(rv, LoadTiled<T>{spec, NS, c}, st, NS, s, gate);
+        const long bsp = (long)(LR / c + 1) * NS * c;
+        row_fwd_v<T, LR, false>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
+        col_v<T, LC, LR, false>(cv, spec, NS, mult, s, gate, B);
+        row_inv_v<T, LR, false>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
         count_launches(3);
         ASB_CUDA(cudaGetLastError());
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
-                       const int* gate) {
+                       const int* gate, int B) {
         const int dbl = sizeof(T) == 8;
-        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS}, PeriodicMult<T>{op.scale, NS},
-              StoreRealRows<T>{y, NS}, spec, s, gate);
+        const long bx = (long)NS * NS;
+        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS, bx},
+              PeriodicMult<T>{op.scale, NS}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
     }
 };
 
@@ -359,18 +388,24 @@ struct PeriodicImpl {
 // full-grid |k| preconditioner (reference: src/fourier_precond.cpp:12-116)
 // ----------------------------------------------------------------------------
 template <typename T>
-struct LoadMaskCentered {  // contact ? g - T(gsum/ng) : 0, pairwise
+struct LoadMaskCentered {  // contact ? g - T(gsum/ng) : 0, pairwise; g = v - T(alpha)
+    static constexpr bool kTiled = false;
     const T* g;
     const uint8_t* mask;
     const PkState* st;
     int pitch;
+    long bs;  // batch stride (elements); instance blockIdx.y uses st[blockIdx.y]
     __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
-        const int nc = st->nc;
-        const T gm = nc ? (T)(st->gcs / nc) : T(0);
-        const size_t i = (size_t)row * pitch + 2 * n;
+        const PkState* sb = st + blockIdx.y;
+        const int nc = sb->nc;
+        const T gm = nc ? (T)(sb->gcs / nc) : T(0);
+        // the solve loop keeps g uncentred (centred by Real(alpha) on the fly;
+        // alpha is 0 for the standalone preconditioner)
+        const T aT = (T)sb->alpha;
+        const size_t i = blockIdx.y * bs + (size_t)row * pitch + 2 * n;
         const cplx<T> v = *reinterpret_cast<const cplx<T>*>(g + i);
         const uchar2 m = *reinterpret_cast<const uchar2*>(mask + i);
-        return mk<T>(m.x ? (T)(v.x - gm) : T(0), m.y ? (T)(v.y - gm) : T(0));
+        return mk<T>(m.x ? (T)((T)(v.x - aT) - gm) : T(0), m.y ? (T)((T)(v.y - aT) - gm) : T(0));
     }
 };
 
@@ -387,15 +422,17 @@ struct FourierMult {  // |k| / Ns^2 as the reference's float table, cast to T
 
 template <typename T>
 struct StoreGather {  // z = contact ? G : 0; contact sum of G -> zmean
+    static constexpr bool kTiled = false;
     T* z;
     const uint8_t* mask;
     int pitch;
     PkState* st;
     double* part;
+    long bs;  // batch stride (elements); instance blockIdx.y uses st / part of its own
     static constexpr bool kFinish = true;
     double zs;
     __device__ __forceinline__ void operator()(int row, int n, cplx<T> v) {
-        const size_t i = (size_t)row * pitch + 2 * n;
+        const size_t i = blockIdx.y * bs + (size_t)row * pitch + 2 * n;
         const uchar2 m = *reinterpret_cast<const uchar2*>(mask + i);
         *reinterpret_cast<cplx<T>*>(z + i) = mk<T>(m.x ? v.x : T(0), m.y ? v.y : T(0));
         if (m.x) zs += (double)v.x;
@@ -404,10 +441,12 @@ struct StoreGather {  // z = contact ? G : 0; contact sum of G -> zmean
     __device__ void finish(double*) {
         double a[1] = {zs};
         const int kinds[1] = {0};
-        if (grid_reduce_last<1>(a, kinds, part, &st->counter[11]) && threadIdx.x == 0) {
-            const int nc = st->nc;
-            st->zmean = nc ? (double)(T)(a[0] / nc) : 0.0;
-            st->pc++;
+        PkState* sb = st + blockIdx.y;
+        double* pb = part + (size_t)blockIdx.y * kPartStride;
+        if (grid_reduce_last<1>(a, kinds, pb, &sb->counter[11]) && threadIdx.x == 0) {
+            const int nc = sb->nc;
+            sb->zmean = nc ? (double)(T)(a[0] / nc) : 0.0;
+            sb->pc++;
         }
     }
 };
@@ -416,13 +455,14 @@ template <typename T, int NS>
 struct FourierImpl {
     using PI = PeriodicImpl<T, NS>;
     static void run(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
-                    double* part, cudaStream_t s, const int* gate) {
-        cplx<T>* spec = static_cast<cplx<T>*>(op.spectrum(sizeof(T) == 8, s));
+                    double* part, cudaStream_t s, const int* gate, int B, void* spec_b) {
+        cplx<T>* spec = static_cast<cplx<T>*>(spec_b ? spec_b : op.spectrum(sizeof(T) == 8, s));
         int rv = 0, cv = 0;
         tuned_variants(OP_PERIODIC, sizeof(T) == 8, NS, rv, cv);
         const float norm = 1.0f / ((float)NS * (float)NS);
-        PI::apply(rv, cv, LoadMaskCentered<T>{g, mask, st, NS}, FourierMult<T>{NS, norm},
-                  StoreGather<T>{z, mask, NS, st, part, 0.0}, spec, s, gate);
+        const long bx = (long)NS * NS;
+        PI::apply(rv, cv, LoadMaskCentered<T>{g, mask, st, NS, bx}, FourierMult<T>{NS, norm},
+                  StoreGather<T>{z, mask, NS, st, part, bx, 0.0}, spec, s, gate, B);
     }
 };
 
@@ -447,7 +487,7 @@ struct KhBuild {
         // pass B over the Ns+1 rows of the transposed buffer (each M long)
         StoreRealTracked sb{nullptr, M, op.kh_canon, nullptr, NS + 1, 0, 0,
                             1.0 / ((double)M * (double)M), mx + 2, 0.0, 0.0};
-        launch_row_fwd<double, LR, false, 0>(LoadRealRows<double>{yt, M}, sb, NS + 1, nullptr,
+        launch_row_fwd<double, LR, false, 0>(LoadRealRows<double>{yt, M, 0}, sb, NS + 1, nullptr,
                                              nullptr);
         ASB_CUDA(cudaGetLastError());
         unsigned long long h[4];
@@ -665,37 +705,73 @@ size_t Operator::resident_bytes() const {
     return n;
 }
 
-void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate) {
-    void* spec = spectrum(dbl, s);
+void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate, int B,
+                      void* spec_b) {
+    void* spec = spec_b ? spec_b : spectrum(dbl, s);
     if (kind == OP_FFT) {
         if (dbl) {
             ASB_SIZE_SWITCH(Ns, FreeImpl<double, NS>::matvec(*this, (const double*)x, (double*)y,
-                                                             (double2*)spec, s, gate));
+                                                             (double2*)spec, s, gate, B));
         } else {
             ASB_SIZE_SWITCH(Ns, FreeImpl<float, NS>::matvec(*this, (const float*)x, (float*)y,
-                                                            (float2*)spec, s, gate));
+                                                            (float2*)spec, s, gate, B));
         }
     } else {
         if (dbl) {
             ASB_SIZE_SWITCH(Ns, PeriodicImpl<double, NS>::matvec(*this, (const double*)x,
                                                                  (double*)y, (double2*)spec, s,
-                                                                 gate));
+                                                                 gate, B));
         } else {
             ASB_SIZE_SWITCH(Ns, PeriodicImpl<float, NS>::matvec(*this, (const float*)x,
                                                                 (float*)y, (float2*)spec, s,
-                                                                gate));
+                                                                gate, B));
         }
     }
 }
 
 template <typename T>
 void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
-                        double* part, cudaStream_t s, const int* gate) {
-    ASB_SIZE_SWITCH(op.Ns, FourierImpl<T, NS>::run(op, g, mask, st, z, part, s, gate));
+                        double* part, cudaStream_t s, const int* gate, int B, void* spec) {
+    ASB_SIZE_SWITCH(op.Ns, FourierImpl<T, NS>::run(op, g, mask, st, z, part, s, gate, B, spec));
 }
 template void fourier_precond_pk<float>(Operator&, const float*, const uint8_t*, PkState*, float*,
-                                        double*, cudaStream_t, const int*);
+                                        double*, cudaStream_t, const int*, int, void*);
 template void fourier_precond_pk<double>(Operator&, const double*, const uint8_t*, PkState*,
-                                         double*, double*, cudaStream_t, const int*);
+                                         double*, double*, cudaStream_t, const int*, int, void*);
+
+// r = S t inside the PK loop with the direction update in the forward row
+// load and the rsum / den sums in the inverse row store (pk_fused.cuh)
+template <typename T, int NS>
+struct FusedTApply {
+    static void run(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
+                    const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
+                    const int* gate, int B, void* spec_b) {
+        cplx<T>* spec = static_cast<cplx<T>*>(spec_b ? spec_b : op.spectrum(sizeof(T) == 8, s));
+        const long bx = (long)NS * NS;
+        LoadTupd<T> ld{z, g, gprev, t, mask, p, best, st, NS, precond, bx};
+        StoreRden<T> sr{g, t, mask, st, part, NS, bx, 0.0, 0.0, 0.0, 0.0};
+        if (op.kind == OP_FFT) {
+            FreeImpl<T, NS>::apply(op, ld, sr, spec, s, gate, B);
+        } else {
+            const int dbl = sizeof(T) == 8;
+            PeriodicImpl<T, NS>::apply(op.rowv[dbl], op.colv[dbl], ld,
+                                       PeriodicMult<T>{op.scale, NS}, sr, spec, s, gate, B);
+        }
+    }
+};
+
+template <typename T>
+void pk_apply_t(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
+                const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
+                const int* gate, int B, void* spec) {
+    ASB_SIZE_SWITCH(op.Ns, FusedTApply<T, NS>::run(op, z, g, gprev, t, mask, p, best, st, part,
+                                                   precond, s, gate, B, spec));
+}
+template void pk_apply_t<float>(Operator&, const float*, const float*, float*, float*,
+                                const uint8_t*, const float*, float*, PkState*, double*, int,
+                                cudaStream_t, const int*, int, void*);
+template void pk_apply_t<double>(Operator&, const double*, const double*, double*, double*,
+                                 const uint8_t*, const double*, double*, PkState*, double*, int,
+                                 cudaStream_t, const int*, int, void*);
 
 }  // namespace asb

@@ -94,7 +94,11 @@ struct Operator {
 
     // u = S x on `stream`; x, y device arrays of Ns*Ns values of the dtype.
     // gate: optional device int; when nonzero at kernel start, kernels return.
-    void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr);
+    // Batched (B > 1): x, y hold B fields back to back, spec_b a spectrum
+    // scratch of B * spectrum_bytes(dbl), and gate[b * kGateStride] gates
+    // instance b.
+    void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr,
+                int B = 1, void* spec_b = nullptr);
     void* spectrum(bool dbl, cudaStream_t s);
     int col_tile(bool dbl, int cv) const;
     void set_variants(bool dbl, int rv, int cv);

@@ -6,25 +6,29 @@
 // double}; every reduction is accumulated in FP64 as in the reference.
 //
 // One CG iteration is the kernel sequence
-//   [apply p->u] eval1 eval2 [precond] dots tupd [apply t->r] rsum den pupd rescale
+//   [apply p->u] eval [evalpk] stencil+dots [apply t->r, tupd / rden fused] pupd rescale
 // where each pass is one HBM sweep and each reduction's scalar logic runs in
-// the last block of its pass (see pk_state.hpp).  The host enqueues several
-// iterations between synchronisations; once a pass sets `halt`, the rest are
-// no-ops.
+// the last block of its pass (see pk_state.hpp).  The loop is a CUDA graph
+// with a while node; once a pass sets `halt`, the rest of the iteration is a
+// no-op.  Every kernel serves B instances at once (gridDim.y = B, instance
+// blockIdx.y reading its own parameters, state, partials and fields).
 #include "../../include/aspher_b200.h"
 #include "ops.hpp"
 #include "pk_state.hpp"
 #include "pcg.hpp"
+#include "pk_fused.cuh"
 #include "reduce.cuh"
 
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 namespace asb {
@@ -74,23 +78,47 @@ __device__ __forceinline__ void stm4(uint8_t* m, long i4, const uint8_t (&a)[4])
 #define GRID_LOOP4(N) \
     for (long i4 = blockIdx.x * (long)blockDim.x + threadIdx.x; i4 < (N) / 4; i4 += (long)gridDim.x * blockDim.x)
 
-__device__ __forceinline__ void set_halt(PkState* st, int h) {
-    st->halt = h;
-    st->skip_mv1 = 1;
-}
 
 // ---- evaluate() -----------------------------------------------------------------
-// pass 1: v = u + (g0 - gshift) -> g; sum of v over p>0, count, min v.
+// The gap buffer holds v = u + (g0 - gshift) uncentred after k_eval; every
+// later consumer centres on the fly with gc(), which is bit-identical to the
+// reference's stored g = Real(v - Real(alpha)) (contact_solver.cpp:283-285),
+// so centring costs no pass of its own.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_eval1(const PkParams* __restrict__ Pp, PkState* st, const T* u,
-                                                       const T* g0, const T* p, T* g,
-                                                       double* part, int final_mode) {
+__device__ __forceinline__ T gc(T v, T aT) { return v - aT; }
+
+// One pass for evaluate() (contact_solver.cpp:263-303): v -> g buffer, the
+// contact mask, and the sums whose last-block logic is the certificate, the
+// convergence test and the best/stall bookkeeping (contact_solver.cpp:379-412).
+// The second-pass sums of the reference are linear in the centring, so they
+// come from first-pass sums:
+//   gcs = sum_C Real(v - a)            -> sum_C v - n_C a
+//   G   = sum p Real(Real(v - a) - m)  -> sum p v - (a + m) sum p
+// with a = Real(alpha), m = Real(gmin) (equal up to the rounding of each
+// Real difference; in FP64 to ~1e-16 relative).  pk = sum p |g| is not
+// linear; k_evalpk computes it when a history is recorded and at the end.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_eval(const PkParams* __restrict__ Pp, PkState* st,
+                                                      const T* u, const T* g0, const T* p, T* g,
+                                                      uint8_t* mask, double* part,
+                                                      int final_mode) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    u += bo_;
+    g0 += bo_;
+    p += bo_;
+    g += bo_;
+    mask += bo_;
     const PkParams& P = *Pp;
     if (!final_mode && st->halt) return;
     const T gs = (T)P.gshift;
-    double acc[3] = {0.0, 0.0, (double)INFINITY};
+    double acc[5] = {0.0, 0.0, (double)INFINITY, 0.0, 0.0};  // sum_C v, n_C, min v, pv, psum
     GRID_LOOP4(P.N) {
         T uu[4], gg0[4], pp[4], vv[4];
+        uint8_t mm[4];
         ldp4(u, i4, uu);
         ldp4(g0, i4, gg0);
         ldp4(p, i4, pp);
@@ -98,88 +126,58 @@ __global__ void __launch_bounds__(kRedThreads) k_eval1(const PkParams* __restric
         for (int j = 0; j < 4; ++j) {
             const T v = uu[j] + (gg0[j] - gs);
             vv[j] = v;
-            const double vd = (double)v;
+            const double vd = (double)v, pd = (double)pp[j];
             acc[2] = fmin(acc[2], vd);
             if (pp[j] > T(0)) { acc[0] += vd; acc[1] += 1.0; }
+            acc[3] += pd * vd;
+            acc[4] += pd;
+            mm[j] = pp[j] > T(0) ? 1 : 0;
         }
         st4(g, i4, vv);
+        stm4(mask, i4, mm);
     }
-    const int kinds[3] = {0, 0, 1};
-    if (grid_reduce_last<3>(acc, kinds, part, &st->counter[0]) && threadIdx.x == 0) {
+    const int kinds[5] = {0, 0, 1, 0, 0};
+    if (grid_reduce_last<5>(acc, kinds, part, &st->counter[0]) && threadIdx.x == 0) {
         if (!final_mode) {
             if (!st->u_fresh) st->mv++;
             st->u_fresh = 0;
             st->skip_mv1 = 0;
+            st->pk_due = 1;
         }
         const int nc = (int)acc[1];
+        const double alpha = nc ? acc[0] / nc : acc[2];
+        const double gmin = acc[2] - alpha;
+        const double aT = (double)(T)alpha, gmT = (double)(T)gmin;
+        const double gcs = acc[0] - (double)nc * aT;
         st->nc = nc;
         st->gsum = acc[0];
         st->vmin = acc[2];
-        st->alpha = nc ? acc[0] / nc : acc[2];
-        st->gmin = acc[2] - st->alpha;
-    }
-}
-
-// pass 2: centre g, certificate sums, contact mask; last block runs the
-// convergence test and the best/stall bookkeeping (contact_solver.cpp:379-412).
-template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_eval2(const PkParams* __restrict__ Pp, PkState* st, const T* p, T* g,
-                                                       uint8_t* mask, double* part, double* hist,
-                                                       int final_mode) {
-    const PkParams& P = *Pp;
-    if (!final_mode && st->halt) return;
-    const T aT = (T)st->alpha, gmT = (T)st->gmin;
-    double acc[5] = {0, 0, 0, 0, 0};  // pv, gcs, e, Gc, psum
-    GRID_LOOP4(P.N) {
-        T pp[4], gv[4];
-        uint8_t mm[4];
-        ldp4(p, i4, pp);
-        ldp4(g, i4, gv);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const double pd = (double)pp[j];
-            acc[0] += pd * (double)gv[j];
-            const T gi = gv[j] - aT;
-            gv[j] = gi;
-            const double gid = (double)gi;
-            if (pd > 0.0) acc[1] += gid;
-            acc[2] += pd * fabs(gid);
-            acc[3] += pd * (double)(gi - gmT);
-            acc[4] += pd;
-            mm[j] = pp[j] > T(0) ? 1 : 0;
-        }
-        st4(g, i4, gv);
-        stm4(mask, i4, mm);
-    }
-    const int kinds[5] = {0, 0, 0, 0, 0};
-    if (grid_reduce_last<5>(acc, kinds, part, &st->counter[1]) && threadIdx.x == 0) {
-        const int nc = st->nc;
-        double alpha = st->alpha, gmin = st->gmin;
+        st->alpha = alpha;
+        st->gmin = gmin;
+        double ar = alpha, gr = gmin;
         if (nc > 0) {  // refine_contact_mean (contact_solver.cpp:94-99)
-            const double d = acc[1] / nc;
-            alpha += d;
-            gmin -= d;
+            const double d = gcs / nc;
+            ar += d;
+            gr -= d;
         }
         const double PG = P.P_total * P.g_ref;
-        st->alpha_ref = alpha;
-        st->gmin_ref = gmin;
-        st->pv = acc[0];
-        st->gcs = acc[1];
-        st->pk = acc[2] / PG;
-        st->G = acc[3];
-        st->fw = acc[3] / PG;
-        st->pen = fmax(0.0, -gmin) / P.g_ref;
+        const double G = acc[3] - (aT + gmT) * acc[4];
+        st->alpha_ref = ar;
+        st->gmin_ref = gr;
+        st->pv = acc[3];
+        st->gcs = gcs;
+        st->G = G;
+        st->fw = G / PG;
+        st->pen = fmax(0.0, -gr) / P.g_ref;
         st->psum = acc[4];
         st->load = fabs(acc[4] - P.P_total) / P.P_total;
-        st->finite = isfinite(st->gsum) && isfinite(st->vmin) && isfinite(acc[4]) &&
-                     isfinite(acc[2]) && isfinite(acc[3]);
+        st->finite = isfinite(acc[0]) && isfinite(acc[2]) && isfinite(acc[4]) && isfinite(acc[3]);
         if (final_mode) return;
         if (!st->finite) {
             st->status = ST_NONFINITE;
             set_halt(st, H_FINAL);
             return;
         }
-        if (P.record_history && hist) hist[st->it] = st->pk;
         if (st->load <= P.load_tol && st->fw <= P.tol && st->pen <= P.tol) {
             st->status = ST_CONVERGED;
             st->u_fresh = 1;
@@ -202,10 +200,61 @@ __global__ void __launch_bounds__(kRedThreads) k_eval2(const PkParams* __restric
     }
 }
 
+// pk = sum p |g| / (P g_ref) (the reference's legacy error, reported and
+// recorded in the history); runs after k_eval of a recorded iteration
+// (pk_due) or in final mode.
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_evalpk(const PkParams* __restrict__ Pp, PkState* st,
+                                                        const T* p, const T* g, double* part,
+                                                        double* hist, int final_mode) {
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    p += bo_;
+    g += bo_;
+    const PkParams& P = *Pp;
+    if (!final_mode && !st->pk_due) return;
+    const T aT = (T)st->alpha;
+    double acc[1] = {0.0};
+    GRID_LOOP4(P.N) {
+        T pp[4], gv[4];
+        ldp4(p, i4, pp);
+        ldp4(g, i4, gv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[0] += (double)pp[j] * fabs((double)gc(gv[j], aT));
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[12]) && threadIdx.x == 0) {
+        st->pk = acc[0] / (P.P_total * P.g_ref);
+        st->finite = st->finite && isfinite(acc[0]);
+        if (final_mode) return;
+        st->pk_due = 0;
+        if (P.record_history && hist) hist[blockIdx.y * P.hist_stride + st->it] = st->pk;
+    }
+}
+
+// g <- centred gap (materialised for the host-side branches and the output)
+template <typename T>
+__global__ void k_center(const PkParams* __restrict__ Pp, const PkState* st, T* g) {
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    g += (long)blockIdx.y * Pp->N;
+    const T aT = (T)st->alpha;
+    GRID_LOOP4(Pp->N) {
+        T gv[4];
+        ldp4(g, i4, gv);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) gv[j] = gc(gv[j], aT);
+        st4(g, i4, gv);
+    }
+}
+
 // ---- stencil preconditioner (stencil_precond.cpp:63-109) ---------------------
 // z = T(sum_t w_t gc(i + d_t)) on contact, gc = contact ? g - gmean : 0 with
-// periodic wrap; the contact mean of z is removed downstream (dots/tupd read
-// z - zmean).  2-D tile of 64 x 16 outputs with an R-cell halo in shared memory.
+// periodic wrap; the contact mean of z is removed downstream.  2-D tile of
+// 64 x 16 outputs with an R-cell halo in shared memory.  k_stencil is the
+// standalone form (g already centred); the solve loop runs k_stencil_dots.
 constexpr int kStX = 64, kStY = 16, kMaxR = 4;
 
 template <typename T>
@@ -257,19 +306,113 @@ inline int stencil_grid(int Ns) {
     return n < kMaxBlocks ? n : kMaxBlocks;
 }
 
+// PR+ / FR ratio from G = <zf, g>, G_pr = <zf, g - g_prev> (contact_solver.cpp:420-446);
+// beta = Real(delta) * Real(ratio) is formed by the caller
+__device__ __forceinline__ void beta_update(const PkParams& P, PkState* st, double G, double Gpr,
+                                            double gg) {
+    const double G_old = st->G_old;
+    const double bv = (G_old != 0.0) ? (P.use_pr ? fmax(0.0, Gpr / G_old) : G / G_old) : 0.0;
+    st->G_old = G;
+    st->gg = gg;
+    st->bv = bv;
+}
+
+// Stencil preconditioner and the CG dots of the loop in one pass: z on
+// contact (as k_stencil, g centred on the fly) and, with zf = Real(z - zm)
+// the contact-mean-free direction, the dots of the reference
+//   G = sum_C zf g,  G_pr = sum_C zf Real(g - gprev),  gg = sum_C g^2
+// from sums linear in zm (zm is this pass's own reduction):
+//   G = sum_C z g - zm sum_C g,  G_pr = sum_C z (g - gprev) - zm sum_C (g - gprev).
+template <typename T>
+__global__ void __launch_bounds__(256) k_stencil_dots(const PkParams* __restrict__ Pp, PkState* st,
+                                                      StencilTaps taps, const T* g,
+                                                      const T* gprev, const uint8_t* mask,
+                                                      T* z, double* part) {
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    g += bo_;
+    gprev += bo_;
+    mask += bo_;
+    z += bo_;
+    const PkParams& P = *Pp;
+    if (st->halt) return;
+    __shared__ double tile[(kStY + 2 * kMaxR) * (kStX + 2 * kMaxR)];
+    const int Ns = P.Ns, R = taps.R;
+    const int TW = kStX + 2 * R, TH = kStY + 2 * R;
+    const double gmean = st->nc ? st->gcs / st->nc : 0.0;
+    const T aT = (T)st->alpha;
+    const int ntx = (Ns + kStX - 1) / kStX, nty = (Ns + kStY - 1) / kStY;
+    // sum z (unrounded), sum zT g, sum g, sum zT (g - gp), sum (g - gp), sum g^2
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int tid = blockIdx.x; tid < ntx * nty; tid += gridDim.x) {
+        const int tx0 = (tid % ntx) * kStX, ty0 = (tid / ntx) * kStY;
+        for (int idx = threadIdx.x; idx < TW * TH; idx += blockDim.x) {
+            const int ly = idx / TW, lx = idx % TW;
+            int gy = ty0 + ly - R, gx = tx0 + lx - R;
+            gy = gy < 0 ? gy + Ns : (gy >= Ns ? gy - Ns : gy);
+            gx = gx < 0 ? gx + Ns : (gx >= Ns ? gx - Ns : gx);
+            const size_t j = (size_t)gy * Ns + gx;
+            tile[ly * TW + lx] = mask[j] ? (double)gc(g[j], aT) - gmean : 0.0;
+        }
+        __syncthreads();
+        for (int o = threadIdx.x; o < kStX * kStY; o += blockDim.x) {
+            const int ly = o / kStX, lx = o % kStX;
+            const int gy = ty0 + ly, gx = tx0 + lx;
+            if (gy >= Ns || gx >= Ns) continue;
+            const size_t i = (size_t)gy * Ns + gx;
+            if (!mask[i]) { z[i] = T(0); continue; }
+            double a = 0.0;
+            for (int t = 0; t < taps.n; ++t)
+                a += taps.w[t] * tile[(ly + R + taps.dy[t]) * TW + (lx + R + taps.dx[t])];
+            const T zT = (T)a;
+            z[i] = zT;
+            const T gi = gc(g[i], aT);
+            const double gd = (double)gi, dg = (double)(T)(gi - gprev[i]);
+            acc[0] += a;
+            acc[1] += (double)zT * gd;
+            acc[2] += gd;
+            acc[3] += (double)zT * dg;
+            acc[4] += dg;
+            acc[5] += gd * gd;
+        }
+        __syncthreads();
+    }
+    const int kinds[6] = {0, 0, 0, 0, 0, 0};
+    if (grid_reduce_last<6>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
+        const double zmean = st->nc ? (double)(T)(acc[0] / st->nc) : 0.0;
+        st->zmean = zmean;
+        st->pc++;
+        beta_update(P, st, acc[1] - zmean * acc[2], acc[3] - zmean * acc[4], acc[5]);
+        st->beta = (double)((T)st->delta * (T)st->bv);
+    }
+}
+
 // ---- CG passes (contact_solver.cpp:420-501) ------------------------------------
 template <typename T>
 __device__ __forceinline__ T zfinal(const PkParams& P, T z, T g, T zm) {
     return P.precond ? (T)(z - zm) : g;
 }
 
+// dots for the unpreconditioned and the FFT-preconditioned loops (z from the
+// preconditioner; g centred on the fly)
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, const T* gprev,
                                                       const uint8_t* mask, double* part) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    z += bo_;
+    g += bo_;
+    gprev += bo_;
+    mask += bo_;
     const PkParams& P = *Pp;
     if (st->halt) return;
-    const T zm = (T)st->zmean;
+    const T zm = (T)st->zmean, aT = (T)st->alpha;
     double acc[3] = {0, 0, 0};  // G, G_pr, gg
     GRID_LOOP4(P.N) {
         T zz[4], gv[4], gp[4];
@@ -281,31 +424,41 @@ __global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (!mm[j]) continue;
-            const T zf = zfinal(P, zz[j], gv[j], zm);
-            const double gd = (double)gv[j];
+            const T gi = gc(gv[j], aT);
+            const T zf = zfinal(P, zz[j], gi, zm);
+            const double gd = (double)gi;
             acc[0] += (double)zf * gd;
-            acc[1] += (double)zf * (double)(gv[j] - gp[j]);
+            acc[1] += (double)zf * (double)(T)(gi - gp[j]);
             acc[2] += gd * gd;
         }
     }
     const int kinds[3] = {0, 0, 0};
     if (grid_reduce_last<3>(acc, kinds, part, &st->counter[3]) && threadIdx.x == 0) {
-        const double G_old = st->G_old;
-        const double bv = (G_old != 0.0) ? (P.use_pr ? fmax(0.0, acc[1] / G_old) : acc[0] / G_old)
-                                         : 0.0;
-        st->beta = (double)((T)st->delta * (T)bv);
-        st->G_old = acc[0];
-        st->gg = acc[2];
+        beta_update(P, st, acc[0], acc[1], acc[2]);
+        st->beta = (double)((T)st->delta * (T)st->bv);
     }
 }
 
+// Direction update and r sums as separate passes around a plain apply (the
+// ASPHER_UNFUSED_T=1 form of pk_apply_t, kept for A/B timing).
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, T* gprev, T* t,
                                                       const uint8_t* mask, const T* p, T* best) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    z += bo_;
+    g += bo_;
+    gprev += bo_;
+    t += bo_;
+    mask += bo_;
+    p += bo_;
+    best += bo_;
     const PkParams& P = *Pp;
     if (st->halt) return;
-    const T zm = (T)st->zmean, beta = (T)st->beta;
+    const T zm = (T)st->zmean, beta = (T)st->beta, aT = (T)st->alpha;
     const int cb = st->copy_best;
     GRID_LOOP4(P.N) {
         T zz[4], gv[4], tt[4];
@@ -315,8 +468,10 @@ __global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict
         ldp4(t, i4, tt);
         if (P.precond) ldp4(z, i4, zz);
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < 4; ++j) {
+            gv[j] = gc(gv[j], aT);
             tt[j] = mm[j] ? (T)(zfinal(P, zz[j], gv[j], zm) + beta * tt[j]) : T(0);
+        }
         st4(t, i4, tt);
         st4(gprev, i4, gv);
         if (cb) {
@@ -328,12 +483,22 @@ __global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_rsum(const PkParams* __restrict__ Pp, PkState* st, const T* r,
+__global__ void __launch_bounds__(kRedThreads) k_rden(const PkParams* __restrict__ Pp, PkState* st, const T* r,
                                                       const T* g, const T* t,
                                                       const uint8_t* mask, double* part) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    r += bo_;
+    g += bo_;
+    t += bo_;
+    mask += bo_;
     const PkParams& P = *Pp;
     if (st->halt) return;
-    double acc[2] = {0, 0};
+    const T aT = (T)st->alpha;
+    double acc[4] = {0, 0, 0, 0};  // sum_C r, sum_C g t, sum_C r t, sum_C t
     GRID_LOOP4(P.N) {
         T rr[4], gv[4], tt[4];
         uint8_t mm[4];
@@ -344,61 +509,32 @@ __global__ void __launch_bounds__(kRedThreads) k_rsum(const PkParams* __restrict
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             if (!mm[j]) continue;
+            const double td = (double)tt[j];
             acc[0] += (double)rr[j];
-            acc[1] += (double)gv[j] * (double)tt[j];
+            acc[1] += (double)gc(gv[j], aT) * td;
+            acc[2] += (double)rr[j] * td;
+            acc[3] += td;
         }
     }
-    const int kinds[2] = {0, 0};
-    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[4]) && threadIdx.x == 0) {
-        st->mv++;
-        if (st->copy_best) {
-            st->copy_best = 0;
-            st->have_best = 1;
-        }
-        st->rsum = acc[0];
-        st->num = acc[1];
-        st->rmean = (double)(T)(st->nc ? acc[0] / st->nc : 0.0);
-    }
-}
-
-template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_den(const PkParams* __restrict__ Pp, PkState* st, const T* r,
-                                                     const T* t, const uint8_t* mask,
-                                                     double* part) {
-    const PkParams& P = *Pp;
-    if (st->halt) return;
-    const T rm = (T)st->rmean;
-    double acc[1] = {0};
-    GRID_LOOP4(P.N) {
-        T rr[4], tt[4];
-        uint8_t mm[4];
-        ldm4(mask, i4, mm);
-        ldp4(r, i4, rr);
-        ldp4(t, i4, tt);
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-            if (mm[j]) acc[0] += (double)(T)(rr[j] - rm) * (double)tt[j];
-    }
-    const int kinds[1] = {0};
-    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[5]) && threadIdx.x == 0) {
-        const double den = acc[0], num = st->num;
-        st->den = den;
-        if (den > 0.0 && isfinite(den) && isfinite(num)) {
-            const T tau = (T)(num / den);
-            st->tau = (double)tau;
-            st->tau_ov = st->gg > 0.0 ? (double)(T)(num * num / (den * st->gg)) : (double)tau;
-        } else {
-            set_halt(st, H_IDENT);  // no usable direction: identification step
-        }
-    }
+    const int kinds[4] = {0, 0, 0, 0};
+    if (grid_reduce_last<4>(acc, kinds, part, &st->counter[4]) && threadIdx.x == 0)
+        rden_tail<T>(st, acc);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict__ Pp, PkState* st, T* p, const T* t,
                                                       const T* g, double* part) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    p += bo_;
+    t += bo_;
+    g += bo_;
     const PkParams& P = *Pp;
     if (st->halt) return;
-    const T tau = (T)st->tau, tov = (T)st->tau_ov;
+    const T tau = (T)st->tau, tov = (T)st->tau_ov, aT = (T)st->alpha;
     double acc[2] = {0, 0};  // changed (max), total
     GRID_LOOP4(P.N) {
         T pp[4], tt[4], gv[4];
@@ -408,12 +544,13 @@ __global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             T pi = pp[j];
+            const T gi = gc(gv[j], aT);
             const bool was = pi > T(0);
             if (was) {
                 const T q = pi - tau * tt[j];
                 pi = q < T(0) ? T(0) : q;
             }
-            if (pi == T(0) && gv[j] < T(0)) pi -= tov * gv[j];
+            if (pi == T(0) && gi < T(0)) pi -= tov * gi;
             if ((pi > T(0)) != was) acc[0] = 1.0;
             pp[j] = pi;
             acc[1] += (double)pi;
@@ -436,6 +573,12 @@ __global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_rescale(const PkParams* __restrict__ Pp, PkState* st, T* p,
                                                          double* part) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    p += bo_;
     const PkParams& P = *Pp;
     if (st->halt) return;
     const int fill = st->fill;
@@ -467,6 +610,15 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(const PkParams* __restri
                                                         const T* a, const T* b, const T* c,
                                                         const T* d, double theta,
                                                         double* part) {
+    // instance blockIdx.y of a batched launch (0 when unbatched)
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    if (a) a += bo_;
+    if (b) b += bo_;
+    if (c) c += bo_;
+    if (d) d += bo_;
     const PkParams& P = *Pp;
     const T gs = (T)P.gshift;
     double acc[3] = {0, 0, 0};
@@ -623,9 +775,13 @@ __global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, cons
 }
 
 // ---- device-side loop control -------------------------------------------------------
-// Last kernel of the graph body: keep looping while no pass has set `halt`.
-__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st) {
-    cudaGraphSetConditional(h, st->halt == H_RUN ? 1u : 0u);
+// Last kernel of the graph body: keep looping while any instance is running.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st, int B) {
+    // one warp: keep looping while any instance is still running
+    int run = 0;
+    for (int b = threadIdx.x; b < B; b += 32) run |= (st[b].halt == H_RUN);
+    run = __any_sync(0xffffffffu, run);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, run ? 1u : 0u);
 }
 
 // ---- host driver -----------------------------------------------------------------
@@ -638,26 +794,31 @@ int red_grid(long N) {
     return (int)g;
 }
 
-// Per-operator, per-precision solver context: the CG workspace, the device
-// parameter block and the instantiated loop graph (a while-conditional node
-// whose body is one CG iteration), reused by every solve with the same
-// preconditioner configuration.
+// Per-operator, per-precision solver context: the CG workspace of up to
+// `cap` instances (fields back to back), the device parameter and state
+// blocks, and the instantiated loop graph (a while-conditional node whose
+// body is one CG iteration of all instances), reused by every solve with the
+// same preconditioner configuration and batch size.
 template <typename T>
 struct SolverCtx : SolverCtxBase {
     Operator& op;
+    int cap = 1;
     long N = 0;
     T *p = nullptr, *t = nullptr, *u = nullptr, *g = nullptr, *gprev = nullptr, *z = nullptr,
       *r = nullptr, *best = nullptr;
-    T* g0c = nullptr;  // the solve's gap, copied in so the loop graph is reusable
+    T* g0c = nullptr;  // the solves' gaps, copied in so the loop graph is reusable
     uint8_t* mask = nullptr;
     double* part = nullptr;
     double* hist = nullptr;
-    int hist_cap = 0;
+    int hist_cap = 0;  // entries per instance
     PkState* st = nullptr;
     PkParams* Pd = nullptr;
+    void* spec = nullptr;  // spectrum scratch of cap instances (cap > 1 only)
     StencilTaps taps{};
     int precond = -1, radius = -1;
     int grid = 1;
+    int graph_B = 0;
+    bool with_hist = false;  // the loop body records pk per iteration (k_evalpk)
     cudaGraphExec_t exec = nullptr;
     cudaGraph_t graph = nullptr;
     // Private non-blocking stream: the loop graph is captured and launched
@@ -666,26 +827,32 @@ struct SolverCtx : SolverCtxBase {
     cudaStream_t ws = nullptr;
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 
-    explicit SolverCtx(Operator& o) : op(o) {
+    SolverCtx(Operator& o, int capacity) : op(o), cap(capacity) {
         ASB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
         ASB_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
         ASB_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
         N = (long)o.Ns * o.Ns;
-        const size_t b = (size_t)N * sizeof(T);
+        const size_t b = (size_t)cap * N * sizeof(T);
         T** vecs[] = {&p, &t, &u, &g, &gprev, &z, &r, &best, &g0c};
         for (T** v : vecs) ASB_CUDA(cudaMalloc((void**)v, b));
-        ASB_CUDA(cudaMalloc((void**)&mask, (size_t)N));
-        ASB_CUDA(cudaMalloc((void**)&part, kMaxBlocks * 8 * sizeof(double)));
-        ASB_CUDA(cudaMalloc((void**)&st, sizeof(PkState)));
-        ASB_CUDA(cudaMalloc((void**)&Pd, sizeof(PkParams)));
-        ASB_CUDA(cudaMemset(st, 0, sizeof(PkState)));
+        ASB_CUDA(cudaMalloc((void**)&mask, (size_t)cap * N));
+        ASB_CUDA(cudaMalloc((void**)&part, (size_t)cap * kPartStride * sizeof(double)));
+        ASB_CUDA(cudaMalloc((void**)&st, (size_t)cap * sizeof(PkState)));
+        ASB_CUDA(cudaMalloc((void**)&Pd, (size_t)cap * sizeof(PkParams)));
+        ASB_CUDA(cudaMemset(st, 0, (size_t)cap * sizeof(PkState)));
+        ASB_CUDA(cudaMemset(z, 0, b));
         grid = red_grid(N);
         (void)o.spectrum(sizeof(T) == 8, nullptr);  // allocate before any capture
+        if (cap > 1) {
+            const size_t sb = o.spectrum_bytes(sizeof(T) == 8) * (size_t)cap;
+            ASB_CUDA(cudaMalloc(&spec, sb));
+            ASB_CUDA(cudaMemset(spec, 0, sb));
+        }
     }
     ~SolverCtx() override {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
-        void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd};
+        void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd, spec};
         for (void* v : all)
             if (v) cudaFree(v);
         if (ev_in) cudaEventDestroy(ev_in);
@@ -693,22 +860,28 @@ struct SolverCtx : SolverCtxBase {
         if (ws) cudaStreamDestroy(ws);
     }
     size_t bytes() const override {
-        return (9 * sizeof(T) + 1) * (size_t)N + hist_cap * sizeof(double) +
-               kMaxBlocks * 8 * sizeof(double);
-    }
-    void ensure_hist(int cap) {
-        if (cap <= hist_cap) return;
-        if (hist) ASB_CUDA(cudaFree(hist));
-        ASB_CUDA(cudaMalloc((void**)&hist, (size_t)cap * sizeof(double)));
-        hist_cap = cap;
-        drop_graph();  // the graph bakes the history pointer
+        return (size_t)cap * ((9 * sizeof(T) + 1) * (size_t)N + hist_cap * sizeof(double) +
+                              kPartStride * sizeof(double));
     }
     void invalidate() override { drop_graph(); }
+    void ensure_hist(int per_instance) {
+        if (per_instance <= hist_cap) return;
+        if (hist) ASB_CUDA(cudaFree(hist));
+        ASB_CUDA(cudaMalloc((void**)&hist, (size_t)cap * per_instance * sizeof(double)));
+        hist_cap = per_instance;
+        drop_graph();  // the graph bakes the history pointer
+    }
     void drop_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         exec = nullptr;
         graph = nullptr;
+        graph_B = 0;
+    }
+    void set_hist(bool on) {
+        if (on == with_hist) return;
+        with_hist = on;
+        drop_graph();
     }
     void configure(int pc, int R) {
         if (pc == precond && (pc != 1 || R == radius)) return;
@@ -717,40 +890,61 @@ struct SolverCtx : SolverCtxBase {
         radius = R;
         drop_graph();
     }
+    T* at(T* v, int b) const { return v + (size_t)b * N; }
 
-    void apply(const T* x, T* y, const int* gate, cudaStream_t s) {
-        op.matvec(sizeof(T) == 8, x, y, s, gate);
+    // B instances: gates per instance, spectrum of the batch when B > 1
+    void apply(const T* x, T* y, const int* gate, cudaStream_t s, int B) {
+        op.matvec(sizeof(T) == 8, x, y, s, gate, B, B > 1 ? spec : nullptr);
     }
-    void precond_apply(const int* gate, cudaStream_t s) {
-        if (precond == 1) {
-            k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, g, mask, z, part,
-                                                            gate != nullptr);
-            count_launches(1);
-            ASB_CUDA(cudaGetLastError());
-        } else if (precond == 2) {
-            fourier_precond_pk<T>(op, g, mask, st, z, part, s, gate);
+    // one CG iteration of B instances (the common path), every pass gated
+    // per instance on the device:
+    //   [apply p->u] eval (evalpk) | stencil+dots  or  [precond] dots |
+    //   [apply t->r with the direction update and the r sums fused] pupd rescale
+    void enqueue_iteration(cudaStream_t s, int B) {
+        const dim3 gr(grid, B);
+        int n = 0;
+        apply(p, u, &st->skip_mv1, s, B);
+        k_eval<T><<<gr, kRedThreads, 0, s>>>(Pd, st, u, g0c, p, g, mask, part, 0);
+        ++n;
+        if (with_hist) {
+            k_evalpk<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, g, part, hist, 0);
+            ++n;
         }
-    }
-    // one CG iteration (the common path), every pass gated on the device
-    void enqueue_iteration(const T* g0, cudaStream_t s) {
-        apply(p, u, &st->skip_mv1, s);
-        k_eval1<T><<<grid, kRedThreads, 0, s>>>(Pd, st, u, g0, p, g, part, 0);
-        k_eval2<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, g, mask, part, hist, 0);
-        if (precond > 0) precond_apply(&st->halt, s);
-        k_dots<T><<<grid, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
-        k_tupd<T><<<grid, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
-        apply(t, r, &st->halt, s);
-        k_rsum<T><<<grid, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
-        k_den<T><<<grid, kRedThreads, 0, s>>>(Pd, st, r, t, mask, part);
-        k_pupd<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
-        k_rescale<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, part);
-        count_launches(8);
+        if (precond == 1) {
+            k_stencil_dots<T><<<dim3(stencil_grid(op.Ns), B), 256, 0, s>>>(Pd, st, taps, g, gprev,
+                                                                          mask, z, part);
+            ++n;
+        } else {
+            if (precond == 2)
+                fourier_precond_pk<T>(op, g, mask, st, z, part, s, &st->halt, B,
+                                      B > 1 ? spec : nullptr);
+            k_dots<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
+            ++n;
+        }
+        if (unfused_t()) {
+            k_tupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
+            apply(t, r, &st->halt, s, B);
+            k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
+            n += 2;
+        } else {
+            pk_apply_t<T>(op, z, g, gprev, t, mask, p, best, st, part, precond, s, &st->halt, B,
+                          B > 1 ? spec : nullptr);
+        }
+        k_pupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
+        k_rescale<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, part);
+        count_launches(n + 2);
         ASB_CUDA(cudaGetLastError());
     }
-    // Graph: while (halt == H_RUN) { iteration }.  The g0 pointer is baked
-    // in, so the graph is rebuilt when a solve passes another gap buffer.
-    const T* graph_g0 = nullptr;
-    void build_graph(const T* g0, cudaStream_t s) {
+    // g <- centred gap for instance b (or all B when b < 0)
+    void center(cudaStream_t s, int B, int b = -1) {
+        if (b < 0)
+            k_center<T><<<dim3(grid, B), kRedThreads, 0, s>>>(Pd, st, g);
+        else
+            k_center<T><<<grid, kRedThreads, 0, s>>>(Pd + b, st + b, at(g, b));
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+    }
+    void build_graph(cudaStream_t s, int B) {
         drop_graph();
         ASB_CUDA(cudaGraphCreate(&graph, 0));
         cudaGraphConditionalHandle h;
@@ -765,47 +959,79 @@ struct SolverCtx : SolverCtxBase {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ASB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeRelaxed));
-        enqueue_iteration(g0, s);
-        k_loop_cond<<<1, 1, 0, s>>>(h, st);
+        enqueue_iteration(s, B);
+        k_loop_cond<<<1, 32, 0, s>>>(h, st, B);
         cudaGraph_t captured = nullptr;
         ASB_CUDA(cudaStreamEndCapture(s, &captured));
         ASB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        graph_g0 = g0;
+        graph_B = B;
     }
     // (Re)build the loop graph if needed.  Before capturing, one fully gated
     // iteration runs eagerly (every kernel returns at entry) so that all
     // function attributes are set outside the capture.  Clobbers st; the
-    // caller writes the initial state afterwards.
-    void ensure_graph(const T* g0, cudaStream_t s) {
-        if (exec && graph_g0 == g0) return;
-        PkState gated;
-        std::memset(&gated, 0, sizeof(gated));
-        gated.halt = H_FINAL;
-        gated.skip_mv1 = 1;
-        ASB_CUDA(cudaMemcpyAsync(st, &gated, sizeof(PkState), cudaMemcpyHostToDevice, s));
-        enqueue_iteration(g0, s);
+    // caller writes the initial states afterwards.
+    void ensure_graph(cudaStream_t s, int B) {
+        if (exec && graph_B == B) return;
+        std::vector<PkState> gated(B);
+        std::memset(gated.data(), 0, B * sizeof(PkState));
+        for (auto& x : gated) {
+            x.halt = H_FINAL;
+            x.skip_mv1 = 1;
+        }
+        ASB_CUDA(cudaMemcpyAsync(st, gated.data(), B * sizeof(PkState), cudaMemcpyHostToDevice, s));
+        enqueue_iteration(s, B);
         ASB_CUDA(cudaStreamSynchronize(s));
-        build_graph(g0, s);
+        build_graph(s, B);
     }
     void launch_graph(cudaStream_t s) {
         ASB_CUDA(cudaGraphLaunch(exec, s));
         count_launches(1);
     }
+    // ASPHER_EAGER_LOOP=1: enqueue iterations as plain launches instead of the
+    // loop graph (same kernels, same gating; for per-kernel profilers)
+    static bool eager_loop() {
+        static const bool e = [] {
+            const char* v = std::getenv("ASPHER_EAGER_LOOP");
+            return v && v[0] == '1';
+        }();
+        return e;
+    }
+    // ASPHER_UNFUSED_T=1: direction update and r sums as separate passes
+    // around a plain apply (A/B timing of the fused t-apply)
+    static bool unfused_t() {
+        static const bool e = [] {
+            const char* v = std::getenv("ASPHER_UNFUSED_T");
+            return v && v[0] == '1';
+        }();
+        return e;
+    }
+};
+
+// One instance's host-side bookkeeping in a (possibly batched) solve.
+struct InstHost {
+    double p_bar = 0.0, P_total = 0.0, g_ref = 1.0, p_ref = 0.0, datum = 0.0;
+    double s_id = 0.0;
+    int forced_id = 0, id_steps = 0;
+    std::string reason;
+    long long mv_host = 0;
+    bool returned_best = false;
+    int status = ST_MAX_ITERATIONS;
 };
 
 template <typename T>
 struct Solver {
     SolverCtx<T>& c;
-    PkParams P{};
     cudaStream_t s;
-    PkState h{};  // host mirror
-    const T* g0 = nullptr;
-    long long mv_host = 0;
-
     cudaStream_t caller;
+    int B = 1;
+    std::vector<PkParams> P;
+    std::vector<PkState> h;  // host mirrors
+    std::vector<InstHost> ih;
+
     // All work runs on the context's private stream, ordered after the
     // caller's pending work and before the caller's later work.
-    Solver(SolverCtx<T>& ctx, cudaStream_t st) : c(ctx), s(ctx.ws), caller(st) {
+    Solver(SolverCtx<T>& ctx, cudaStream_t st, int batch = 1)
+        : c(ctx), s(ctx.ws), caller(st), B(batch), P(batch), h(batch), ih(batch) {
         ASB_CUDA(cudaEventRecord(c.ev_in, caller));
         ASB_CUDA(cudaStreamWaitEvent(s, c.ev_in, 0));
     }
@@ -813,40 +1039,46 @@ struct Solver {
         if (cudaEventRecord(c.ev_out, s) == cudaSuccess) cudaStreamWaitEvent(caller, c.ev_out, 0);
     }
 
-    void read_state() {
-        ASB_CUDA(cudaMemcpyAsync(&h, c.st, sizeof(PkState), cudaMemcpyDeviceToHost, s));
+    void read_states() {
+        ASB_CUDA(cudaMemcpyAsync(h.data(), c.st, B * sizeof(PkState), cudaMemcpyDeviceToHost, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
-    void write_state() {
-        ASB_CUDA(cudaMemcpyAsync(c.st, &h, sizeof(PkState), cudaMemcpyHostToDevice, s));
+    void write_states() {
+        ASB_CUDA(cudaMemcpyAsync(c.st, h.data(), B * sizeof(PkState), cudaMemcpyHostToDevice, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
-    // results of the helper reductions live in st->red; only that slice is
-    // read back so the host mirror `h` is never clobbered mid-update
-    void read_red(double (&r)[8]) {
-        ASB_CUDA(cudaMemcpyAsync(r, c.st->red, sizeof(r), cudaMemcpyDeviceToHost, s));
+    void write_params() {
+        ASB_CUDA(cudaMemcpyAsync(c.Pd, P.data(), B * sizeof(PkParams), cudaMemcpyHostToDevice, s));
+    }
+    // results of the helper reductions live in st[b].red; only that slice is
+    // read back so the host mirrors are never clobbered mid-update
+    void read_red(int b, double (&r)[8]) {
+        ASB_CUDA(cudaMemcpyAsync(r, c.st[b].red, sizeof(r), cudaMemcpyDeviceToHost, s));
         ASB_CUDA(cudaStreamSynchronize(s));
     }
-    double reduce(int mode, const T* a, const T* b, const T* cc, const T* d, double theta,
+    // reduction of instance b (pointers are instance b's fields)
+    double reduce(int b, int mode, const T* a, const T* bb, const T* cc, const T* d, double theta,
                   double* out3 = nullptr) {
-        k_reduce<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, mode, a, b, cc, d, theta, c.part);
+        k_reduce<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd + b, c.st + b, mode, a, bb, cc, d, theta,
+                                                 c.part + (size_t)b * kPartStride);
         count_launches(1);
         ASB_CUDA(cudaGetLastError());
         double r[8];
-        read_red(r);
+        read_red(b, r);
         if (out3) { out3[0] = r[0]; out3[1] = r[1]; out3[2] = r[2]; }
         return r[0];
     }
 
-    // project_load_simplex on c.z (contact_solver.cpp:31-60)
-    void project_simplex(double P_total) {
-        const long N = P.N;
-        double ssum = reduce(1, c.z, nullptr, nullptr, nullptr, 0.0);
+    // project_load_simplex on instance b's z (contact_solver.cpp:31-60)
+    void project_simplex(int b, double P_total) {
+        const long N = c.N;
+        T* z = c.at(c.z, b);
+        double ssum = reduce(b, 1, z, nullptr, nullptr, nullptr, 0.0);
         long nact = N;
         double theta = (ssum - P_total) / (double)nact;
         for (int pass = 0; pass < 64; ++pass) {
             double o[3];
-            reduce(4, c.z, nullptr, nullptr, nullptr, theta, o);
+            reduce(b, 4, z, nullptr, nullptr, nullptr, theta, o);
             const long n2 = (long)o[1];
             if (n2 == 0) break;
             if (n2 == nact) break;
@@ -854,275 +1086,353 @@ struct Solver {
             ssum = o[0];
             theta = (ssum - P_total) / (double)nact;
         }
-        k_threshold<T><<<c.grid, kRedThreads, 0, s>>>(N, c.z, (T)theta);
+        k_threshold<T><<<c.grid, kRedThreads, 0, s>>>(N, z, (T)theta);
         count_launches(1);
         ASB_CUDA(cudaGetLastError());
     }
 
-    // identification step (contact_solver.cpp:314-364); host mirror h is current
-    bool identification_step(double& s_id, int& id_steps) {
+    // identification step of instance b (contact_solver.cpp:314-364); reads
+    // the centred gap (the caller materialises it first)
+    bool identification_step(int b) {
+        InstHost& I = ih[b];
+        PkState& H = h[b];
+        T *p = c.at(c.p, b), *u = c.at(c.u, b), *g = c.at(c.g, b), *z = c.at(c.z, b),
+          *r = c.at(c.r, b), *t = c.at(c.t, b), *gp = c.at(c.gprev, b);
+        const T* g0 = c.at(c.g0c, b);
         double o[3];
-        reduce(2, c.p, c.u, g0, nullptr, 0.0, o);
+        reduce(b, 2, p, u, g0, nullptr, 0.0, o);
         const double f_cur = o[0];
-        if (!(s_id > 0.0)) {
+        if (!(I.s_id > 0.0)) {
             const double pp = o[1], pu = o[2];
-            s_id = (pu > 0.0 && pp > 0.0) ? pp / pu : 1.0;
+            I.s_id = (pu > 0.0 && pp > 0.0) ? pp / pu : 1.0;
         }
         for (int trial = 0; trial < 12; ++trial) {
-            k_axpy_trial<T><<<c.grid, kRedThreads, 0, s>>>(P.N, c.z, c.p, c.g, (T)s_id);
+            k_axpy_trial<T><<<c.grid, kRedThreads, 0, s>>>(c.N, z, p, g, (T)I.s_id);
             count_launches(1);
-            project_simplex(P.P_total);
-            c.apply(c.z, c.r, nullptr, s);
-            mv_host++;
-            reduce(3, c.z, c.r, g0, nullptr, 0.0, o);
+            project_simplex(b, I.P_total);
+            c.op.matvec(sizeof(T) == 8, z, r, s, nullptr);  // unbatched scratch
+            I.mv_host++;
+            reduce(b, 3, z, r, g0, nullptr, 0.0, o);
             const double f_try = o[0];
-            k_gd<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.g, c.z, c.p, c.part);
+            k_gd<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd + b, c.st + b, g, z, p,
+                                                 c.part + (size_t)b * kPartStride);
             count_launches(1);
             double rr[8];
-            read_red(rr);
+            read_red(b, rr);
             const double gd = rr[3];
             if (std::isfinite(f_try) && gd < 0.0 && f_try <= f_cur + 1e-4 * gd) {
-                const size_t b = (size_t)P.N * sizeof(T);
-                ASB_CUDA(cudaMemcpyAsync(c.p, c.z, b, cudaMemcpyDeviceToDevice, s));
-                ASB_CUDA(cudaMemcpyAsync(c.u, c.r, b, cudaMemcpyDeviceToDevice, s));
-                ASB_CUDA(cudaMemsetAsync(c.t, 0, b, s));
-                ASB_CUDA(cudaMemsetAsync(c.gprev, 0, b, s));
-                h.u_fresh = 1;
-                h.delta = 0.0;
-                h.G_old = 1.0;
-                ++id_steps;
-                if (trial == 0) s_id *= 2.0;
+                const size_t bytes = (size_t)c.N * sizeof(T);
+                ASB_CUDA(cudaMemcpyAsync(p, z, bytes, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemcpyAsync(u, r, bytes, cudaMemcpyDeviceToDevice, s));
+                ASB_CUDA(cudaMemsetAsync(t, 0, bytes, s));
+                ASB_CUDA(cudaMemsetAsync(gp, 0, bytes, s));
+                H.u_fresh = 1;
+                H.delta = 0.0;
+                H.G_old = 1.0;
+                ++I.id_steps;
+                if (trial == 0) I.s_id *= 2.0;
                 return true;
             }
-            s_id *= 0.25;
+            I.s_id *= 0.25;
         }
         return false;
     }
 
-    void run(const aspher_solve_opts& o, const T* g0_, double p_bar, const T* p_init,
-             double* pressure, double* disp, double* gap, double* hist_host, int hist_cap,
-             aspher_result& res) {
+    // Solve B instances that share the operator and the options.  g0s[b],
+    // p_inits[b] (nullable) are device fields of T; outputs FP64 (disps /
+    // gaps / hist only honoured for B == 1).  datum_b / gref_b (nullable):
+    // per-instance datum and g_ref overriding opts' (used with the datum
+    // modes solver / caller).
+    void run(const aspher_solve_opts& o, const T* const* g0s, const double* p_bars,
+             const T* const* p_inits, double* const* pressures, double* disp, double* gap,
+             double* hist_host, int hist_cap, aspher_result* res,
+             const double* datum_b = nullptr, const double* gref_b = nullptr) {
         const auto t_start = std::chrono::steady_clock::now();
         const int Ns = c.op.Ns;
         const long N = (long)Ns * Ns;
-        // the caller's gap is read once into the context (zero-copy is not
-        // needed on a 180 GB device, and a fixed address keeps the graph valid)
-        if (g0_ != c.g0c)
-            ASB_CUDA(cudaMemcpyAsync(c.g0c, g0_, (size_t)N * sizeof(T), cudaMemcpyDeviceToDevice,
-                                     s));
-        g0 = c.g0c;
         constexpr bool is_double = sizeof(T) == 8;
-        if (!(p_bar > 0.0) || !std::isfinite(p_bar))
-            throw Error(ASPHER_EINVAL, "solve_contact: empty gap or p_bar <= 0");
+        if (B < 1 || B > c.cap) throw Error(ASPHER_EINVAL, "solve: batch size out of range");
+        for (int b = 0; b < B; ++b)
+            if (!(p_bars[b] > 0.0) || !std::isfinite(p_bars[b]))
+                throw Error(ASPHER_EINVAL, "solve_contact: empty gap or p_bar <= 0");
         if (!(o.tol > 0.0)) throw Error(ASPHER_EINVAL, "solve_contact: tol must be positive");
         if (o.max_iter < 0) throw Error(ASPHER_EINVAL, "solve_contact: max_iter must be >= 0");
         if (o.precond < 0 || o.precond > 2) throw Error(ASPHER_EINVAL, "solve_contact: bad precond");
         c.configure(o.precond, o.precond_radius);
-        if (o.record_history) c.ensure_hist(o.max_iter + 1);
-        P.N = N;
-        P.Ns = Ns;
-        // validation before any operator apply (contact_solver.cpp:159-168)
-        double mm[3];
-        ASB_CUDA(cudaMemcpyAsync(c.Pd, &P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
-        reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
-        if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
-        const double P_total = (double)(T)p_bar * (double)N;
-        const double gmin_v = mm[0], gmax_v = mm[1];
-        double g_ref = o.g_ref;
-        if (!(g_ref > 0.0)) g_ref = gmax_v - gmin_v;
-        if (!(g_ref > 0.0)) g_ref = 1.0;
-        const double p_ref = o.p_ref > 0.0 ? o.p_ref : (double)(T)p_bar;
+        const bool rec = o.record_history && B == 1 && hist_host && hist_cap > 0;
+        if (rec) c.ensure_hist(o.max_iter + 1);
+        c.set_hist(rec);
+        // the caller's gaps are read once into the context (a fixed address
+        // keeps the graph valid)
+        for (int b = 0; b < B; ++b) {
+            P[b] = PkParams{};
+            P[b].N = N;
+            P[b].Ns = Ns;
+            if (g0s[b] != c.at(c.g0c, b))
+                ASB_CUDA(cudaMemcpyAsync(c.at(c.g0c, b), g0s[b], (size_t)N * sizeof(T),
+                                         cudaMemcpyDeviceToDevice, s));
+        }
+        write_params();
+        // validation before any operator apply (contact_solver.cpp:159-168):
+        // min, max and non-finite count of every gap in one batched pass
+        k_reduce<T><<<dim3(c.grid, B), kRedThreads, 0, s>>>(c.Pd, c.st, 0, c.g0c, nullptr, nullptr,
+                                                          nullptr, 0.0, c.part);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+        read_states();
         const double load_tol = o.load_tol > 0.0 ? o.load_tol : (is_double ? 1e-12 : 5e-7);
         const double tol = o.tol;
         const double req_tol = o.requested_tol > 0.0 ? o.requested_tol : tol;
-        double datum = 0.0;
-        bool subtract = false;
-        if (o.datum_mode == ASPHER_DATUM_AUTOMATIC) {
-            datum = gmin_v + 0.5 * (gmax_v - gmin_v);
-            subtract = true;
-        } else if (o.datum_mode == ASPHER_DATUM_SOLVER) {
-            datum = o.datum;
-            subtract = true;
-        } else {
-            datum = o.datum;
+        for (int b = 0; b < B; ++b) {
+            InstHost& I = ih[b];
+            const double gmin_v = h[b].red[0], gmax_v = h[b].red[1];
+            if (h[b].red[2] > 0.0)
+                throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
+            I.p_bar = p_bars[b];
+            I.P_total = (double)(T)p_bars[b] * (double)N;
+            double g_ref = gref_b ? gref_b[b] : o.g_ref;
+            if (!(g_ref > 0.0)) g_ref = gmax_v - gmin_v;
+            if (!(g_ref > 0.0)) g_ref = 1.0;
+            I.g_ref = g_ref;
+            I.p_ref = o.p_ref > 0.0 ? o.p_ref : (double)(T)p_bars[b];
+            bool subtract = false;
+            if (o.datum_mode == ASPHER_DATUM_AUTOMATIC) {
+                I.datum = gmin_v + 0.5 * (gmax_v - gmin_v);
+                subtract = true;
+            } else if (o.datum_mode == ASPHER_DATUM_SOLVER) {
+                I.datum = datum_b ? datum_b[b] : o.datum;
+                subtract = true;
+            } else {
+                I.datum = datum_b ? datum_b[b] : o.datum;
+            }
+            PkParams& Q = P[b];
+            Q.max_iter = o.max_iter;
+            Q.stall_limit = o.stall_limit > 0 ? o.stall_limit : 200;
+            Q.keep_best = o.keep_best;
+            Q.record_history = rec ? 1 : 0;
+            Q.hist_stride = c.hist_cap;
+            Q.use_pr = o.use_pr;
+            Q.precond = o.precond;
+            Q.P_total = I.P_total;
+            Q.g_ref = g_ref;
+            Q.tol = tol;
+            Q.load_tol = load_tol;
+            Q.p_bar = (double)(T)p_bars[b];
+            Q.gshift = subtract ? (double)(T)I.datum : 0.0;
         }
-        P.max_iter = o.max_iter;
-        P.stall_limit = o.stall_limit > 0 ? o.stall_limit : 200;
-        P.keep_best = o.keep_best;
-        P.record_history = o.record_history && c.hist_cap > 0;
-        P.use_pr = o.use_pr;
-        P.precond = o.precond;
-        P.P_total = P_total;
-        P.g_ref = g_ref;
-        P.tol = tol;
-        P.load_tol = load_tol;
-        P.p_bar = (double)(T)p_bar;
-        P.gshift = subtract ? (double)(T)datum : 0.0;
-        ASB_CUDA(cudaMemcpyAsync(c.Pd, &P, sizeof(PkParams), cudaMemcpyHostToDevice, s));
+        write_params();
 
-        // initial pressure (contact_solver.cpp:204-223)
-        const T pb = (T)p_bar;
-        if (p_init) {
-            k_clamp_pos<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, p_init);
+        // initial pressures (contact_solver.cpp:204-223)
+        for (int b = 0; b < B; ++b) {
+            T* p = c.at(c.p, b);
+            const T pb = (T)p_bars[b];
+            if (p_inits && p_inits[b]) {
+                k_clamp_pos<T><<<c.grid, kRedThreads, 0, s>>>(N, p, p_inits[b]);
+                count_launches(1);
+                const double ssum = reduce(b, 1, p, nullptr, nullptr, nullptr, 0.0);
+                if (ssum > 0.0)
+                    k_scale<T><<<c.grid, kRedThreads, 0, s>>>(N, p, (T)(ih[b].P_total / ssum));
+                else
+                    k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, p, pb);
+            } else {
+                k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, p, pb);
+            }
             count_launches(1);
-            const double ssum = reduce(1, c.p, nullptr, nullptr, nullptr, 0.0);
-            if (ssum > 0.0) k_scale<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, (T)(P_total / ssum));
-            else k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, pb);
-        } else {
-            k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, c.p, pb);
         }
-        count_launches(1);
-        ASB_CUDA(cudaMemsetAsync(c.t, 0, (size_t)N * sizeof(T), s));
-        ASB_CUDA(cudaMemsetAsync(c.gprev, 0, (size_t)N * sizeof(T), s));
-        ASB_CUDA(cudaMemsetAsync(c.z, 0, (size_t)N * sizeof(T), s));
-        std::memset(&h, 0, sizeof(h));
-        h.G_old = 1.0;
-        h.delta = 0.0;
-        h.best_merit = std::numeric_limits<double>::infinity();
-        h.seen_merit = std::numeric_limits<double>::infinity();
-        h.status = ST_MAX_ITERATIONS;
-        h.halt = o.max_iter > 0 ? H_RUN : H_FINAL;
-        h.skip_mv1 = h.halt ? 1 : 0;
-        c.ensure_graph(g0, s);
-        write_state();
+        const size_t vb = (size_t)B * N * sizeof(T);
+        ASB_CUDA(cudaMemsetAsync(c.t, 0, vb, s));
+        ASB_CUDA(cudaMemsetAsync(c.gprev, 0, vb, s));
+        ASB_CUDA(cudaMemsetAsync(c.z, 0, vb, s));
+        for (int b = 0; b < B; ++b) {
+            PkState& H = h[b];
+            std::memset(&H, 0, sizeof(H));
+            H.G_old = 1.0;
+            H.delta = 0.0;
+            H.best_merit = std::numeric_limits<double>::infinity();
+            H.seen_merit = std::numeric_limits<double>::infinity();
+            H.status = ST_MAX_ITERATIONS;
+            H.halt = o.max_iter > 0 ? H_RUN : H_FINAL;
+            H.skip_mv1 = H.halt ? 1 : 0;
+        }
+        if (!SolverCtx<T>::eager_loop()) c.ensure_graph(s, B);
+        write_states();
 
-        double s_id = 0.0;
-        int forced_id = 0, id_steps = 0;
-        std::string reason;
-        while (h.halt == H_RUN) {
-            c.launch_graph(s);
-            read_state();
-            if (h.halt == H_RUN || h.halt == H_FINAL) break;
-            if (h.copy_best) {
-                ASB_CUDA(cudaMemcpyAsync(c.best, c.p, (size_t)N * sizeof(T),
-                                         cudaMemcpyDeviceToDevice, s));
-                h.copy_best = 0;
-                h.have_best = 1;
+        // ---- the loop: device-driven, the host services rare branches
+        auto any_running = [&]() {
+            for (int b = 0; b < B; ++b)
+                if (h[b].halt == H_RUN) return true;
+            return false;
+        };
+        while (any_running()) {
+            if (SolverCtx<T>::eager_loop()) {
+                for (int k = 0; k < 8; ++k) c.enqueue_iteration(s, B);
+            } else {
+                c.launch_graph(s);
             }
-            if (h.halt == H_STALL) {
-                if (forced_id < 3 && identification_step(s_id, id_steps)) {
-                    ++forced_id;
-                    h.stall = 0;
-                } else {
-                    h.status = ST_STAGNATED;
-                    reason = "stall";
-                    h.halt = H_FINAL;
-                    break;
+            read_states();
+            bool changed = false;
+            for (int b = 0; b < B; ++b) {
+                PkState& H = h[b];
+                InstHost& I = ih[b];
+                if (H.halt != H_STALL && H.halt != H_IDENT) continue;
+                changed = true;
+                if (H.copy_best) {
+                    ASB_CUDA(cudaMemcpyAsync(c.at(c.best, b), c.at(c.p, b), (size_t)N * sizeof(T),
+                                             cudaMemcpyDeviceToDevice, s));
+                    H.copy_best = 0;
+                    H.have_best = 1;
                 }
-            } else if (h.halt == H_IDENT) {
-                if (!identification_step(s_id, id_steps)) {
-                    h.status = ST_NONPOSITIVE_CURVATURE;
-                    h.halt = H_FINAL;
-                    break;
+                c.center(s, B, b);  // the identification step reads the centred gap
+                bool resume = true;
+                if (H.halt == H_STALL) {
+                    if (I.forced_id < 3 && identification_step(b)) {
+                        ++I.forced_id;
+                        H.stall = 0;
+                    } else {
+                        H.status = ST_STAGNATED;
+                        I.reason = "stall";
+                        H.halt = H_FINAL;
+                        resume = false;
+                    }
+                } else if (!identification_step(b)) {
+                    H.status = ST_NONPOSITIVE_CURVATURE;
+                    H.halt = H_FINAL;
+                    resume = false;
                 }
+                if (!resume) continue;
+                // the loop body's end increments the iteration counter
+                H.it++;
+                H.mv += I.mv_host;
+                I.mv_host = 0;
+                if (H.it >= o.max_iter) {
+                    H.halt = H_FINAL;
+                    continue;
+                }
+                H.halt = H_RUN;
+                H.skip_mv1 = H.u_fresh ? 1 : 0;
             }
-            // resume: the loop body's end increments the iteration counter
-            h.it++;
-            h.mv += mv_host;
-            mv_host = 0;
-            if (h.it >= o.max_iter) {
-                h.halt = H_FINAL;
-                break;
-            }
-            h.halt = H_RUN;
-            h.skip_mv1 = h.u_fresh ? 1 : 0;
-            write_state();
+            if (changed) write_states();
         }
-        h.mv += mv_host;
-        mv_host = 0;
-        int status = h.status;
+
         // ---- final, freshly evaluated diagnostics (contact_solver.cpp:518-586)
-        bool returned_best = false;
-        if (status != ST_CONVERGED && o.keep_best && h.have_best) {
-            const double merit = std::max(h.fw, h.pen);
-            if (!(merit <= h.best_merit)) {
-                ASB_CUDA(cudaMemcpyAsync(c.p, c.best, (size_t)N * sizeof(T),
-                                         cudaMemcpyDeviceToDevice, s));
-                h.u_fresh = 0;
-                returned_best = true;
+        for (int b = 0; b < B; ++b) {
+            PkState& H = h[b];
+            InstHost& I = ih[b];
+            H.mv += I.mv_host;
+            I.mv_host = 0;
+            I.status = H.status;
+            if (I.status != ST_CONVERGED && o.keep_best && H.have_best) {
+                const double merit = std::max(H.fw, H.pen);
+                if (!(merit <= H.best_merit)) {
+                    ASB_CUDA(cudaMemcpyAsync(c.at(c.p, b), c.at(c.best, b), (size_t)N * sizeof(T),
+                                             cudaMemcpyDeviceToDevice, s));
+                    H.u_fresh = 0;
+                    I.returned_best = true;
+                }
             }
+            if (!H.u_fresh) H.mv++;
+            H.skip_mv1 = H.u_fresh ? 1 : 0;  // gates the final apply per instance
+            H.halt = H_FINAL;
         }
-        if (!h.u_fresh) {
-            c.apply(c.p, c.u, nullptr, s);
-            h.mv++;
-        }
-        h.halt = H_FINAL;
-        write_state();
-        k_eval1<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.u, g0, c.p, c.g, c.part, 1);
-        k_eval2<T><<<c.grid, kRedThreads, 0, s>>>(c.Pd, c.st, c.p, c.g, c.mask, c.part, nullptr, 1);
+        write_states();
+        c.apply(c.p, c.u, &c.st->skip_mv1, s, B);
+        k_eval<T><<<dim3(c.grid, B), kRedThreads, 0, s>>>(c.Pd, c.st, c.u, c.g0c, c.p, c.g, c.mask,
+                                                        c.part, 1);
+        k_evalpk<T><<<dim3(c.grid, B), kRedThreads, 0, s>>>(c.Pd, c.st, c.p, c.g, c.part, nullptr,
+                                                          1);
         count_launches(2);
         ASB_CUDA(cudaGetLastError());
-        read_state();
-        if (!h.finite && status != ST_NONFINITE) status = ST_NONFINITE;
-        if (status == ST_CONVERGED && !(h.load <= load_tol && h.fw <= tol && h.pen <= tol)) {
-            status = ST_VERIFICATION_FAILED;
-            reason = "final_check";
-        }
-        if (status == ST_CONVERGED && req_tol < tol && !o.allow_tolerance_relaxation) {
-            if (!(h.fw <= req_tol && h.pen <= req_tol)) {
-                status = ST_STAGNATED;
-                reason = "precision_limit";
-            }
-        }
-        double ob[3];
-        reduce(5, c.p, c.u, g0, nullptr, 0.0, ob);
-        k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, pressure, c.p);
+        read_states();
+        // objective sum p (0.5 u + g0s) of every instance in one batched pass
+        k_reduce<T><<<dim3(c.grid, B), kRedThreads, 0, s>>>(c.Pd, c.st, 5, c.p, c.u, c.g0c, nullptr,
+                                                          0.0, c.part);
         count_launches(1);
-        if (!o.light) {
+        std::vector<PkState> ob(B);
+        ASB_CUDA(cudaMemcpyAsync(ob.data(), c.st, B * sizeof(PkState), cudaMemcpyDeviceToHost, s));
+        for (int b = 0; b < B; ++b) {
+            k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, pressures[b], c.at(c.p, b));
+            count_launches(1);
+        }
+        if (B == 1 && !o.light) {
             if (disp) { k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, disp, c.u); count_launches(1); }
-            if (gap) { k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, gap, c.g); count_launches(1); }
+            if (gap) {
+                c.center(s, 1);
+                k_to_f64<T><<<c.grid, kRedThreads, 0, s>>>(N, gap, c.g);
+                count_launches(1);
+            }
         }
         ASB_CUDA(cudaGetLastError());
         int hl = 0;
-        if (o.record_history && hist_host && hist_cap > 0 && c.hist_cap > 0) {
-            hl = std::min(h.it, hist_cap);
+        if (rec) {
+            hl = std::min(h[0].it, hist_cap);
             if (hl > 0)
                 ASB_CUDA(cudaMemcpyAsync(hist_host, c.hist, hl * sizeof(double),
                                          cudaMemcpyDeviceToHost, s));
         }
         ASB_CUDA(cudaStreamSynchronize(s));
-
-        std::memset(&res, 0, sizeof(res));
-        res.status = status;
-        std::strncpy(res.status_reason, reason.c_str(), sizeof(res.status_reason) - 1);
-        res.iterations = h.it;
-        res.converged = status == ST_CONVERGED;
-        res.contact_fraction = (double)h.nc / (double)N;
-        res.mean_pressure = h.psum / (double)N;
-        res.approach = h.alpha_ref + datum;
-        res.objective = ob[0] + datum * P_total;
-        res.error = h.pk;
-        res.pk_error = h.pk;
-        res.fw_gap = h.G;
-        res.fw_error = h.fw;
-        res.load_error = h.load;
-        res.pressure_violation = 0.0;
-        res.penetration_error = h.pen;
-        res.requested_tol = req_tol;
-        res.effective_tol = tol;
-        res.p_ref = p_ref;
-        res.g_ref = g_ref;
-        res.matvec_count = h.mv;
-        res.precond_count = h.pc;
-        res.identification_steps = id_steps;
-        res.returned_best = returned_best;
-        res.history_len = hl;
-        const long long rb = sizeof(T);
-        res.mem_cg_state = 7LL * N * rb;
-        res.mem_best_iterate = o.keep_best ? N * rb : 0;
-        res.mem_contact_mask = N;
-        res.mem_output_arrays = (rb == 8 ? 0 : N * 8LL) + (o.light ? 0 : 2LL * N * 8);
-        res.mem_peak = res.mem_cg_state + res.mem_best_iterate + res.mem_contact_mask +
-                       res.mem_output_arrays;
-        res.time_total = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start)
-                             .count();
+        const double secs =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+        for (int b = 0; b < B; ++b) {
+            const PkState& H = h[b];
+            const InstHost& I = ih[b];
+            int status = I.status;
+            std::string reason = I.reason;
+            if (!H.finite && status != ST_NONFINITE) status = ST_NONFINITE;
+            if (status == ST_CONVERGED && !(H.load <= load_tol && H.fw <= tol && H.pen <= tol)) {
+                status = ST_VERIFICATION_FAILED;
+                reason = "final_check";
+            }
+            if (status == ST_CONVERGED && req_tol < tol && !o.allow_tolerance_relaxation) {
+                if (!(H.fw <= req_tol && H.pen <= req_tol)) {
+                    status = ST_STAGNATED;
+                    reason = "precision_limit";
+                }
+            }
+            aspher_result& R = res[b];
+            std::memset(&R, 0, sizeof(R));
+            R.status = status;
+            std::strncpy(R.status_reason, reason.c_str(), sizeof(R.status_reason) - 1);
+            R.iterations = H.it;
+            R.converged = status == ST_CONVERGED;
+            R.contact_fraction = (double)H.nc / (double)N;
+            R.mean_pressure = H.psum / (double)N;
+            R.approach = H.alpha_ref + I.datum;
+            R.objective = ob[b].red[0] + I.datum * I.P_total;
+            R.error = H.pk;
+            R.pk_error = H.pk;
+            R.fw_gap = H.G;
+            R.fw_error = H.fw;
+            R.load_error = H.load;
+            R.pressure_violation = 0.0;
+            R.penetration_error = H.pen;
+            R.requested_tol = req_tol;
+            R.effective_tol = tol;
+            R.p_ref = I.p_ref;
+            R.g_ref = I.g_ref;
+            R.matvec_count = H.mv;
+            R.precond_count = H.pc;
+            R.identification_steps = I.id_steps;
+            R.returned_best = I.returned_best;
+            R.history_len = b == 0 ? hl : 0;
+            const long long rb = sizeof(T);
+            R.mem_cg_state = 7LL * N * rb;
+            R.mem_best_iterate = o.keep_best ? N * rb : 0;
+            R.mem_contact_mask = N;
+            R.mem_output_arrays = (rb == 8 ? 0 : N * 8LL) + (o.light ? 0 : 2LL * N * 8);
+            R.mem_peak = R.mem_cg_state + R.mem_best_iterate + R.mem_contact_mask +
+                         R.mem_output_arrays;
+            R.time_total = secs;
+        }
     }
 };
 
 template <typename T>
-SolverCtx<T>& get_ctx(Operator& op) {
+SolverCtx<T>& get_ctx(Operator& op, int cap = 1) {
     std::shared_ptr<SolverCtxBase>& slot = sizeof(T) == 8 ? op.ctx_d : op.ctx_f;
-    if (!slot) slot = std::make_shared<SolverCtx<T>>(op);
+    if (!slot || static_cast<SolverCtx<T>&>(*slot).cap < cap) {
+        slot.reset();  // free the smaller workspace first
+        slot = std::make_shared<SolverCtx<T>>(op, cap);
+    }
     return static_cast<SolverCtx<T>&>(*slot);
 }
 
@@ -1190,7 +1500,9 @@ void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
                 int hist_cap, aspher_result& res, cudaStream_t s) {
     Solver<T> S(get_ctx<T>(op), s);
-    S.run(o, (const T*)g0, p_bar, (const T*)p_init, pressure, disp, gap, hist, hist_cap, res);
+    const T* g = (const T*)g0;
+    const T* pi = (const T*)p_init;
+    S.run(o, &g, &p_bar, &pi, &pressure, disp, gap, hist, hist_cap, &res);
 }
 template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*, double,
                                 const void*, double*, double*, double*, double*, int,
@@ -1199,59 +1511,90 @@ template void solve_impl<double>(Operator&, const aspher_solve_opts&, const void
                                  const void*, double*, double*, double*, double*, int,
                                  aspher_result&, cudaStream_t);
 
-
-// FP32 stage + FP64 polish (the reference's float_then_double staging,
-// nested_solve.cpp:871-974, on one level): the gap is centred by its
-// midpoint datum and cast to FP32 on the device, the FP32 PK solve runs to
-// float_tol with FP64 reductions, and -- when polish -- an FP64 PK solve
-// warm-started from that pressure certifies the requested tol.
-void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
-                 const double* p_init, double float_tol, int polish, double* pressure,
-                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
-                 cudaStream_t s) {
-    SolverCtx<double>& cd = get_ctx<double>(op);
-    SolverCtx<float>& cf = get_ctx<float>(op);
+namespace {
+// FP64 min / max / non-finite count of B FP64 gaps (validation before any
+// apply), the FP32 stage's datum and g_ref per instance, and the centred FP32
+// copies of the gaps in the FP32 context.
+void mixed_prepare(Operator& op, const aspher_solve_opts& o, int B, const double* const* g0s,
+                   std::vector<double>& datum, std::vector<double>& gref, cudaStream_t s) {
+    SolverCtx<double>& cd = get_ctx<double>(op, B);
+    SolverCtx<float>& cf = get_ctx<float>(op, B);
     const long N = (long)op.Ns * op.Ns;
-    // FP64 statistics of the gap (validation before any apply)
-    double mm[3];
-    {
-        Solver<double> probe(cd, s);
-        probe.P.N = N;
-        probe.P.Ns = op.Ns;
-        ASB_CUDA(cudaMemcpyAsync(cd.Pd, &probe.P, sizeof(PkParams), cudaMemcpyHostToDevice,
-                                 probe.s));
-        probe.reduce(0, g0, nullptr, nullptr, nullptr, 0.0, mm);
+    datum.assign(B, 0.0);
+    gref.assign(B, 0.0);
+    Solver<double> probe(cd, s, B);
+    for (int b = 0; b < B; ++b) {
+        probe.P[b].N = N;
+        probe.P[b].Ns = op.Ns;
     }
-    if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
-    const double datum = o.datum_mode == ASPHER_DATUM_AUTOMATIC ? mm[0] + 0.5 * (mm[1] - mm[0])
-                                                                 : o.datum;
-    double g_ref = o.g_ref;
-    if (!(g_ref > 0.0)) g_ref = mm[1] - mm[0];
-    if (!(g_ref > 0.0)) g_ref = 1.0;
-    const int grid = red_grid(N);
-    k_center_cast<<<grid, kRedThreads, 0, s>>>(N, cf.g0c, g0, o.datum_mode == ASPHER_DATUM_CALLER ? 0.0 : datum);
-    count_launches(1);
-    float* pinit_f = nullptr;
-    if (p_init) {
-        pinit_f = cf.r;  // scratch: read by the FP32 solve before r is first written
-        k_cast_f32<<<grid, kRedThreads, 0, s>>>(N, pinit_f, p_init);
+    probe.write_params();
+    for (int b = 0; b < B; ++b) {
+        double mm[3];
+        probe.reduce(b, 0, g0s[b], nullptr, nullptr, nullptr, 0.0, mm);
+        if (mm[2] > 0.0) throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
+        datum[b] = o.datum_mode == ASPHER_DATUM_AUTOMATIC ? mm[0] + 0.5 * (mm[1] - mm[0]) : o.datum;
+        double g_ref = o.g_ref;
+        if (!(g_ref > 0.0)) g_ref = mm[1] - mm[0];
+        if (!(g_ref > 0.0)) g_ref = 1.0;
+        gref[b] = g_ref;
+        // on the caller's stream: the FP32 solve's stream waits for it
+        k_center_cast<<<red_grid(N), kRedThreads, 0, s>>>(
+            N, cf.at(cf.g0c, b), g0s[b], o.datum_mode == ASPHER_DATUM_CALLER ? 0.0 : datum[b]);
         count_launches(1);
     }
     ASB_CUDA(cudaGetLastError());
+}
+
+aspher_solve_opts float_stage_opts(const aspher_solve_opts& o, double float_tol, int polish) {
     aspher_solve_opts of = o;
     of.dtype = ASPHER_F32;
     of.tol = float_tol;
     of.requested_tol = polish ? float_tol : (o.requested_tol > 0.0 ? o.requested_tol : o.tol);
     of.allow_tolerance_relaxation = polish ? 1 : o.allow_tolerance_relaxation;
     of.datum_mode = ASPHER_DATUM_CALLER;
-    of.datum = datum;
-    of.g_ref = g_ref;
+    return of;
+}
+
+// the reported work is the sum of both stages (nested_solve.cpp:445-450)
+void add_stage(aspher_result& r, const aspher_result& rf) {
+    r.iterations += rf.iterations;
+    r.matvec_count += rf.matvec_count;
+    r.precond_count += rf.precond_count;
+    r.identification_steps += rf.identification_steps;
+    r.time_total += rf.time_total;
+}
+}  // namespace
+
+// FP32 stage + FP64 polish (the reference's float_then_double staging,
+// nested_solve.cpp:871-974, on one level): the gap is centred by its
+// midpoint datum and cast to FP32 on the device, the FP32 PK solve runs to
+// float_tol with FP64 reductions, and -- when polish -- an FP64 PK solve
+// warm-started from that pressure certifies opts.tol (the caller may ask
+// for a polish tolerance below the requested one).
+void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
+                 const double* p_init, double float_tol, int polish, double* pressure,
+                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
+                 cudaStream_t s) {
+    std::vector<double> datum, gref;
+    mixed_prepare(op, o, 1, &g0, datum, gref, s);
+    SolverCtx<double>& cd = get_ctx<double>(op);
+    SolverCtx<float>& cf = get_ctx<float>(op);
+    const long N = (long)op.Ns * op.Ns;
+    const float* pinit_f = nullptr;
+    if (p_init) {
+        pinit_f = cf.r;  // scratch: read by the FP32 solve before r is first written
+        k_cast_f32<<<red_grid(N), kRedThreads, 0, s>>>(N, cf.r, p_init);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+    }
+    aspher_solve_opts of = float_stage_opts(o, float_tol, polish);
     of.light = polish ? 1 : o.light;
     aspher_result rf;
     {
         Solver<float> S(cf, s);
-        S.run(of, cf.g0c, p_bar, pinit_f, pressure, polish ? nullptr : disp,
-              polish ? nullptr : gap, nullptr, 0, rf);
+        const float* g0f = cf.g0c;
+        S.run(of, &g0f, &p_bar, &pinit_f, &pressure, polish ? nullptr : disp,
+              polish ? nullptr : gap, nullptr, 0, &rf, datum.data(), gref.data());
     }
     if (res_float) *res_float = rf;
     if (!polish) {
@@ -1261,18 +1604,73 @@ void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, dou
     aspher_solve_opts od = o;
     od.dtype = ASPHER_F64;
     od.datum_mode = ASPHER_DATUM_SOLVER;
-    od.datum = datum;
-    od.g_ref = g_ref;
     {
         Solver<double> S(cd, s);
-        S.run(od, g0, p_bar, pressure, pressure, disp, gap, nullptr, 0, res);
+        const double* pw = pressure;
+        S.run(od, &g0, &p_bar, &pw, &pressure, disp, gap, nullptr, 0, &res, datum.data(),
+              gref.data());
     }
-    // the reported work is the sum of both stages (nested_solve.cpp:445-450)
-    res.iterations += rf.iterations;
-    res.matvec_count += rf.matvec_count;
-    res.precond_count += rf.precond_count;
-    res.identification_steps += rf.identification_steps;
-    res.time_total += rf.time_total;
+    add_stage(res, rf);
+}
+
+// Batched solve of B instances sharing the operator and the options, in one
+// loop graph (per-instance gates = convergence masks).
+template <typename T>
+void solve_batch_impl(Operator& op, const aspher_solve_opts& o, int B, const void* const* g0s,
+                      const double* p_bars, const void* const* p_inits, double* const* pressures,
+                      aspher_result* res, cudaStream_t s) {
+    if (B < 1) throw Error(ASPHER_EINVAL, "solve_batch: batch must be >= 1");
+    Solver<T> S(get_ctx<T>(op, B), s, B);
+    aspher_solve_opts ob = o;
+    if (B > 1) ob.light = 1;
+    S.run(ob, reinterpret_cast<const T* const*>(g0s), p_bars,
+          reinterpret_cast<const T* const*>(p_inits), pressures, nullptr, nullptr, nullptr, 0,
+          res);
+}
+template void solve_batch_impl<float>(Operator&, const aspher_solve_opts&, int, const void* const*,
+                                      const double*, const void* const*, double* const*,
+                                      aspher_result*, cudaStream_t);
+template void solve_batch_impl<double>(Operator&, const aspher_solve_opts&, int,
+                                       const void* const*, const double*, const void* const*,
+                                       double* const*, aspher_result*, cudaStream_t);
+
+// Batched FP32 stage + FP64 polish (solve_mixed for B instances).
+void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const double* const* g0s,
+                       const double* p_bars, double float_tol, int polish,
+                       double* const* pressures, aspher_result* res, aspher_result* res_float,
+                       cudaStream_t s) {
+    if (B < 1) throw Error(ASPHER_EINVAL, "solve_batch: batch must be >= 1");
+    std::vector<double> datum, gref;
+    mixed_prepare(op, o, B, g0s, datum, gref, s);
+    SolverCtx<double>& cd = get_ctx<double>(op, B);
+    SolverCtx<float>& cf = get_ctx<float>(op, B);
+    aspher_solve_opts of = float_stage_opts(o, float_tol, polish);
+    of.light = 1;
+    std::vector<aspher_result> rf(B);
+    {
+        Solver<float> S(cf, s, B);
+        std::vector<const float*> gf(B);
+        for (int b = 0; b < B; ++b) gf[b] = cf.at(cf.g0c, b);
+        S.run(of, gf.data(), p_bars, nullptr, pressures, nullptr, nullptr, nullptr, 0, rf.data(),
+              datum.data(), gref.data());
+    }
+    if (res_float)
+        for (int b = 0; b < B; ++b) res_float[b] = rf[b];
+    if (!polish) {
+        for (int b = 0; b < B; ++b) res[b] = rf[b];
+        return;
+    }
+    aspher_solve_opts od = o;
+    od.dtype = ASPHER_F64;
+    od.datum_mode = ASPHER_DATUM_SOLVER;
+    od.light = 1;
+    {
+        Solver<double> S(cd, s, B);
+        std::vector<const double*> pw(pressures, pressures + B);
+        S.run(od, g0s, p_bars, pw.data(), pressures, nullptr, nullptr, nullptr, 0, res,
+              datum.data(), gref.data());
+    }
+    for (int b = 0; b < B; ++b) add_stage(res[b], rf[b]);
 }
 
 // Standalone preconditioner apply: z = M^-1 g on contact, contact-mean removed.
@@ -1283,8 +1681,8 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     PkState* st = nullptr;
     double* part = nullptr;
     ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
-    ASB_CUDA(cudaMallocAsync((void**)&part, kMaxBlocks * 8 * sizeof(double), s));
-    ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));
+    ASB_CUDA(cudaMallocAsync((void**)&part, kPartStride * sizeof(double), s));
+    ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));  // alpha = 0: g used as given
     PkParams P{};
     P.N = N;
     P.Ns = op.Ns;
@@ -1314,5 +1712,304 @@ template void precond_apply_impl<float>(Operator&, int, int, const float*, const
                                         cudaStream_t);
 template void precond_apply_impl<double>(Operator&, int, int, const double*, const uint8_t*,
                                          double*, cudaStream_t);
+
+// ---- adjoint of a converged solve ------------------------------------------------
+// No reference counterpart.  At a converged solve with contact set
+// C = {p > 0} the KKT system restricted to C,
+//     S_CC p_C - alpha 1 = -g0_C,   1^T p_C = P,
+// is linear in (g0, P), so for a loss L(p) with w = dL/dp the adjoint pair
+// (lam, mu) solves the symmetric system
+//     S_CC lam - mu 1 = w_C,   1^T lam = 0,
+// and dL/dg0 = -lam on C (0 off C), dL/dP = -mu, dL/dp_bar = -mu N.  lam is
+// found by CG on V = {x : x = 0 off C, sum_C x = 0} with the projected
+// operator Pi S Pi and the projected stencil preconditioner (the PK solve's
+// own Pi M Pi); mu = mean_C(S lam - w) once lam has converged.  Nothing of
+// the forward iterates is needed (they are not stored).
+//
+// The state reuses PkState: nc / gcs (= 0) / zmean / pc for the stencil
+// kernel, halt / it / status for the loop, G_old = previous r.z, beta,
+// tau = step length, gg = |r|^2, total = |r0|^2, rmean = contact mean of q,
+// alpha = contact mean of w.
+namespace {
+
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_init(const PkParams* __restrict__ Pp, PkState* st,
+                                                          const double* p, const double* w,
+                                                          uint8_t* mask, T* wT, double* part) {
+    const PkParams& P = *Pp;
+    double acc[2] = {0.0, 0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P.N; i += (long)gridDim.x * blockDim.x) {
+        const bool c = p[i] > 0.0;
+        const T wi = (T)w[i];
+        mask[i] = c ? 1 : 0;
+        wT[i] = wi;
+        if (c) { acc[0] += (double)wi; acc[1] += 1.0; }
+    }
+    const int kinds[2] = {0, 0};
+    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[0]) && threadIdx.x == 0) {
+        st->nc = (int)acc[1];
+        st->alpha = st->nc ? acc[0] / st->nc : 0.0;
+        st->gcs = 0.0;
+        st->halt = st->nc < 2 ? H_FINAL : H_RUN;
+        st->status = st->nc < 2 ? ST_NONPOSITIVE_CURVATURE : ST_MAX_ITERATIONS;
+    }
+}
+
+// r = Pi w, lam = d = 0, |r0|^2
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_r0(const PkParams* __restrict__ Pp, PkState* st,
+                                                        const uint8_t* mask, const T* wT, T* r,
+                                                        T* lam, T* d, double* part) {
+    const PkParams& P = *Pp;
+    const T wm = (T)st->alpha;
+    double acc[1] = {0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P.N; i += (long)gridDim.x * blockDim.x) {
+        const T ri = mask[i] ? (T)(wT[i] - wm) : T(0);
+        r[i] = ri;
+        lam[i] = T(0);
+        d[i] = T(0);
+        acc[0] += (double)ri * (double)ri;
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[1]) && threadIdx.x == 0) {
+        st->total = acc[0];
+        st->gg = acc[0];
+        st->it = 0;
+        st->G_old = 0.0;
+        if (!(acc[0] > 0.0)) {  // w is constant on C: lam = 0 solves exactly
+            st->status = ST_CONVERGED;
+            st->halt = H_FINAL;
+        }
+    }
+}
+
+// rz = <Pi z, r>, beta = rz / rz_old; z = r when unpreconditioned
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_rz(const PkParams* __restrict__ Pp, PkState* st,
+                                                        const T* z, const T* r,
+                                                        const uint8_t* mask, double* part) {
+    const PkParams& P = *Pp;
+    if (st->halt) return;
+    const T zm = (T)st->zmean;
+    double acc[1] = {0.0};
+    GRID_LOOP4(P.N) {
+        T zz[4], rr[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(r, i4, rr);
+        ldp4(z, i4, zz);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (mm[j]) acc[0] += (double)(T)(zz[j] - zm) * (double)rr[j];
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[3]) && threadIdx.x == 0) {
+        st->beta = (st->it > 0 && st->G_old != 0.0) ? (double)(T)(acc[0] / st->G_old) : 0.0;
+        st->G_old = acc[0];
+        if (!(acc[0] > 0.0) || !isfinite(acc[0])) {  // preconditioner lost definiteness
+            st->status = isfinite(acc[0]) ? ST_NONPOSITIVE_CURVATURE : ST_NONFINITE;
+            st->halt = H_FINAL;
+        }
+    }
+}
+
+// d = Pi z + beta d on C
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_d(const PkParams* __restrict__ Pp, const PkState* st,
+                                                       const T* z, const uint8_t* mask, T* d) {
+    const PkParams& P = *Pp;
+    if (st->halt) return;
+    const T zm = (T)st->zmean, beta = (T)st->beta;
+    GRID_LOOP4(P.N) {
+        T zz[4], dd[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(z, i4, zz);
+        ldp4(d, i4, dd);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dd[j] = mm[j] ? (T)((T)(zz[j] - zm) + beta * dd[j]) : T(0);
+        st4(d, i4, dd);
+    }
+}
+
+// a = rz / <d, q>, qm = contact mean of q (q = S d)
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_dq(const PkParams* __restrict__ Pp, PkState* st,
+                                                        const T* d, const T* q,
+                                                        const uint8_t* mask, double* part) {
+    const PkParams& P = *Pp;
+    if (st->halt) return;
+    double acc[2] = {0.0, 0.0};
+    GRID_LOOP4(P.N) {
+        T dd[4], qq[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(d, i4, dd);
+        ldp4(q, i4, qq);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (mm[j]) { acc[0] += (double)dd[j] * (double)qq[j]; acc[1] += (double)qq[j]; }
+    }
+    const int kinds[2] = {0, 0};
+    if (grid_reduce_last<2>(acc, kinds, part, &st->counter[4]) && threadIdx.x == 0) {
+        st->rmean = (double)(T)(acc[1] / st->nc);
+        if (acc[0] > 0.0 && isfinite(acc[0])) {
+            st->tau = (double)(T)(st->G_old / acc[0]);
+        } else {
+            st->status = isfinite(acc[0]) ? ST_NONPOSITIVE_CURVATURE : ST_NONFINITE;
+            st->halt = H_FINAL;
+        }
+    }
+}
+
+// lam += a d; r -= a Pi q; convergence |r| <= tol |r0|
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_upd(const PkParams* __restrict__ Pp, PkState* st,
+                                                         const T* d, const T* q,
+                                                         const uint8_t* mask, T* lam, T* r,
+                                                         double* part) {
+    const PkParams& P = *Pp;
+    if (st->halt) return;
+    const T a = (T)st->tau, qm = (T)st->rmean;
+    double acc[1] = {0.0};
+    GRID_LOOP4(P.N) {
+        T dd[4], qq[4], ll[4], rr[4];
+        uint8_t mm[4];
+        ldm4(mask, i4, mm);
+        ldp4(d, i4, dd);
+        ldp4(q, i4, qq);
+        ldp4(lam, i4, ll);
+        ldp4(r, i4, rr);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!mm[j]) { rr[j] = T(0); continue; }
+            ll[j] = ll[j] + a * dd[j];
+            rr[j] = rr[j] - a * (T)(qq[j] - qm);
+            acc[0] += (double)rr[j] * (double)rr[j];
+        }
+        st4(lam, i4, ll);
+        st4(r, i4, rr);
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[5]) && threadIdx.x == 0) {
+        st->gg = acc[0];
+        st->it++;
+        if (!isfinite(acc[0])) {
+            st->status = ST_NONFINITE;
+            st->halt = H_FINAL;
+        } else if (acc[0] <= P.tol * P.tol * st->total) {
+            st->status = ST_CONVERGED;
+            st->halt = H_FINAL;
+        } else if (st->it >= P.max_iter) {
+            st->halt = H_FINAL;
+        }
+    }
+}
+
+// mu = mean_C(S lam - w); grad_g0 = -lam on C (0 off C), FP64
+template <typename T>
+__global__ void __launch_bounds__(kRedThreads) k_adj_out(const PkParams* __restrict__ Pp, PkState* st,
+                                                         const T* q, const T* wT, const T* lam,
+                                                         const uint8_t* mask, double* grad,
+                                                         double* part) {
+    const PkParams& P = *Pp;
+    double acc[1] = {0.0};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < P.N; i += (long)gridDim.x * blockDim.x) {
+        const bool c = mask[i] != 0;
+        grad[i] = c ? -(double)lam[i] : 0.0;
+        if (c) acc[0] += (double)q[i] - (double)wT[i];
+    }
+    const int kinds[1] = {0};
+    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[6]) && threadIdx.x == 0)
+        st->red[0] = st->nc ? acc[0] / st->nc : 0.0;
+}
+
+}  // namespace
+
+template <typename T>
+void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
+                  int precond, int radius, double* grad_g0, double* grad_pbar,
+                  aspher_adjoint_info* info, cudaStream_t s) {
+    if (!(tol > 0.0)) throw Error(ASPHER_EINVAL, "adjoint: tol must be positive");
+    if (max_iter < 1) throw Error(ASPHER_EINVAL, "adjoint: max_iter must be >= 1");
+    if (precond != ASPHER_PRECOND_NONE && precond != ASPHER_PRECOND_STENCIL)
+        throw Error(ASPHER_EINVAL, "adjoint: precond must be NONE or STENCIL");
+    const auto t0 = std::chrono::steady_clock::now();
+    const long N = (long)op.Ns * op.Ns;
+    const size_t vb = (size_t)N * sizeof(T);
+    StencilTaps taps{};
+    if (precond == ASPHER_PRECOND_STENCIL) taps = make_stencil_taps(op.Ns, radius);
+    T *wT = nullptr, *r = nullptr, *z = nullptr, *d = nullptr, *q = nullptr, *lam = nullptr;
+    uint8_t* mask = nullptr;
+    double* part = nullptr;
+    PkState* st = nullptr;
+    PkParams* Pd = nullptr;
+    T** vecs[] = {&wT, &r, &z, &d, &q, &lam};
+    for (T** v : vecs) ASB_CUDA(cudaMallocAsync((void**)v, vb, s));
+    ASB_CUDA(cudaMallocAsync((void**)&mask, (size_t)N, s));
+    ASB_CUDA(cudaMallocAsync((void**)&part, kPartStride * sizeof(double), s));
+    ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
+    ASB_CUDA(cudaMallocAsync((void**)&Pd, sizeof(PkParams), s));
+    ASB_CUDA(cudaMemsetAsync(st, 0, sizeof(PkState), s));
+    PkParams P{};
+    P.N = N;
+    P.Ns = op.Ns;
+    P.tol = tol;
+    P.max_iter = max_iter;
+    P.precond = precond;
+    ASB_CUDA(cudaMemcpyAsync(Pd, &P, sizeof(P), cudaMemcpyHostToDevice, s));
+    const int grid = red_grid(N);
+    k_adj_init<T><<<grid, kRedThreads, 0, s>>>(Pd, st, p, w, mask, wT, part);
+    k_adj_r0<T><<<grid, kRedThreads, 0, s>>>(Pd, st, mask, wT, r, lam, d, part);
+    count_launches(2);
+    ASB_CUDA(cudaGetLastError());
+    PkState h{};
+    auto read = [&]() {
+        ASB_CUDA(cudaMemcpyAsync(&h, st, sizeof(h), cudaMemcpyDeviceToHost, s));
+        ASB_CUDA(cudaStreamSynchronize(s));
+    };
+    read();
+    while (h.halt == H_RUN) {
+        for (int k = 0; k < 16; ++k) {  // kernels return at entry once halted
+            const T* zz = r;
+            if (precond == ASPHER_PRECOND_STENCIL) {
+                k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, r, mask, z, part, 1);
+                zz = z;
+                count_launches(1);
+            }
+            k_adj_rz<T><<<grid, kRedThreads, 0, s>>>(Pd, st, zz, r, mask, part);
+            k_adj_d<T><<<grid, kRedThreads, 0, s>>>(Pd, st, zz, mask, d);
+            op.matvec(sizeof(T) == 8, d, q, s, &st->halt);
+            k_adj_dq<T><<<grid, kRedThreads, 0, s>>>(Pd, st, d, q, mask, part);
+            k_adj_upd<T><<<grid, kRedThreads, 0, s>>>(Pd, st, d, q, mask, lam, r, part);
+            count_launches(4);
+        }
+        ASB_CUDA(cudaGetLastError());
+        read();
+    }
+    op.matvec(sizeof(T) == 8, lam, q, s, nullptr);
+    k_adj_out<T><<<grid, kRedThreads, 0, s>>>(Pd, st, q, wT, lam, mask, grad_g0, part);
+    count_launches(1);
+    ASB_CUDA(cudaGetLastError());
+    read();
+    const double mu = h.red[0];
+    if (grad_pbar) *grad_pbar = -mu * (double)N;
+    if (info) {
+        std::memset(info, 0, sizeof(*info));
+        info->status = h.status;
+        info->iterations = h.it;
+        info->residual = h.total > 0.0 ? std::sqrt(h.gg / h.total) : 0.0;
+        info->contact_count = h.nc;
+        info->mu = mu;
+        info->time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    void* all[] = {wT, r, z, d, q, lam, mask, part, st, Pd};
+    for (void* v : all) cudaFreeAsync(v, s);
+    ASB_CUDA(cudaStreamSynchronize(s));
+}
+template void adjoint_impl<float>(Operator&, const double*, const double*, double, int, int, int,
+                                  double*, double*, aspher_adjoint_info*, cudaStream_t);
+template void adjoint_impl<double>(Operator&, const double*, const double*, double, int, int, int,
+                                   double*, double*, aspher_adjoint_info*, cudaStream_t);
 
 }  // namespace asb

@@ -17,14 +17,27 @@ struct StencilTaps {
 };
 StencilTaps make_stencil_taps(int Ns, int R);
 
-// Full-grid |k| preconditioner inside a PK solve: centre g on the contact
-// mask by st->gcs / st->nc, transform, multiply by |k|/Ns^2 (FP32 table
-// values, fourier_precond.cpp:12-28), gather on contact into z and leave
-// T(contact mean of z) in st->zmean (st->pc incremented).  Kernels return at
-// entry when gate != nullptr and *gate != 0.  Defined in operators.cu.
+// Full-grid |k| preconditioner inside a PK solve: centre g (held as v and
+// centred by Real(st->alpha) on the fly) on the contact mask by
+// st->gcs / st->nc, transform, multiply by |k|/Ns^2 (FP32 table values,
+// fourier_precond.cpp:12-28), gather on contact into z and leave T(contact
+// mean of z) in st->zmean (st->pc incremented).  Kernels return at entry
+// when gate != nullptr and gate[b * kGateStride] != 0 (instance b of B;
+// spec: B spectra, or nullptr for the operator's own when B = 1).
+// Defined in operators.cu.
 template <typename T>
 void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
-                        double* part, cudaStream_t s, const int* gate);
+                        double* part, cudaStream_t s, const int* gate, int B = 1,
+                        void* spec = nullptr);
+
+// r = S t of the PK loop with the direction update t = chi_C(z_f + beta t)
+// (and g_prev = g, best = p when copy_best) fused into the forward row load
+// and the rsum / num / den sums of r fused into the inverse row store; r is
+// not written.  Defined in operators.cu (functors in pk_fused.cuh).
+template <typename T>
+void pk_apply_t(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
+                const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
+                const int* gate, int B = 1, void* spec = nullptr);
 
 template <typename T>
 void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
@@ -42,6 +55,20 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
                   int stage_cap, int* nstages, cudaStream_t s);
 bool stencil_for_level(int engine, bool precond, double prev_occupancy, double occupancy_max);
 void clear_operator_cache();
+
+template <typename T>
+void solve_batch_impl(Operator& op, const aspher_solve_opts& o, int B, const void* const* g0s,
+                      const double* p_bars, const void* const* p_inits, double* const* pressures,
+                      aspher_result* res, cudaStream_t s);
+void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const double* const* g0s,
+                       const double* p_bars, double float_tol, int polish,
+                       double* const* pressures, aspher_result* res, aspher_result* res_float,
+                       cudaStream_t s);
+
+template <typename T>
+void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
+                  int precond, int radius, double* grad_g0, double* grad_pbar,
+                  aspher_adjoint_info* info, cudaStream_t s);
 
 template <typename T>
 void precond_apply_impl(Operator& op, int precond, int radius, const T* g, const uint8_t* mask,

@@ -42,11 +42,12 @@ struct PkParams {
     double load_tol;
     double p_bar;
     double gshift;  // datum subtracted on the fly (0 in caller mode)
+    long hist_stride;  // history entries per instance (batched solves)
 };
 
 struct PkState {
     // evaluate() -- contact_solver.cpp:260-303
-    double alpha, gmin;  // alpha: one-pass mean (used to centre g); refined below
+    double alpha, gmin;  // alpha: one-pass mean (g is centred by Real(alpha)); refined below
     double alpha_ref, gmin_ref;
     double gsum, vmin;
     double pk, G, fw, pen, psum, pv, load, gcs;
@@ -61,9 +62,10 @@ struct PkState {
     int copy_best, have_best;
     int status;
     int fill;  // total <= 0 -> p = p_bar
+    int pk_due;  // k_eval ran; k_evalpk records this iteration's pk
     double best_merit, seen_merit;
     // CG recurrences
-    double G_old, delta, beta, gg;
+    double G_old, delta, beta, gg, bv;  // bv: PR+ / FR ratio before the delta gate
     double zmean;  // preconditioner output contact mean
     double rsum, num, rmean, den, tau, tau_ov;
     double total, scale;

@@ -9,8 +9,13 @@
 namespace asb {
 
 constexpr int kRedThreads = 256;
-// upper bound on the grid of any reducing kernel (sizes the partials buffer)
+// upper bound on the grid of the vector-pass reducing kernels
 constexpr int kMaxBlocks = 1184;
+// partials per instance of a batched solve: 8 values for the largest grid of
+// any reducing kernel -- the row kernels of an 8192-row transform run up to
+// 8192 blocks (reductions fused into their stores)
+constexpr int kMaxRowBlocks = 8192;
+constexpr int kPartStride = kMaxRowBlocks * 8;
 
 template <int NV>
 __device__ __forceinline__ void ident_init(double (&v)[NV], const int (&kinds)[NV]) {

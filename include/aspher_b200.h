@@ -223,6 +223,47 @@ int aspher_solve_mixed(aspher_op* op, const aspher_solve_opts* opts, const doubl
                        double* pressure_dev, double* displacement_dev, double* gap_dev,
                        aspher_result* res, aspher_result* res_float, void* stream);
 
+/* Batched solves: `batch` independent problems on the same operator and
+ * options (per-problem gap, p_bar, warm start and pressure output) solved
+ * together, every kernel of the loop launched once for the whole batch with
+ * one CUDA-graph loop and per-problem convergence masks.  Each problem's
+ * result is the result aspher_solve / aspher_solve_mixed would return for it
+ * alone, up to reduction order.  Arrays of pointers live in host memory and
+ * point to device fields; outputs are pressures only (light).  No reference
+ * counterpart (the reference solves one problem per call).  Synchronous. */
+int aspher_solve_batch(aspher_op* op, const aspher_solve_opts* opts, int batch,
+                       const void* const* g0_devs, const double* p_bars,
+                       const void* const* p_init_devs, double* const* pressure_devs,
+                       aspher_result* res, void* stream);
+int aspher_solve_batch_mixed(aspher_op* op, const aspher_solve_opts* opts, int batch,
+                             const double* const* g0_devs, const double* p_bars, double float_tol,
+                             int polish, double* const* pressure_devs, aspher_result* res,
+                             aspher_result* res_float, void* stream);
+
+/* ---- adjoint of a converged solve ------------------------------------------ */
+/* No reference counterpart (the reference has no derivative of the solve).
+ * With C = {p > 0} the contact set of a converged solve of (op, g0, p_bar)
+ * and w = dL/dp, solves  S_CC lam - mu 1 = w_C,  sum_C lam = 0  by CG on the
+ * contact set (the same operator; optional stencil preconditioner) and
+ * returns dL/dg0 = -lam (0 off C) and dL/dp_bar = -mu N.  p_dev, w_dev and
+ * grad_g0_dev are FP64 device fields of N entries; dtype (ASPHER_F32 /
+ * ASPHER_F64) is the working precision of the CG (reductions always FP64).
+ * tol: relative residual |r| <= tol |r0|.  Synchronous. */
+typedef struct {
+    int status;        /* aspher_status: CONVERGED, MAX_ITERATIONS, ... */
+    int iterations;
+    int contact_count; /* |C| */
+    int reserved;
+    double residual;   /* final |r| / |r0| */
+    double mu;         /* the load multiplier */
+    double time;       /* seconds */
+} aspher_adjoint_info;
+
+int aspher_adjoint(aspher_op* op, int dtype, const double* p_dev, const double* w_dev,
+                   double tol, int max_iter, int precond, int precond_radius,
+                   double* grad_g0_dev, double* grad_pbar, aspher_adjoint_info* info,
+                   void* stream);
+
 /* Allocation-free doubly periodic apply, y = S x (no counterpart in the
  * reference).  For callers that cannot allocate device memory: real-time
  * loops that must not block in the allocator, and applications whose own
