@@ -6,7 +6,7 @@
 // double}; every reduction is accumulated in FP64 as in the reference.
 //
 // One CG iteration is the kernel sequence
-//   [apply p->u] eval [evalpk] stencil+dots [apply t->r, tupd / rden fused] pupd rescale
+//   [apply p->u] eval [evalpk] stencil+dots tupd [apply t->r] rden pupd rescale
 // where each pass is one HBM sweep and each reduction's scalar logic runs in
 // the last block of its pass (see pk_state.hpp).  The loop is a CUDA graph
 // with a while node; once a pass sets `halt`, the rest of the iteration is a
@@ -439,8 +439,9 @@ __global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict
     }
 }
 
-// Direction update and r sums as separate passes around a plain apply (the
-// ASPHER_UNFUSED_T=1 form of pk_apply_t, kept for A/B timing).
+// Direction update t = chi_C(z_f + beta t), g_prev = g (and best = p when
+// copy_best) before the t apply; k_rden consumes r after it.  pk_apply_t is
+// the same pair fused into the apply's row kernels (ASPHER_FUSED_T=1).
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, T* gprev, T* t,
@@ -899,7 +900,7 @@ struct SolverCtx : SolverCtxBase {
     // one CG iteration of B instances (the common path), every pass gated
     // per instance on the device:
     //   [apply p->u] eval (evalpk) | stencil+dots  or  [precond] dots |
-    //   [apply t->r with the direction update and the r sums fused] pupd rescale
+    //   tupd [apply t->r] rden | pupd rescale
     void enqueue_iteration(cudaStream_t s, int B) {
         const dim3 gr(grid, B);
         int n = 0;
@@ -921,14 +922,14 @@ struct SolverCtx : SolverCtxBase {
             k_dots<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
             ++n;
         }
-        if (unfused_t()) {
+        if (fused_t()) {
+            pk_apply_t<T>(op, z, g, gprev, t, mask, p, best, st, part, precond, s, &st->halt, B,
+                          B > 1 ? spec : nullptr);
+        } else {
             k_tupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
             apply(t, r, &st->halt, s, B);
             k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
             n += 2;
-        } else {
-            pk_apply_t<T>(op, z, g, gprev, t, mask, p, best, st, part, precond, s, &st->halt, B,
-                          B > 1 ? spec : nullptr);
         }
         k_pupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
         k_rescale<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, part);
@@ -996,11 +997,14 @@ struct SolverCtx : SolverCtxBase {
         }();
         return e;
     }
-    // ASPHER_UNFUSED_T=1: direction update and r sums as separate passes
-    // around a plain apply (A/B timing of the fused t-apply)
-    static bool unfused_t() {
+    // ASPHER_FUSED_T=1: the direction update and the r sums inside the row
+    // kernels of the t apply (pk_apply_t) instead of two streaming passes
+    // around a plain apply.  Off by default: the row kernels are latency-bound
+    // and the extra loads in them cost more than the passes they save
+    // (measured on B200 at Ns=2048: 1-2 % slower per solve).
+    static bool fused_t() {
         static const bool e = [] {
-            const char* v = std::getenv("ASPHER_UNFUSED_T");
+            const char* v = std::getenv("ASPHER_FUSED_T");
             return v && v[0] == '1';
         }();
         return e;
