@@ -144,13 +144,98 @@ __host__ __device__ constexpr bool col_fits(int LC) {
     return col_smem<T>(LC, 1) <= kSmemPerSM;
 }
 
+// ---- software pipeline ----------------------------------------------------------
+// The pass kernels are persistent: a CTA walks row groups (or column tiles)
+// blockIdx.x, blockIdx.x + gridDim.x, ...  When the input of a unit is a
+// plain contiguous block (raw rows, tiled spectrum chunks, a column tile) and
+// a staging buffer fits beside the FFT workspace, the next unit's input is
+// copied global -> shared with cp.async while the current unit is being
+// transformed, so the load latency of one unit hides behind the arithmetic
+// of the previous one.  The waits are the hardware's own (cp.async.wait_all):
+// no software spin.
+__host__ __device__ constexpr int align16(int b) { return (b + 15) & ~15; }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+// one complex element global -> shared (8 or 16 bytes)
+template <typename T>
+__device__ __forceinline__ void cp_async_cplx(cplx<T>* smem, const cplx<T>* gmem) {
+    if constexpr (sizeof(cplx<T>) == 16) cp_async16(smem, gmem);
+    else cp_async8(smem, gmem);
+}
+
+// Row forward: staging of RB raw rows (Ns reals each) for loads that expose
+// contiguous rows (Load::kRaw).
+template <typename T, int LR, bool PAD, int V>
+__host__ __device__ constexpr int row_fwd_stage_bytes() {
+    return row_rb_v<T>(LR, V) * (PAD ? LR : 2 * LR) * (int)sizeof(T);
+}
+template <typename T, int LR, bool PAD, int V, bool RAW>
+__host__ __device__ constexpr bool row_fwd_staged() {
+    return RAW && (PAD ? LR : 2 * LR) % (16 / (int)sizeof(T)) == 0 &&
+           (align16(row_smem_v<T>(LR, V)) + row_fwd_stage_bytes<T, LR, PAD, V>()) *
+                   row_minb<T>(LR, V) <= kSmemPerSM;
+}
+template <typename T, int LR, bool PAD, int V, class Load>
+__host__ __device__ constexpr int row_fwd_smem() {
+    return row_fwd_staged<T, LR, PAD, V, Load::kRaw>()
+               ? align16(row_smem_v<T>(LR, V)) + row_fwd_stage_bytes<T, LR, PAD, V>()
+               : row_smem_v<T>(LR, V);
+}
+// Row inverse: staging of RB half-spectrum rows in the workspace's padded
+// layout for tiled loads (Load::kTiled).
+template <typename T, int LR, int V, bool TILED>
+__host__ __device__ constexpr bool row_inv_staged() {
+    return TILED && (align16(row_smem_v<T>(LR, V)) + row_smem_v<T>(LR, V)) * row_minb<T>(LR, V) <=
+                        kSmemPerSM;
+}
+template <typename T, int LR, int V, class Load>
+__host__ __device__ constexpr int row_inv_smem() {
+    return row_inv_staged<T, LR, V, Load::kTiled>()
+               ? align16(row_smem_v<T>(LR, V)) + row_smem_v<T>(LR, V)
+               : row_smem_v<T>(LR, V);
+}
+// Column: staging of one tile (its stored rows x CT columns, contiguous).
+template <typename T, int LC, int NCM1, bool PAD, int V>
+__host__ __device__ constexpr int col_stage_bytes() {
+    return (PAD ? LC / 2 : LC) * col_ct_v<T>(LC, NCM1, V) * (int)sizeof(cplx<T>);
+}
+template <typename T, int LC, int NCM1, bool PAD, int V>
+__host__ __device__ constexpr bool col_staged() {
+    return (align16(col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V))) +
+            col_stage_bytes<T, LC, NCM1, PAD, V>()) *
+               col_minb<T>(LC, NCM1, V) <= kSmemPerSM;
+}
+template <typename T, int LC, int NCM1, bool PAD, int V>
+__host__ __device__ constexpr int col_smem_total() {
+    return col_staged<T, LC, NCM1, PAD, V>()
+               ? align16(col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V))) +
+                     col_stage_bytes<T, LC, NCM1, PAD, V>()
+               : col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V));
+}
+
 // ---- row forward ---------------------------------------------------------------
-// Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1])
+// Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1]);
+//        static constexpr bool kRaw: true when x / pitch / bs expose plain
+//        contiguous rows (then the kernel stages them with cp.async)
 // Store: void operator()(int row, int k, cplx<T> X), k in [0, LR]
 //        static constexpr bool kTiled: true for the tiled half-spectrum store
 //        (then the kernel writes whole tile chunks through base / nrows / ct /
 //        bs itself); static constexpr bool kFinish: when true, every thread
-//        calls finish(double* scratch) after a __syncthreads() at the end
+//        calls finish(double* scratch) once, after a __syncthreads() at the end
+// Dynamic shared memory: row_fwd_smem<T, LR, PAD, V, Load>().
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 __global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
@@ -158,19 +243,29 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
     if (gate && gate[blockIdx.y * kGateStride]) return;
     constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
+    constexpr int RB = row_rb_v<T>(LR, V);
+    constexpr bool STAGED = row_fwd_staged<T, LR, PAD, V, Load::kRaw>();
+    constexpr int NREAL = PAD ? LR : 2 * LR;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    T* stg = reinterpret_cast<T*>(smraw + align16(row_smem_v<T>(LR, V)));
     const int r = threadIdx.x / TT, t = threadIdx.x % TT;
-    const int row = blockIdx.x * row_rb_v<T>(LR, V) + r;
-    const bool valid = row < nrows;
     const int off = r * sm_len(LR + 1);
-    cplx<T> v[RPT];
-#pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-        else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
-    }
-    block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
+    const int ngroups = (nrows + RB - 1) / RB;
+    auto issue = [&](int grp) {  // the group's rows -> stg (cp.async)
+        if constexpr (STAGED) {
+            constexpr int PER = 16 / (int)sizeof(T);
+            constexpr int VPR = NREAL / PER;  // 16-byte vectors per row
+            const int row0 = grp * RB;
+            const int nr = nrows - row0 < RB ? nrows - row0 : RB;
+            const T* src = ld.x + blockIdx.y * ld.bs + (size_t)row0 * ld.pitch;
+            for (int f = threadIdx.x; f < nr * VPR; f += blockDim.x) {
+                const int rr = f / VPR, e = (f - rr * VPR) * PER;
+                cp_async16(stg + rr * NREAL + e, src + (size_t)rr * ld.pitch + e);
+            }
+            cp_async_commit();
+        }
+    };
     // split step of the real transform: X[k] = E + w^k O with
     // E = (Z[k] + conj Z[-k])/2, O = (Z[k] - conj Z[-k])/(2i), k in [0, LR]
     auto split = [&](cplx<T> zk, cplx<T> zn, int k) {
@@ -180,48 +275,74 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         const cplx<T> w = __ldg(&tw_2lr[k]);
         return cadd(cscale(A, T(0.5)), cmul(w, O));
     };
+    int grp = blockIdx.x;
+    if (grp < ngroups) issue(grp);
+    for (; grp < ngroups; grp += gridDim.x) {
+        const int row = grp * RB + r;
+        const bool valid = row < nrows;
+        cplx<T> v[RPT];
+        if constexpr (STAGED) {
+            cp_async_wait_all();
+            __syncthreads();
+            const cplx<T>* srow = reinterpret_cast<const cplx<T>*>(stg + r * NREAL);
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
-    __syncthreads();
-    if constexpr (Store::kTiled) {
-        // each output reads Z[k] and Z[-k] from shared memory and goes straight
-        // to its tile chunk (RB rows x ct columns, contiguous in HBM)
-        constexpr int RB = row_rb_v<T>(LR, V);
-        const int row0 = blockIdx.x * RB;
-        const int nr = nrows - row0 < RB ? nrows - row0 : RB;
-        const int ct = st.ct;
-        const int chunk = nr * ct;
-        const int ntiles = LR / ct + 1;
-        const int lct = __ffs(ct) - 1;  // ct is a power of two
-        const bool full = nr == RB;
-        const int lchunk = lct + ilog2c(RB);
-        cplx<T>* base = st.base + blockIdx.y * st.bs + (size_t)row0 * ct;
-        for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
-            const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
-            const int rr = e >> lct, c = e & (ct - 1);
-            const int k = j * ct + c;
-            if (k > LR) continue;
-            const int o = rr * sm_len(LR + 1);
-            const cplx<T> zk = sm[smaddr(k & (LR - 1), 1, o)];
-            cplx<T> X;
-            if (k == LR) {
-                X = mk<T>(zk.x - zk.y, T(0));  // zk = Z[0]
-            } else {
-                X = split(zk, sm[smaddr((LR - k) & (LR - 1), 1, o)], k);
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = valid ? srow[t + m * TT] : mk<T>(0, 0);
             }
-            base[(size_t)j * st.nrows * ct + e] = X;
-        }
-    } else {
-        const cplx<T> z0 = v[0];
+            __syncthreads();
+            if (grp + (int)gridDim.x < ngroups) issue(grp + gridDim.x);
+        } else {
 #pragma unroll
-        for (int m = 0; m < RPT; ++m) {
-            const int k = t + m * TT;
-            v[m] = split(v[m], sm[smaddr((LR - k) & (LR - 1), 1, off)], k);
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
+            }
         }
+        block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
 #pragma unroll
-        for (int m = 0; m < RPT; ++m)
-            if (valid) st(row, t + m * TT, v[m]);
-        if (t == 0 && valid) st(row, LR, mk<T>(z0.x - z0.y, T(0)));
+        for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
+        __syncthreads();
+        if constexpr (Store::kTiled) {
+            // each output reads Z[k] and Z[-k] from shared memory and goes
+            // straight to its tile chunk (RB rows x ct columns, contiguous)
+            const int row0 = grp * RB;
+            const int nr = nrows - row0 < RB ? nrows - row0 : RB;
+            const int ct = st.ct;
+            const int chunk = nr * ct;
+            const int ntiles = LR / ct + 1;
+            const int lct = __ffs(ct) - 1;  // ct is a power of two
+            const bool full = nr == RB;
+            const int lchunk = lct + ilog2c(RB);
+            cplx<T>* base = st.base + blockIdx.y * st.bs + (size_t)row0 * ct;
+            for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
+                const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+                const int rr = e >> lct, c = e & (ct - 1);
+                const int k = j * ct + c;
+                if (k > LR) continue;
+                const int o = rr * sm_len(LR + 1);
+                const cplx<T> zk = sm[smaddr(k & (LR - 1), 1, o)];
+                cplx<T> X;
+                if (k == LR) {
+                    X = mk<T>(zk.x - zk.y, T(0));  // zk = Z[0]
+                } else {
+                    X = split(zk, sm[smaddr((LR - k) & (LR - 1), 1, o)], k);
+                }
+                base[(size_t)j * st.nrows * ct + e] = X;
+            }
+        } else {
+            const cplx<T> z0 = v[0];
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                const int k = t + m * TT;
+                v[m] = split(v[m], sm[smaddr((LR - k) & (LR - 1), 1, off)], k);
+            }
+#pragma unroll
+            for (int m = 0; m < RPT; ++m)
+                if (valid) st(row, t + m * TT, v[m]);
+            if (t == 0 && valid) st(row, LR, mk<T>(z0.x - z0.y, T(0)));
+        }
+        __syncthreads();  // the workspace is rewritten by the next group
     }
     if constexpr (Store::kFinish) {
         __syncthreads();
@@ -231,9 +352,11 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 
 // ---- row inverse ----------------------------------------------------------------
 // Load:  cplx<T> operator()(int row, int k), k in [0, LR]; kTiled as for the
-//        forward store (whole tile chunks into shared memory)
+//        forward store (whole tile chunks, staged with cp.async when the
+//        staging buffer fits)
 // Store: void operator()(int row, int n, cplx<T> z) -> (x[2n], x[2n+1]);
 //        static constexpr bool kFinish (see row_fwd_kernel)
+// Dynamic shared memory: row_inv_smem<T, LR, V, Load>().
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 __global__ void __launch_bounds__(row_threads<T>(LR, V), row_minb<T>(LR, V))
 row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
@@ -241,52 +364,77 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
     if (gate && gate[blockIdx.y * kGateStride]) return;
     constexpr int RPT = row_rpt<T>(LR, V);
     constexpr int TT = LR / RPT;
+    constexpr int RB = row_rb_v<T>(LR, V);
+    constexpr bool STAGED = row_inv_staged<T, LR, V, Load::kTiled>();
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw + align16(row_smem_v<T>(LR, V)));
     const int r = threadIdx.x / TT, t = threadIdx.x % TT;
-    const int row = blockIdx.x * row_rb_v<T>(LR, V) + r;
-    const bool valid = row < nrows;
     const int off = r * sm_len(LR + 1);
-    if constexpr (Load::kTiled) {
-        // whole tile chunks (RB rows x ct columns, contiguous) per access
-        constexpr int RB = row_rb_v<T>(LR, V);
-        const int row0 = blockIdx.x * RB;
-        const int nr = nrows - row0 < RB ? nrows - row0 : RB;
-        const int ct = ld.ct;
-        const int chunk = nr * ct;
-        const int ntiles = LR / ct + 1;
-        const int lct = __ffs(ct) - 1;  // ct is a power of two
-        const bool full = nr == RB;
-        const int lchunk = lct + ilog2c(RB);
-        const cplx<T>* base = ld.base + blockIdx.y * ld.bs + (size_t)row0 * ct;
-        for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
-            const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
-            const int rr = e >> lct, c = e & (ct - 1);
-            const int k = j * ct + c;
-            if (k <= LR) sm[smaddr(k, 1, rr * sm_len(LR + 1))] = base[(size_t)j * ld.nrows * ct + e];
+    const int ngroups = (nrows + RB - 1) / RB;
+    // the group's tile chunks (RB rows x ct columns, contiguous in HBM) into
+    // `dst` in the padded row layout; cp.async when staged
+    auto gather = [&](int grp, cplx<T>* dst) {
+        if constexpr (Load::kTiled) {
+            const int row0 = grp * RB;
+            const int nr = nrows - row0 < RB ? nrows - row0 : RB;
+            const int ct = ld.ct;
+            const int chunk = nr * ct;
+            const int ntiles = LR / ct + 1;
+            const int lct = __ffs(ct) - 1;  // ct is a power of two
+            const bool full = nr == RB;
+            const int lchunk = lct + ilog2c(RB);
+            const cplx<T>* base = ld.base + blockIdx.y * ld.bs + (size_t)row0 * ct;
+            for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
+                const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+                const int rr = e >> lct, c = e & (ct - 1);
+                const int k = j * ct + c;
+                if (k > LR) continue;
+                cplx<T>* d = &dst[smaddr(k, 1, rr * sm_len(LR + 1))];
+                const cplx<T>* g = &base[(size_t)j * ld.nrows * ct + e];
+                if constexpr (STAGED) cp_async_cplx<T>(d, g);
+                else *d = *g;
+            }
+            if constexpr (STAGED) cp_async_commit();
         }
-    } else {
-        for (int k = t; k <= LR; k += TT)
-            sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
-    }
-    __syncthreads();
-    cplx<T> v[RPT];
+    };
+    int grp = blockIdx.x;
+    if (STAGED && grp < ngroups) gather(grp, stg);
+    for (; grp < ngroups; grp += gridDim.x) {
+        const int row = grp * RB + r;
+        const bool valid = row < nrows;
+        const cplx<T>* src = sm;
+        if constexpr (STAGED) {
+            cp_async_wait_all();
+            src = stg;
+        } else if constexpr (Load::kTiled) {
+            gather(grp, sm);
+        } else {
+            for (int k = t; k <= LR; k += TT)
+                sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
+        }
+        __syncthreads();
+        cplx<T> v[RPT];
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        const int k = t + m * TT;
-        const cplx<T> xk = sm[smaddr(k, 1, off)];
-        const cplx<T> xn = sm[smaddr(LR - k, 1, off)];
-        const cplx<T> A = mk<T>(xk.x + xn.x, xk.y - xn.y);
-        const cplx<T> B = mk<T>(xk.x - xn.x, xk.y + xn.y);
-        const cplx<T> Bw = cmulc(B, __ldg(&tw_2lr[k]));  // B * exp(+2 pi i k / 2LR)
-        v[m] = mk<T>(A.x - Bw.y, A.y + Bw.x);             // A + i Bw
-    }
-    __syncthreads();
-    block_fft<T, LR, RPT, +1, 1>(v, t, sm, off, tw_lr);
+        for (int m = 0; m < RPT; ++m) {
+            const int k = t + m * TT;
+            const cplx<T> xk = src[smaddr(k, 1, off)];
+            const cplx<T> xn = src[smaddr(LR - k, 1, off)];
+            const cplx<T> A = mk<T>(xk.x + xn.x, xk.y - xn.y);
+            const cplx<T> B = mk<T>(xk.x - xn.x, xk.y + xn.y);
+            const cplx<T> Bw = cmulc(B, __ldg(&tw_2lr[k]));  // B * exp(+2 pi i k / 2LR)
+            v[m] = mk<T>(A.x - Bw.y, A.y + Bw.x);             // A + i Bw
+        }
+        __syncthreads();
+        if constexpr (STAGED)
+            if (grp + (int)gridDim.x < ngroups) gather(grp + gridDim.x, stg);
+        block_fft<T, LR, RPT, +1, 1>(v, t, sm, off, tw_lr);
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        if (PAD && m >= RPT / 2) continue;
-        if (valid) st(row, t + m * TT, v[m]);
+        for (int m = 0; m < RPT; ++m) {
+            if (PAD && m >= RPT / 2) continue;
+            if (valid) st(row, t + m * TT, v[m]);
+        }
+        __syncthreads();  // the workspace is rewritten by the next group
     }
     if constexpr (Store::kFinish) {
         __syncthreads();
@@ -295,7 +443,9 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 }
 
 // ---- column forward * multiplier * inverse --------------------------------------
-// Mult: cplx<T> operator()(cplx<T> X, int kx, int ky)
+// Mult: cplx<T> operator()(cplx<T> X, int kx, int ky).  One unit = one tile
+// of CT columns; instance blockIdx.y owns NCM1/CT + 1 contiguous tiles.
+// Dynamic shared memory: col_smem_total<T, LC, NCM1, PAD, V>().
 template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
 __global__ void __launch_bounds__(col_threads<T>(LC, NCM1, V), col_minb<T>(LC, NCM1, V))
 col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
@@ -304,27 +454,56 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     constexpr int RPT = col_rpt<T>(LC, V);
     constexpr int CT = col_ct_v<T>(LC, NCM1, V);
     constexpr int TT = LC / RPT;
+    constexpr int NTILES = NCM1 / CT + 1;
+    constexpr bool STAGED = col_staged<T, LC, NCM1, PAD, V>();
+    constexpr int ROWS = PAD ? LC / 2 : LC;  // stored rows of a tile
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw + align16(col_smem<T>(LC, CT)));
     const int c = threadIdx.x % CT, t = threadIdx.x / CT;
-    const int tile = blockIdx.x;
-    // instance blockIdx.y owns gridDim.x contiguous tiles
-    cplx<T>* base = spec + ((size_t)blockIdx.y * gridDim.x + tile) * nrows * CT;
-    cplx<T> v[RPT];
+    cplx<T>* inst = spec + (size_t)blockIdx.y * NTILES * nrows * CT;
+    auto issue = [&](int tile) {  // the tile's stored rows -> stg (cp.async)
+        if constexpr (STAGED) {
+            constexpr int NV = ROWS * CT * (int)sizeof(cplx<T>) / 16;
+            const char* src = reinterpret_cast<const char*>(inst + (size_t)tile * nrows * CT);
+            char* dst = reinterpret_cast<char*>(stg);
+            for (int f = threadIdx.x; f < NV; f += blockDim.x) cp_async16(dst + 16 * f, src + 16 * f);
+            cp_async_commit();
+        }
+    };
+    int tile = blockIdx.x;
+    if (tile < NTILES) issue(tile);
+    for (; tile < NTILES; tile += gridDim.x) {
+        cplx<T>* base = inst + (size_t)tile * nrows * CT;
+        cplx<T> v[RPT];
+        if constexpr (STAGED) {
+            cp_async_wait_all();
+            __syncthreads();
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-        else v[m] = base[(size_t)(t + m * TT) * CT + c];
-    }
-    block_fft<T, LC, RPT, -1, CT>(v, t, sm, c, tw_lc);
-    const int kx = tile * CT + c;
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = stg[(t + m * TT) * CT + c];
+            }
+            __syncthreads();
+            if (tile + (int)gridDim.x < NTILES) issue(tile + gridDim.x);
+        } else {
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, t + m * TT);
-    block_fft<T, LC, RPT, +1, CT>(v, t, sm, c, tw_lc);
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = base[(size_t)(t + m * TT) * CT + c];
+            }
+        }
+        block_fft<T, LC, RPT, -1, CT>(v, t, sm, c, tw_lc);
+        const int kx = tile * CT + c;
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) {
-        if (PAD && m >= RPT / 2) continue;
-        base[(size_t)(t + m * TT) * CT + c] = v[m];
+        for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, t + m * TT);
+        block_fft<T, LC, RPT, +1, CT>(v, t, sm, c, tw_lc);
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            if (PAD && m >= RPT / 2) continue;
+            base[(size_t)(t + m * TT) * CT + c] = v[m];
+        }
+        __syncthreads();  // the workspace is rewritten by the next tile
     }
 }
 

@@ -14,6 +14,7 @@ struct LoadRealRows {  // z[n] = (x[row*pitch + 2n], x[row*pitch + 2n + 1])
     int pitch;
     long bs;
     static constexpr bool kTiled = false;
+    static constexpr bool kRaw = true;  // plain rows: the row kernel may stage them
     __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
         return *reinterpret_cast<const cplx<T>*>(x + blockIdx.y * bs + (size_t)row * pitch +
                                                   2 * n);
@@ -52,6 +53,7 @@ struct LoadTiled {
     int nrows, ct;
     long bs;
     static constexpr bool kTiled = true;  // row kernels load whole tile chunks
+    static constexpr bool kRaw = false;
     __device__ __forceinline__ cplx<T> operator()(int row, int k) const {
         return base[blockIdx.y * bs + (size_t)(k / ct) * nrows * ct + (size_t)row * ct +
                     (k % ct)];

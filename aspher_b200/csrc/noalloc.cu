@@ -100,21 +100,21 @@ void na_apply(const NaDevice& d, double scale, const T* x, T* y, cudaStream_t s)
     cplx<T>* spec = static_cast<cplx<T>*>(d.spec);
     {
         constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-        constexpr int sm = row_smem_v<T>(LR, V);
+        constexpr int sm = row_fwd_smem<T, LR, false, V, LoadRealRows<T>>();
         auto k = row_fwd_kernel<T, LR, false, V, LoadRealRows<T>, StoreTiled<T>>;
         na_attrs((const void*)k, sm);
         k<<<(NS + rb - 1) / rb, thr, sm, s>>>(LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, ct},
                                               NS, tw + LR, tw + 2 * LR, nullptr);
     }
     {
-        constexpr int thr = col_threads<T>(LC, LR, V), sm = col_smem<T>(LC, ct);
+        constexpr int thr = col_threads<T>(LC, LR, V), sm = col_smem_total<T, LC, LR, false, V>();
         auto k = col_kernel<T, LC, LR, false, V, PeriodicMult<T>>;
         na_attrs((const void*)k, sm);
         k<<<LR / ct + 1, thr, sm, s>>>(spec, NS, PeriodicMult<T>{scale, NS}, tw + LC, nullptr);
     }
     {
         constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-        constexpr int sm = row_smem_v<T>(LR, V);
+        constexpr int sm = row_inv_smem<T, LR, V, LoadTiled<T>>();
         auto k = row_inv_kernel<T, LR, false, V, LoadTiled<T>, StoreRealRows<T>>;
         na_attrs((const void*)k, sm);
         k<<<(NS + rb - 1) / rb, thr, sm, s>>>(LoadTiled<T>{spec, NS, ct}, StoreRealRows<T>{y, NS},

@@ -139,6 +139,7 @@ __global__ void love_table_kernel(double* __restrict__ tab, int Ns, double h, do
 // with row/column Ns zero (fft_operator.cpp:31-44), generated on the fly.
 struct LoadEmbedded {
     static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
     const double* tab;
     int Ns, M;
     __device__ __forceinline__ double at(int iy, int ix) const {
@@ -263,30 +264,61 @@ void fft_attrs(const void* func, int bytes) {
     g_attr_done[key] = bytes;
 }
 
+// Persistent grid of a pass kernel: at most as many CTAs as fit on the device
+// at once (occupancy x SMs, cached per kernel, block shape and device), and
+// no more than the units (row groups / column tiles) to process.
+namespace {
+std::mutex g_occ_mu;
+std::map<std::tuple<const void*, int, int, int>, int> g_occ;
+}  // namespace
+int persistent_blocks(const void* func, int threads, int smem, int units) {
+    int dev = 0;
+    ASB_CUDA(cudaGetDevice(&dev));
+    const auto key = std::make_tuple(func, threads, smem, dev);
+    int resident = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        auto it = g_occ.find(key);
+        if (it != g_occ.end()) resident = it->second;
+    }
+    if (!resident) {
+        int per_sm = 0, nsm = 0;
+        ASB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, threads, smem));
+        ASB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        resident = (per_sm > 0 ? per_sm : 1) * nsm;
+        std::lock_guard<std::mutex> lk(g_occ_mu);
+        g_occ[key] = resident;
+    }
+    return units < resident ? units : resident;
+}
+
 // B > 1: gridDim.y = B instances (functors / gates / spectrum per instance)
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
-    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
+    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
+    constexpr int sm = row_fwd_smem<T, LR, PAD, V, Load>();
     auto k = row_fwd_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    k<<<dim3((nrows + rb - 1) / rb, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR),
-                                                      gate);
+    const int gx = persistent_blocks((const void*)k, thr, sm, (nrows + rb - 1) / rb);
+    k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
 }
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
-    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V), sm = row_smem_v<T>(LR, V);
+    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
+    constexpr int sm = row_inv_smem<T, LR, V, Load>();
     auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    k<<<dim3((nrows + rb - 1) / rb, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR),
-                                                      gate);
+    const int gx = persistent_blocks((const void*)k, thr, sm, (nrows + rb - 1) / rb);
+    k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
 }
 template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
 void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate, int B = 1) {
     constexpr int ct = col_ct_v<T>(LC, NCM1, V), thr = col_threads<T>(LC, NCM1, V);
-    constexpr int sm = col_smem<T>(LC, ct);
+    constexpr int sm = col_smem_total<T, LC, NCM1, PAD, V>();
     auto k = col_kernel<T, LC, NCM1, PAD, V, Mult>;
     fft_attrs((const void*)k, sm);
-    k<<<dim3(NCM1 / ct + 1, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
+    const int gx = persistent_blocks((const void*)k, thr, sm, NCM1 / ct + 1);
+    k<<<dim3(gx, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
 }
 
 #define ASB_V_SWITCH(VV, L, ...)                                                   \
@@ -390,6 +422,7 @@ struct PeriodicImpl {
 template <typename T>
 struct LoadMaskCentered {  // contact ? g - T(gsum/ng) : 0, pairwise; g = v - T(alpha)
     static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
     const T* g;
     const uint8_t* mask;
     const PkState* st;

@@ -53,6 +53,7 @@ __device__ inline void rden_tail(PkState* st, const double (&acc)[4]) {
 template <typename T>
 struct LoadTupd {
     static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
     const T* z;
     const T* g;  // v (uncentred)
     T* gprev;
