@@ -140,6 +140,7 @@ int aspher_op_love_table(const aspher_op* op, double* host_out) {
     if (op->impl->kind != asb::OP_FFT || !op->impl->table)
         throw asb::Error(ASPHER_EINVAL, "aspher_op_love_table: only the fft backend has a table");
     const size_t n = (size_t)op->impl->Ns * op->impl->Ns;
+    std::lock_guard<std::recursive_mutex> setup(asb::setup_mutex());
     ASB_CUDA(cudaMemcpy(host_out, op->impl->table, n * sizeof(double), cudaMemcpyDeviceToHost));
     return ASPHER_OK;
     ASB_API_END

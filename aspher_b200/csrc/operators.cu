@@ -35,7 +35,6 @@ namespace asb {
 // twiddle tables
 // ----------------------------------------------------------------------------
 namespace {
-std::mutex g_tw_mu;
 void* g_tw[64][2] = {};  // [device][dbl]
 
 void build_tw(int dev) {
@@ -65,7 +64,7 @@ const void* tw_table(bool dbl, int L) {
     ASB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) throw Error(-2, "device index out of range");
     if (!g_tw[dev][0]) {
-        std::lock_guard<std::mutex> lk(g_tw_mu);
+        std::lock_guard<std::recursive_mutex> lk(setup_mutex());
         if (!g_tw[dev][0]) build_tw(dev);
     }
     if (L < 1 || L > kMaxTw) throw Error(-1, "twiddle length out of range");
@@ -74,6 +73,11 @@ const void* tw_table(bool dbl, int L) {
 }
 
 bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }
+
+std::recursive_mutex& setup_mutex() {
+    static std::recursive_mutex m;
+    return m;
+}
 
 namespace {
 std::atomic<long long> g_launches{0};
@@ -578,6 +582,7 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
         throw Error(-1, "grid_size must be a power of two in [16, 8192]");
     if (!(L > 0.0) || !std::isfinite(L)) throw Error(-1, "domain_size must be positive");
     if (!(E_star > 0.0) || !std::isfinite(E_star)) throw Error(-1, "E_star must be positive");
+    std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ASB_CUDA(cudaGetDevice(&device));
     (void)tw_table(false, 2);
     if (kind == OP_PERIODIC) {
@@ -605,6 +610,7 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
 }
 
 Operator::~Operator() {
+    std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ctx_f.reset();
     ctx_d.reset();
     cudaFree(kh_d);
@@ -630,6 +636,7 @@ int Operator::col_tile(bool dbl, int cv) const {
 void Operator::set_variants(bool dbl, int rv, int cv) {
     if (rv < 0 || rv >= kVariants || cv < 0 || cv >= kVariants)
         throw Error(-1, "launch variant out of range");
+    std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     const int c = col_tile(dbl, cv);
     if (kind == OP_FFT && c != ct[dbl]) {
         // re-tile Kh of this precision for the new column tile width
@@ -646,6 +653,7 @@ void Operator::set_variants(bool dbl, int rv, int cv) {
 }
 
 double Operator::autotune(bool dbl, int reps, int& best_rv, int& best_cv) {
+    std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     const long N = (long)Ns * Ns;
     const size_t eb = dbl ? 8 : 4;
     void *x = nullptr, *y = nullptr, *flush = nullptr;
@@ -719,6 +727,7 @@ void* Operator::spectrum(bool dbl, cudaStream_t) {
     void*& p = dbl ? spec_d : spec_f;
     size_t& nb = dbl ? spec_d_bytes : spec_f_bytes;
     if (!p) {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         nb = spectrum_bytes(dbl);
         ASB_CUDA(cudaMalloc(&p, nb));
         ASB_CUDA(cudaMemset(p, 0, nb));

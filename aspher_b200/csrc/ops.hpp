@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 
@@ -57,6 +58,12 @@ bool is_pow2(long v);
 // launch variants chosen for (kind, precision, Ns): the autotuned entry of
 // this process if any, else the built-in default
 void tuned_variants(int kind, int dbl, int Ns, int& rv, int& cv);
+
+// Process-wide lock for work that must not overlap a CUDA-graph capture in
+// another host thread: graph capture itself and the set-up / tear-down calls
+// that synchronise the device (cudaMalloc / cudaMemset / cudaFree /
+// cudaDeviceSynchronize / blocking copies).  Recursive: set-up paths nest.
+std::recursive_mutex& setup_mutex();
 
 // Opt into >48 KB dynamic shared memory once per kernel per device.
 void smem_optin(const void* func, int bytes);

@@ -829,6 +829,7 @@ struct SolverCtx : SolverCtxBase {
     cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 
     SolverCtx(Operator& o, int capacity) : op(o), cap(capacity) {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         ASB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
         ASB_CUDA(cudaEventCreateWithFlags(&ev_in, cudaEventDisableTiming));
         ASB_CUDA(cudaEventCreateWithFlags(&ev_out, cudaEventDisableTiming));
@@ -851,6 +852,7 @@ struct SolverCtx : SolverCtxBase {
         }
     }
     ~SolverCtx() override {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd, spec};
@@ -867,6 +869,7 @@ struct SolverCtx : SolverCtxBase {
     void invalidate() override { drop_graph(); }
     void ensure_hist(int per_instance) {
         if (per_instance <= hist_cap) return;
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         if (hist) ASB_CUDA(cudaFree(hist));
         ASB_CUDA(cudaMalloc((void**)&hist, (size_t)cap * per_instance * sizeof(double)));
         hist_cap = per_instance;
@@ -960,8 +963,17 @@ struct SolverCtx : SolverCtxBase {
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ASB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeRelaxed));
-        enqueue_iteration(s, B);
-        k_loop_cond<<<1, 32, 0, s>>>(h, st, B);
+        try {
+            enqueue_iteration(s, B);
+            k_loop_cond<<<1, 32, 0, s>>>(h, st, B);
+        } catch (...) {
+            // leave no capture open on the stream, then report the failure
+            cudaGraph_t partial = nullptr;
+            cudaStreamEndCapture(s, &partial);
+            cudaGetLastError();
+            drop_graph();
+            throw;
+        }
         cudaGraph_t captured = nullptr;
         ASB_CUDA(cudaStreamEndCapture(s, &captured));
         ASB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
@@ -971,8 +983,11 @@ struct SolverCtx : SolverCtxBase {
     // iteration runs eagerly (every kernel returns at entry) so that all
     // function attributes are set outside the capture.  Clobbers st; the
     // caller writes the initial states afterwards.
+    // The capture holds setup_mutex(): no other host thread may synchronise
+    // the device (a set-up call) while this stream is capturing.
     void ensure_graph(cudaStream_t s, int B) {
         if (exec && graph_B == B) return;
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         std::vector<PkState> gated(B);
         std::memset(gated.data(), 0, B * sizeof(PkState));
         for (auto& x : gated) {
@@ -1434,6 +1449,7 @@ template <typename T>
 SolverCtx<T>& get_ctx(Operator& op, int cap = 1) {
     std::shared_ptr<SolverCtxBase>& slot = sizeof(T) == 8 ? op.ctx_d : op.ctx_f;
     if (!slot || static_cast<SolverCtx<T>&>(*slot).cap < cap) {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         slot.reset();  // free the smaller workspace first
         slot = std::make_shared<SolverCtx<T>>(op, cap);
     }
