@@ -98,29 +98,42 @@ def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max
     groups = {}
     for i, pr in enumerate(problems):
         groups.setdefault((pr["backend"], int(pr["grid_size"])), []).append(i)
-    for (b, Ns) in groups:  # build every operator before any thread starts
-        ops.get(b, Ns)
-    results = [None] * len(problems)
+    # Everything that allocates or copies is done here, before any worker
+    # starts: the operators, the groups' streams, gaps and outputs.  The
+    # workers then only run the library's batched solves (which serialise
+    # their own graph captures and set-up against each other).
     caller = torch.cuda.current_stream(dev)
+    streams, inputs, outputs = {}, {}, {}
+    for key, idx in groups.items():
+        ops.get(*key)
+        streams[key] = torch.cuda.Stream(device=dev)
+        inputs[key] = [torch.as_tensor(gaps[i], dtype=torch.float64).to(dev).reshape(-1)
+                       for i in idx]
+        N = key[1] * key[1]
+        outputs[key] = [torch.empty(N, dtype=torch.float64, device=dev) for _ in idx]
+    torch.cuda.synchronize(dev)
+    results = [None] * len(problems)
     done = []
 
     def run_group(key):
         b, Ns = key
         idx = groups[key]
         op = ops.get(b, Ns)
-        stream = torch.cuda.Stream(device=dev)
+        stream = streams[key]
         stream.wait_stream(caller)
         with torch.cuda.device(dev), torch.cuda.stream(stream):
-            g = [torch.as_tensor(gaps[i], dtype=torch.float64).to(dev).reshape(-1) for i in idx]
+            g = inputs[key]
             pn = [problems[i]["p_nominal"] for i in idx]
             if precision == "double":
                 rs = solve_device_batch(op, g, pn, tol=tol, max_iter=max_iter, precond=precond,
-                                        dtype=torch.float64, keep_best=False)
+                                        dtype=torch.float64, keep_best=False,
+                                        pressures_out=outputs[key])
             else:
                 rs, _ = solve_device_batch_mixed(op, g, pn, tol=tol, max_iter=max_iter,
                                                  precond=precond, keep_best=False,
                                                  polish=precision == "float_then_double",
-                                                 polish_tol=polish_tol)
+                                                 polish_tol=polish_tol,
+                                                 pressures_out=outputs[key])
             ev = torch.cuda.Event()
             ev.record(stream)
             done.append(ev)
