@@ -114,7 +114,7 @@ void na_apply(const NaDevice& d, double scale, const T* x, T* y, cudaStream_t s)
     }
     {
         constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-        constexpr int sm = row_inv_smem<T, LR, V, LoadTiled<T>>();
+        constexpr int sm = row_inv_smem<T, LR, false, V, LoadTiled<T>>();
         auto k = row_inv_kernel<T, LR, false, V, LoadTiled<T>, StoreRealRows<T>>;
         na_attrs((const void*)k, sm);
         k<<<(NS + rb - 1) / rb, thr, sm, s>>>(LoadTiled<T>{spec, NS, ct}, StoreRealRows<T>{y, NS},

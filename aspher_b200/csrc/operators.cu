@@ -309,7 +309,7 @@ void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gat
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
 void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
     constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-    constexpr int sm = row_inv_smem<T, LR, V, Load>();
+    constexpr int sm = row_inv_smem<T, LR, PAD, V, Load>();
     auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
     const int gx = persistent_blocks((const void*)k, thr, sm, (nrows + rb - 1) / rb);
