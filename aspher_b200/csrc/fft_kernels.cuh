@@ -145,17 +145,19 @@ __host__ __device__ constexpr bool col_fits(int LC) {
 }
 
 // ---- software pipeline ----------------------------------------------------------
-// The pass kernels are persistent: a CTA walks row groups (or column tiles)
-// blockIdx.x, blockIdx.x + gridDim.x, ...  When the input of a unit is a
-// plain contiguous block (raw rows, tiled spectrum chunks, a column tile) and
-// a staging buffer fits beside the FFT workspace, the next unit's input is
-// copied global -> shared with cp.async while the current unit is being
-// transformed, so the load latency of one unit hides behind the arithmetic
+// When the input of a unit (a row group or a column tile) is a plain
+// contiguous block (raw rows, tiled spectrum chunks, a column tile) and a
+// staging buffer fits beside the FFT workspace, the pass kernel is
+// persistent -- a CTA walks units blockIdx.x, blockIdx.x + gridDim.x, ... --
+// and the next unit's input is copied global -> shared with cp.async while
+// the current unit is being transformed, so the load latency of one unit hides behind the arithmetic
 // of the previous one.  The waits are the hardware's own (cp.async.wait_all):
 // no software spin.  Staging is used for the unpadded transforms only: on
 // B200 it sped the periodic applies up by 8-16 % (Ns 2048-4096) but slowed
 // the zero-padded free-space ones (whose staged inputs are half empty and
-// whose larger shared-memory footprint costs resident CTAs).
+// whose larger shared-memory footprint costs resident CTAs).  Unstaged
+// kernels process one unit per CTA: the loop would cost registers (the
+// 4096-point FP32 column kernel spilled with it).
 __host__ __device__ constexpr int align16(int b) { return (b + 15) & ~15; }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -278,30 +280,10 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         const cplx<T> w = __ldg(&tw_2lr[k]);
         return cadd(cscale(A, T(0.5)), cmul(w, O));
     };
-    int grp = blockIdx.x;
-    if (grp < ngroups) issue(grp);
-    for (; grp < ngroups; grp += gridDim.x) {
+    // transform of group grp from the strided registers v, and its store
+    auto body = [&](int grp, cplx<T> (&v)[RPT]) {
         const int row = grp * RB + r;
         const bool valid = row < nrows;
-        cplx<T> v[RPT];
-        if constexpr (STAGED) {
-            cp_async_wait_all();
-            __syncthreads();
-            const cplx<T>* srow = reinterpret_cast<const cplx<T>*>(stg + r * NREAL);
-#pragma unroll
-            for (int m = 0; m < RPT; ++m) {
-                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-                else v[m] = valid ? srow[t + m * TT] : mk<T>(0, 0);
-            }
-            __syncthreads();
-            if (grp + (int)gridDim.x < ngroups) issue(grp + gridDim.x);
-        } else {
-#pragma unroll
-            for (int m = 0; m < RPT; ++m) {
-                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-                else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
-            }
-        }
         block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
 #pragma unroll
         for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
@@ -345,7 +327,40 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
                 if (valid) st(row, t + m * TT, v[m]);
             if (t == 0 && valid) st(row, LR, mk<T>(z0.x - z0.y, T(0)));
         }
-        __syncthreads();  // the workspace is rewritten by the next group
+    };
+    if constexpr (STAGED) {
+        // persistent loop: the next group's rows are staged during this one
+        int grp = blockIdx.x;
+        if (grp < ngroups) issue(grp);
+        for (; grp < ngroups; grp += gridDim.x) {
+            const bool valid = grp * RB + r < nrows;
+            cplx<T> v[RPT];
+            cp_async_wait_all();
+            __syncthreads();
+            const cplx<T>* srow = reinterpret_cast<const cplx<T>*>(stg + r * NREAL);
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = valid ? srow[t + m * TT] : mk<T>(0, 0);
+            }
+            __syncthreads();
+            if (grp + (int)gridDim.x < ngroups) issue(grp + gridDim.x);
+            body(grp, v);
+            __syncthreads();  // the workspace is rewritten by the next group
+        }
+    } else {
+        // one group per CTA (a loop costs registers the unstaged kernel
+        // cannot spare)
+        const int grp = blockIdx.x;
+        const int row = grp * RB + r;
+        const bool valid = row < nrows;
+        cplx<T> v[RPT];
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+            else v[m] = valid ? ld(row, t + m * TT) : mk<T>(0, 0);
+        }
+        body(grp, v);
     }
     if constexpr (Store::kFinish) {
         __syncthreads();
@@ -401,22 +416,10 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             if constexpr (STAGED) cp_async_commit();
         }
     };
-    int grp = blockIdx.x;
-    if (STAGED && grp < ngroups) gather(grp, stg);
-    for (; grp < ngroups; grp += gridDim.x) {
+    // split step from `src` (padded rows), transform and store of group grp
+    auto body = [&](int grp, const cplx<T>* src) {
         const int row = grp * RB + r;
         const bool valid = row < nrows;
-        const cplx<T>* src = sm;
-        if constexpr (STAGED) {
-            cp_async_wait_all();
-            src = stg;
-        } else if constexpr (Load::kTiled) {
-            gather(grp, sm);
-        } else {
-            for (int k = t; k <= LR; k += TT)
-                sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
-        }
-        __syncthreads();
         cplx<T> v[RPT];
 #pragma unroll
         for (int m = 0; m < RPT; ++m) {
@@ -437,7 +440,30 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             if (PAD && m >= RPT / 2) continue;
             if (valid) st(row, t + m * TT, v[m]);
         }
-        __syncthreads();  // the workspace is rewritten by the next group
+    };
+    if constexpr (STAGED) {
+        // persistent loop: the next group's chunks are staged during this one
+        int grp = blockIdx.x;
+        if (grp < ngroups) gather(grp, stg);
+        for (; grp < ngroups; grp += gridDim.x) {
+            cp_async_wait_all();
+            __syncthreads();
+            body(grp, stg);
+            __syncthreads();  // the workspace is rewritten by the next group
+        }
+    } else {
+        // one group per CTA
+        const int grp = blockIdx.x;
+        if constexpr (Load::kTiled) {
+            gather(grp, sm);
+        } else {
+            const int row = grp * RB + r;
+            const bool valid = row < nrows;
+            for (int k = t; k <= LR; k += TT)
+                sm[smaddr(k, 1, off)] = valid ? ld(row, k) : mk<T>(0, 0);
+        }
+        __syncthreads();
+        body(grp, sm);
     }
     if constexpr (Store::kFinish) {
         __syncthreads();
@@ -474,28 +500,9 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
             cp_async_commit();
         }
     };
-    int tile = blockIdx.x;
-    if (tile < NTILES) issue(tile);
-    for (; tile < NTILES; tile += gridDim.x) {
+    // transform, multiply, inverse and store of tile `tile` from registers v
+    auto body = [&](int tile, cplx<T> (&v)[RPT]) {
         cplx<T>* base = inst + (size_t)tile * nrows * CT;
-        cplx<T> v[RPT];
-        if constexpr (STAGED) {
-            cp_async_wait_all();
-            __syncthreads();
-#pragma unroll
-            for (int m = 0; m < RPT; ++m) {
-                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-                else v[m] = stg[(t + m * TT) * CT + c];
-            }
-            __syncthreads();
-            if (tile + (int)gridDim.x < NTILES) issue(tile + gridDim.x);
-        } else {
-#pragma unroll
-            for (int m = 0; m < RPT; ++m) {
-                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-                else v[m] = base[(size_t)(t + m * TT) * CT + c];
-            }
-        }
         block_fft<T, LC, RPT, -1, CT>(v, t, sm, c, tw_lc);
         const int kx = tile * CT + c;
 #pragma unroll
@@ -506,7 +513,37 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
             if (PAD && m >= RPT / 2) continue;
             base[(size_t)(t + m * TT) * CT + c] = v[m];
         }
-        __syncthreads();  // the workspace is rewritten by the next tile
+    };
+    if constexpr (STAGED) {
+        // persistent loop: the next tile is staged during this one
+        int tile = blockIdx.x;
+        if (tile < NTILES) issue(tile);
+        for (; tile < NTILES; tile += gridDim.x) {
+            cplx<T> v[RPT];
+            cp_async_wait_all();
+            __syncthreads();
+#pragma unroll
+            for (int m = 0; m < RPT; ++m) {
+                if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+                else v[m] = stg[(t + m * TT) * CT + c];
+            }
+            __syncthreads();
+            if (tile + (int)gridDim.x < NTILES) issue(tile + gridDim.x);
+            body(tile, v);
+            __syncthreads();  // the workspace is rewritten by the next tile
+        }
+    } else {
+        // one tile per CTA (a loop costs registers the unstaged kernel cannot
+        // spare)
+        const int tile = blockIdx.x;
+        const cplx<T>* base = inst + (size_t)tile * nrows * CT;
+        cplx<T> v[RPT];
+#pragma unroll
+        for (int m = 0; m < RPT; ++m) {
+            if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
+            else v[m] = base[(size_t)(t + m * TT) * CT + c];
+        }
+        body(tile, v);
     }
 }
 

@@ -303,7 +303,9 @@ void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gat
     constexpr int sm = row_fwd_smem<T, LR, PAD, V, Load>();
     auto k = row_fwd_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    const int gx = persistent_blocks((const void*)k, thr, sm, (nrows + rb - 1) / rb);
+    const int units = (nrows + rb - 1) / rb;
+    const int gx = row_fwd_staged<T, LR, PAD, V, Load::kRaw>()
+                       ? persistent_blocks((const void*)k, thr, sm, units) : units;
     k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
 }
 template <typename T, int LR, bool PAD, int V, class Load, class Store>
@@ -312,7 +314,9 @@ void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gat
     constexpr int sm = row_inv_smem<T, LR, PAD, V, Load>();
     auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
     fft_attrs((const void*)k, sm);
-    const int gx = persistent_blocks((const void*)k, thr, sm, (nrows + rb - 1) / rb);
+    const int units = (nrows + rb - 1) / rb;
+    const int gx = row_inv_staged<T, LR, PAD, V, Load::kTiled>()
+                       ? persistent_blocks((const void*)k, thr, sm, units) : units;
     k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
 }
 template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
@@ -321,7 +325,9 @@ void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gat
     constexpr int sm = col_smem_total<T, LC, NCM1, PAD, V>();
     auto k = col_kernel<T, LC, NCM1, PAD, V, Mult>;
     fft_attrs((const void*)k, sm);
-    const int gx = persistent_blocks((const void*)k, thr, sm, NCM1 / ct + 1);
+    const int gx = col_staged<T, LC, NCM1, PAD, V>()
+                       ? persistent_blocks((const void*)k, thr, sm, NCM1 / ct + 1)
+                       : NCM1 / ct + 1;
     k<<<dim3(gx, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
 }
 

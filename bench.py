@@ -456,9 +456,13 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     """Adjoint gradient (FP32 and FP64 CG) of L = sum sigmoid(p/1e-4)/N^2 +
     0.5 mean(p^2) on a periodic Ns=1024 H=0.8 surface vs central differences
     of the FP64 solve (tol 1e-12, warm-started from the unperturbed solution;
-    unit-RMS directions, step 1e-6 rms).  Errors are reported relative to the
-    finite difference itself and relative to |grad| |d| (the first is
-    unbounded for directions nearly orthogonal to the gradient)."""
+    step 1e-6 rms).  The directions are gap perturbations of the surface law
+    (self-affine random fields, seeds 100.., unit RMS).  White-noise
+    directions are not used: on a 1024^2 grid a 2e-9 white-noise step moves
+    contact-boundary points in and out of contact, so their central
+    differences do not converge to the (one-sided) derivative at this step --
+    the difference to the adjoint shrinks with the step (1.4e-2 -> 6e-4 from
+    1e-6 to 1e-8 rms) while smooth directions agree to 1e-7."""
     import numpy as np
     import torch
     import aspher_b200 as asb
@@ -502,7 +506,7 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     pairs = []
     dn = float(np.sqrt(N))  # |d| of a unit-RMS direction
     for k in range(n_dirs):
-        d = torch.as_tensor(rng.standard_normal(N), device=dev)
+        d = torch.from_numpy(self_affine_gap(Ns, hurst=0.8, rms=1.0, seed=100 + k)).to(dev)
         d /= torch.sqrt(torch.mean(d ** 2))
         fd = (L_of(g0 + h * d, warm=p0)[0] - L_of(g0 - h * d, warm=p0)[0]) / (2 * h)
         for name in errs:
@@ -520,7 +524,7 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
         out[name]["rel_err_fd_pnominal"] = abs(grads[name][1] - fdp) / abs(fdp)
     out["f64_adjoint_vs_fd_pairs"] = pairs
     out["fd_directions"] = n_dirs
-    out["fd_step"] = "1e-6 * rms(gap), unit-RMS directions"
+    out["fd_step"] = "1e-6 * rms(gap); directions: self-affine random fields (seeds 100..), unit RMS"
     out["pass"] = all(out[n]["max_rel_err_fd_gap"] <= 1e-4 and
                       out[n]["rel_err_fd_pnominal"] <= 1e-4 for n in errs)
     return out
