@@ -250,62 +250,6 @@ __global__ void k_center(const PkParams* __restrict__ Pp, const PkState* st, T* 
     }
 }
 
-// ---- stencil preconditioner (stencil_precond.cpp:63-109) ---------------------
-// z = T(sum_t w_t gc(i + d_t)) on contact, gc = contact ? g - gmean : 0 with
-// periodic wrap; the contact mean of z is removed downstream.  2-D tile of
-// 64 x 16 outputs with an R-cell halo in shared memory.  k_stencil is the
-// standalone form (g already centred); the solve loop runs k_stencil_dots.
-constexpr int kStX = 64, kStY = 16, kMaxR = 4;
-
-template <typename T>
-__global__ void __launch_bounds__(256) k_stencil(const PkParams* __restrict__ Pp, PkState* st, StencilTaps taps,
-                                                 const T* g, const uint8_t* mask, T* z,
-                                                 double* part, int gated) {
-    const PkParams& P = *Pp;
-    if (gated && st->halt) return;
-    __shared__ double tile[(kStY + 2 * kMaxR) * (kStX + 2 * kMaxR)];
-    const int Ns = P.Ns, R = taps.R;
-    const int TW = kStX + 2 * R, TH = kStY + 2 * R;
-    const double gmean = st->nc ? st->gcs / st->nc : 0.0;
-    const int ntx = (Ns + kStX - 1) / kStX, nty = (Ns + kStY - 1) / kStY;
-    double acc[1] = {0.0};
-    for (int tid = blockIdx.x; tid < ntx * nty; tid += gridDim.x) {
-        const int tx0 = (tid % ntx) * kStX, ty0 = (tid / ntx) * kStY;
-        for (int idx = threadIdx.x; idx < TW * TH; idx += blockDim.x) {
-            const int ly = idx / TW, lx = idx % TW;
-            int gy = ty0 + ly - R, gx = tx0 + lx - R;
-            gy = gy < 0 ? gy + Ns : (gy >= Ns ? gy - Ns : gy);
-            gx = gx < 0 ? gx + Ns : (gx >= Ns ? gx - Ns : gx);
-            const size_t j = (size_t)gy * Ns + gx;
-            tile[ly * TW + lx] = mask[j] ? (double)g[j] - gmean : 0.0;
-        }
-        __syncthreads();
-        for (int o = threadIdx.x; o < kStX * kStY; o += blockDim.x) {
-            const int ly = o / kStX, lx = o % kStX;
-            const int gy = ty0 + ly, gx = tx0 + lx;
-            if (gy >= Ns || gx >= Ns) continue;
-            const size_t i = (size_t)gy * Ns + gx;
-            if (!mask[i]) { z[i] = T(0); continue; }
-            double a = 0.0;
-            for (int t = 0; t < taps.n; ++t)
-                a += taps.w[t] * tile[(ly + R + taps.dy[t]) * TW + (lx + R + taps.dx[t])];
-            z[i] = (T)a;
-            acc[0] += a;
-        }
-        __syncthreads();
-    }
-    const int kinds[1] = {0};
-    if (grid_reduce_last<1>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
-        st->zmean = st->nc ? (double)(T)(acc[0] / st->nc) : 0.0;
-        st->pc++;
-    }
-}
-
-inline int stencil_grid(int Ns) {
-    const int n = ((Ns + kStX - 1) / kStX) * ((Ns + kStY - 1) / kStY);
-    return n < kMaxBlocks ? n : kMaxBlocks;
-}
-
 // PR+ / FR ratio from G = <zf, g>, G_pr = <zf, g - g_prev> (contact_solver.cpp:420-446);
 // beta = Real(delta) * Real(ratio) is formed by the caller
 __device__ __forceinline__ void beta_update(const PkParams& P, PkState* st, double G, double Gpr,
@@ -317,76 +261,136 @@ __device__ __forceinline__ void beta_update(const PkParams& P, PkState* st, doub
     st->bv = bv;
 }
 
-// Stencil preconditioner and the CG dots of the loop in one pass: z on
-// contact (as k_stencil, g centred on the fly) and, with zf = Real(z - zm)
-// the contact-mean-free direction, the dots of the reference
-//   G = sum_C zf g,  G_pr = sum_C zf Real(g - gprev),  gg = sum_C g^2
+// ---- stencil preconditioner (stencil_precond.cpp:63-109) ---------------------
+// z = T(sum_t w_t gc(i + d_t)) on contact, gc = contact ? g - gmean : 0 with
+// periodic wrap; the contact mean of z is removed downstream.  A CTA of 256
+// threads owns a 64 x 32 tile of outputs whose (64 + 2R) x (32 + 2R) halo
+// of centred values sits in shared memory (FP64, as the reference
+// accumulates); thread (x, q) computes the 8 outputs (x, 8q .. 8q + 7) with
+// the disc's taps unrolled at compile time (R is a template parameter) and
+// summed in the reference's tap order (dy-major, dx-minor).
+constexpr int kStX = 64, kStY = 32, kStRows = 8, kMaxR = 4;
+
+// the disc's weights by (|dy|, |dx|) (they depend on the distance only)
+struct StencilW {
+    double w[kMaxR + 1][kMaxR + 1];
+};
+
+// LAZY: g holds v uncentred (the solve loop; centred by Real(alpha) on the
+// fly), else g is used as given (standalone preconditioner, adjoint).
+// DOTS: also the CG dots of the loop -- with zf = Real(z - zm) the
+// contact-mean-free direction,
+//   G = sum_C zf g,  G_pr = sum_C zf Real(g - gprev),  gg = sum_C g^2,
 // from sums linear in zm (zm is this pass's own reduction):
 //   G = sum_C z g - zm sum_C g,  G_pr = sum_C z (g - gprev) - zm sum_C (g - gprev).
-template <typename T>
-__global__ void __launch_bounds__(256) k_stencil_dots(const PkParams* __restrict__ Pp, PkState* st,
-                                                      StencilTaps taps, const T* g,
-                                                      const T* gprev, const uint8_t* mask,
-                                                      T* z, double* part) {
+template <typename T, int R, bool LAZY, bool DOTS>
+__global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ Pp, PkState* st,
+                                                   StencilW W, const T* g, const T* gprev,
+                                                   const uint8_t* mask, T* z, double* part,
+                                                   int gated) {
+    // instance blockIdx.y of a batched solve (0 when unbatched)
     Pp += blockIdx.y;
     st += blockIdx.y;
     part += (size_t)blockIdx.y * kPartStride;
     const long bo_ = (long)blockIdx.y * Pp->N;
     g += bo_;
-    gprev += bo_;
     mask += bo_;
     z += bo_;
+    if (DOTS) gprev += bo_;
     const PkParams& P = *Pp;
-    if (st->halt) return;
-    __shared__ double tile[(kStY + 2 * kMaxR) * (kStX + 2 * kMaxR)];
-    const int Ns = P.Ns, R = taps.R;
-    const int TW = kStX + 2 * R, TH = kStY + 2 * R;
+    if (gated && st->halt) return;
+    constexpr int TW = kStX + 2 * R, TH = kStY + 2 * R;
+    __shared__ double tile[TH * TW];
+    const int Ns = P.Ns, msk = Ns - 1;  // Ns is a power of two
     const double gmean = st->nc ? st->gcs / st->nc : 0.0;
-    const T aT = (T)st->alpha;
+    const T aT = LAZY ? (T)st->alpha : T(0);
     const int ntx = (Ns + kStX - 1) / kStX, nty = (Ns + kStY - 1) / kStY;
+    const int tx = threadIdx.x % kStX, tq = threadIdx.x / kStX;
     // sum z (unrounded), sum zT g, sum g, sum zT (g - gp), sum (g - gp), sum g^2
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double acc[DOTS ? 6 : 1];
+#pragma unroll
+    for (int i = 0; i < (DOTS ? 6 : 1); ++i) acc[i] = 0.0;
     for (int tid = blockIdx.x; tid < ntx * nty; tid += gridDim.x) {
         const int tx0 = (tid % ntx) * kStX, ty0 = (tid / ntx) * kStY;
         for (int idx = threadIdx.x; idx < TW * TH; idx += blockDim.x) {
-            const int ly = idx / TW, lx = idx % TW;
-            int gy = ty0 + ly - R, gx = tx0 + lx - R;
-            gy = gy < 0 ? gy + Ns : (gy >= Ns ? gy - Ns : gy);
-            gx = gx < 0 ? gx + Ns : (gx >= Ns ? gx - Ns : gx);
+            const int ly = idx / TW, lx = idx - ly * TW;
+            const int gy = (ty0 + ly - R) & msk, gx = (tx0 + lx - R) & msk;
             const size_t j = (size_t)gy * Ns + gx;
-            tile[ly * TW + lx] = mask[j] ? (double)gc(g[j], aT) - gmean : 0.0;
+            tile[idx] = mask[j] ? (double)(LAZY ? (T)(g[j] - aT) : g[j]) - gmean : 0.0;
         }
         __syncthreads();
-        for (int o = threadIdx.x; o < kStX * kStY; o += blockDim.x) {
-            const int ly = o / kStX, lx = o % kStX;
-            const int gy = ty0 + ly, gx = tx0 + lx;
-            if (gy >= Ns || gx >= Ns) continue;
-            const size_t i = (size_t)gy * Ns + gx;
-            if (!mask[i]) { z[i] = T(0); continue; }
+        const int x = tx0 + tx;
+#pragma unroll
+        for (int k = 0; k < kStRows; ++k) {
+            const int ly = tq * kStRows + k, y = ty0 + ly;
+            if (x >= Ns || y >= Ns) continue;
+            const size_t i = (size_t)y * Ns + x;
+            if (!mask[i]) {
+                z[i] = T(0);
+                continue;
+            }
             double a = 0.0;
-            for (int t = 0; t < taps.n; ++t)
-                a += taps.w[t] * tile[(ly + R + taps.dy[t]) * TW + (lx + R + taps.dx[t])];
+#pragma unroll
+            for (int dy = -R; dy <= R; ++dy)
+#pragma unroll
+                for (int dx = -R; dx <= R; ++dx)
+                    if (dx * dx + dy * dy <= R * R)
+                        a += W.w[dy < 0 ? -dy : dy][dx < 0 ? -dx : dx] *
+                             tile[(ly + R + dy) * TW + (tx + R + dx)];
             const T zT = (T)a;
             z[i] = zT;
-            const T gi = gc(g[i], aT);
-            const double gd = (double)gi, dg = (double)(T)(gi - gprev[i]);
             acc[0] += a;
-            acc[1] += (double)zT * gd;
-            acc[2] += gd;
-            acc[3] += (double)zT * dg;
-            acc[4] += dg;
-            acc[5] += gd * gd;
+            if constexpr (DOTS) {
+                const T gi = LAZY ? (T)(g[i] - aT) : g[i];
+                const double gd = (double)gi, dg = (double)(T)(gi - gprev[i]);
+                acc[1] += (double)zT * gd;
+                acc[2] += gd;
+                acc[3] += (double)zT * dg;
+                acc[4] += dg;
+                acc[5] += gd * gd;
+            }
         }
         __syncthreads();
     }
-    const int kinds[6] = {0, 0, 0, 0, 0, 0};
-    if (grid_reduce_last<6>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
+    int kinds[DOTS ? 6 : 1];
+#pragma unroll
+    for (int i = 0; i < (DOTS ? 6 : 1); ++i) kinds[i] = 0;
+    if (grid_reduce_last<DOTS ? 6 : 1>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
         const double zmean = st->nc ? (double)(T)(acc[0] / st->nc) : 0.0;
         st->zmean = zmean;
         st->pc++;
-        beta_update(P, st, acc[1] - zmean * acc[2], acc[3] - zmean * acc[4], acc[5]);
-        st->beta = (double)((T)st->delta * (T)st->bv);
+        if constexpr (DOTS) {
+            beta_update(P, st, acc[1] - zmean * acc[2], acc[3] - zmean * acc[4], acc[5]);
+            st->beta = (double)((T)st->delta * (T)st->bv);
+        }
     }
+}
+
+inline int stencil_grid(int Ns) {
+    const int n = ((Ns + kStX - 1) / kStX) * ((Ns + kStY - 1) / kStY);
+    return n < kMaxRowBlocks ? n : kMaxRowBlocks;
+}
+
+StencilW stencil_weights(const StencilTaps& taps) {
+    StencilW W{};
+    for (int t = 0; t < taps.n; ++t)
+        W.w[std::abs(taps.dy[t])][std::abs(taps.dx[t])] = taps.w[t];
+    return W;
+}
+
+// launch of k_stencil_t for the runtime radius R in [1, kMaxR]
+template <typename T, bool LAZY, bool DOTS>
+void launch_stencil(int R, dim3 grid, cudaStream_t s, const PkParams* Pp, PkState* st,
+                    const StencilW& W, const T* g, const T* gprev, const uint8_t* mask, T* z,
+                    double* part, int gated) {
+    switch (R) {
+        case 1: k_stencil_t<T, 1, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+        case 2: k_stencil_t<T, 2, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+        case 3: k_stencil_t<T, 3, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+        case 4: k_stencil_t<T, 4, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+        default: throw Error(ASPHER_EINVAL, "stencil radius must be in [1, 4]");
+    }
+    count_launches(1);
 }
 
 // ---- CG passes (contact_solver.cpp:420-501) ------------------------------------
@@ -816,6 +820,7 @@ struct SolverCtx : SolverCtxBase {
     PkParams* Pd = nullptr;
     void* spec = nullptr;  // spectrum scratch of cap instances (cap > 1 only)
     StencilTaps taps{};
+    StencilW W{};
     int precond = -1, radius = -1;
     int grid = 1;
     int graph_B = 0;
@@ -889,7 +894,10 @@ struct SolverCtx : SolverCtxBase {
     }
     void configure(int pc, int R) {
         if (pc == precond && (pc != 1 || R == radius)) return;
-        if (pc == 1) taps = make_stencil_taps(op.Ns, R);
+        if (pc == 1) {
+            taps = make_stencil_taps(op.Ns, R);
+            W = stencil_weights(taps);
+        }
         precond = pc;
         radius = R;
         drop_graph();
@@ -915,8 +923,8 @@ struct SolverCtx : SolverCtxBase {
             ++n;
         }
         if (precond == 1) {
-            k_stencil_dots<T><<<dim3(stencil_grid(op.Ns), B), 256, 0, s>>>(Pd, st, taps, g, gprev,
-                                                                          mask, z, part);
+            launch_stencil<T, true, true>(radius, dim3(stencil_grid(op.Ns), B), s, Pd, st, W, g,
+                                          gprev, mask, z, part, 1);
             ++n;
         } else {
             if (precond == 2)
@@ -1714,8 +1722,8 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
     if (precond == 1) {
         StencilTaps taps = make_stencil_taps(op.Ns, radius);
-        k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, g, mask, z, part, 0);
-        count_launches(1);
+        launch_stencil<T, false, false>(radius, dim3(stencil_grid(op.Ns)), s, Pd, st,
+                                        stencil_weights(taps), g, nullptr, mask, z, part, 0);
     } else {
         fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
     }
@@ -1957,8 +1965,8 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     const auto t0 = std::chrono::steady_clock::now();
     const long N = (long)op.Ns * op.Ns;
     const size_t vb = (size_t)N * sizeof(T);
-    StencilTaps taps{};
-    if (precond == ASPHER_PRECOND_STENCIL) taps = make_stencil_taps(op.Ns, radius);
+    StencilW W{};
+    if (precond == ASPHER_PRECOND_STENCIL) W = stencil_weights(make_stencil_taps(op.Ns, radius));
     T *wT = nullptr, *r = nullptr, *z = nullptr, *d = nullptr, *q = nullptr, *lam = nullptr;
     uint8_t* mask = nullptr;
     double* part = nullptr;
@@ -1993,9 +2001,9 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
         for (int k = 0; k < 16; ++k) {  // kernels return at entry once halted
             const T* zz = r;
             if (precond == ASPHER_PRECOND_STENCIL) {
-                k_stencil<T><<<stencil_grid(op.Ns), 256, 0, s>>>(Pd, st, taps, r, mask, z, part, 1);
+                launch_stencil<T, false, false>(radius, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
+                                                nullptr, mask, z, part, 1);
                 zz = z;
-                count_launches(1);
             }
             k_adj_rz<T><<<grid, kRedThreads, 0, s>>>(Pd, st, zz, r, mask, part);
             k_adj_d<T><<<grid, kRedThreads, 0, s>>>(Pd, st, zz, mask, d);

@@ -518,6 +518,7 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     hp = 1e-6 * pbar
     fdp = (L_of(g0, pbar + hp, warm=p0)[0] - L_of(g0, pbar - hp, warm=p0)[0]) / (2 * hp)
     for name in errs:
+        out[name]["n_within_1e-4"] = sum(e <= 1e-4 for e in errs[name])
         out[name]["max_rel_err_fd_gap"] = max(errs[name])
         out[name]["median_rel_err_fd_gap"] = float(np.median(errs[name]))
         out[name]["max_err_rel_grad_norm"] = max(errn[name])
