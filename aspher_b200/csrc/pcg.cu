@@ -310,22 +310,51 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
     double acc[DOTS ? 6 : 1];
 #pragma unroll
     for (int i = 0; i < (DOTS ? 6 : 1); ++i) acc[i] = 0.0;
+    // each thread issues all of its loads before it uses any (none depends
+    // on another), so a tile costs about one memory latency, not one per
+    // element
+    constexpr int NL = (TW * TH + 255) / 256;  // halo elements per thread
     for (int tid = blockIdx.x; tid < ntx * nty; tid += gridDim.x) {
         const int tx0 = (tid % ntx) * kStX, ty0 = (tid / ntx) * kStY;
-        for (int idx = threadIdx.x; idx < TW * TH; idx += blockDim.x) {
-            const int ly = idx / TW, lx = idx - ly * TW;
-            const int gy = (ty0 + ly - R) & msk, gx = (tx0 + lx - R) & msk;
-            const size_t j = (size_t)gy * Ns + gx;
-            tile[idx] = mask[j] ? (double)(LAZY ? (T)(g[j] - aT) : g[j]) - gmean : 0.0;
+        T hv[NL];
+        uint8_t hm[NL];
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int idx = threadIdx.x + u * 256;
+            if (idx < TW * TH) {
+                const int ly = idx / TW, lx = idx - ly * TW;
+                const int gy = (ty0 + ly - R) & msk, gx = (tx0 + lx - R) & msk;
+                const size_t j = (size_t)gy * Ns + gx;
+                hm[u] = mask[j];
+                hv[u] = g[j];
+            }
+        }
+        const int x = tx0 + tx;
+        const bool xin = x < Ns;
+        uint8_t om[kStRows];
+        T og[kStRows], op[kStRows];
+#pragma unroll
+        for (int k = 0; k < kStRows; ++k) {
+            const int y = ty0 + tq * kStRows + k;
+            const bool in = xin && y < Ns;
+            const size_t i = (size_t)(in ? y : 0) * Ns + (in ? x : 0);
+            om[k] = in ? mask[i] : 0;
+            og[k] = g[i];
+            if constexpr (DOTS) op[k] = gprev[i];
+        }
+#pragma unroll
+        for (int u = 0; u < NL; ++u) {
+            const int idx = threadIdx.x + u * 256;
+            if (idx < TW * TH)
+                tile[idx] = hm[u] ? (double)(LAZY ? (T)(hv[u] - aT) : hv[u]) - gmean : 0.0;
         }
         __syncthreads();
-        const int x = tx0 + tx;
 #pragma unroll
         for (int k = 0; k < kStRows; ++k) {
             const int ly = tq * kStRows + k, y = ty0 + ly;
-            if (x >= Ns || y >= Ns) continue;
+            if (!xin || y >= Ns) continue;
             const size_t i = (size_t)y * Ns + x;
-            if (!mask[i]) {
+            if (!om[k]) {
                 z[i] = T(0);
                 continue;
             }
@@ -341,8 +370,8 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
             z[i] = zT;
             acc[0] += a;
             if constexpr (DOTS) {
-                const T gi = LAZY ? (T)(g[i] - aT) : g[i];
-                const double gd = (double)gi, dg = (double)(T)(gi - gprev[i]);
+                const T gi = LAZY ? (T)(og[k] - aT) : og[k];
+                const double gd = (double)gi, dg = (double)(T)(gi - op[k]);
                 acc[1] += (double)zT * gd;
                 acc[2] += gd;
                 acc[3] += (double)zT * dg;
