@@ -395,6 +395,180 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
     }
 }
 
+// Register-blocked form for Ns >= 128 (the tile form above serves smaller
+// grids): a warp owns a 128-wide segment of a 32-row strip, lane l the four
+// consecutive columns x0 = seg*128 + 4l .. x0+3.  It streams the strip's
+// rows top to bottom through a window of 2R+1 rows of centred values in
+// registers (one float4 / double2x2 load of g and one uchar4 of the mask per
+// new row); horizontal neighbours come from the adjacent lanes by shuffles
+// and, at the segment edges, from the strip's halo columns staged in shared
+// memory once per strip.  No block-wide barrier inside the strip.
+constexpr int kSwSeg = 128, kSwRows = 32, kSwWarps = 4;
+
+template <typename T, int R, bool LAZY, bool DOTS>
+__global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __restrict__ Pp,
+                                                             PkState* st, StencilW W, const T* g,
+                                                             const T* gprev, const uint8_t* mask,
+                                                             T* z, double* part, int gated) {
+    Pp += blockIdx.y;
+    st += blockIdx.y;
+    part += (size_t)blockIdx.y * kPartStride;
+    const long bo_ = (long)blockIdx.y * Pp->N;
+    g += bo_;
+    mask += bo_;
+    z += bo_;
+    if (DOTS) gprev += bo_;
+    const PkParams& P = *Pp;
+    if (gated && st->halt) return;
+    constexpr int WR = 2 * R + 1;            // window rows
+    constexpr int HR = kSwRows + 2 * R;      // halo rows of a strip
+    __shared__ double halo[kSwWarps][HR][2 * R];
+    const int Ns = P.Ns, msk = Ns - 1;
+    const double gmean = st->nc ? st->gcs / st->nc : 0.0;
+    const T aT = LAZY ? (T)st->alpha : T(0);
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nseg = Ns / kSwSeg, nstrips = nseg * (Ns / kSwRows);
+    auto centred = [&](uint8_t m, T v) -> double {
+        return m ? (double)(LAZY ? (T)(v - aT) : v) - gmean : 0.0;
+    };
+    auto load4 = [&](const T* base, size_t i, T (&o)[4]) {
+        if constexpr (sizeof(T) == 4) {
+            const float4 q = *reinterpret_cast<const float4*>(base + i);
+            o[0] = q.x; o[1] = q.y; o[2] = q.z; o[3] = q.w;
+        } else {
+            const double2 q0 = *reinterpret_cast<const double2*>(base + i);
+            const double2 q1 = *reinterpret_cast<const double2*>(base + i + 2);
+            o[0] = q0.x; o[1] = q0.y; o[2] = q1.x; o[3] = q1.y;
+        }
+    };
+    double acc[DOTS ? 6 : 1];
+#pragma unroll
+    for (int i = 0; i < (DOTS ? 6 : 1); ++i) acc[i] = 0.0;
+    for (int sw = blockIdx.x * kSwWarps + wib; sw < nstrips; sw += gridDim.x * kSwWarps) {
+        const int seg = sw % nseg, y0 = (sw / nseg) * kSwRows;
+        const int xs = seg * kSwSeg, x0 = xs + 4 * lane;
+        // the strip's halo columns (R left of the segment, R right), centred
+        for (int e = lane; e < HR * 2 * R; e += 32) {
+            const int hr = e / (2 * R), c = e - hr * (2 * R);
+            const int x = (c < R ? xs - R + c : xs + kSwSeg + (c - R)) & msk;
+            const size_t j = (size_t)((y0 - R + hr) & msk) * Ns + x;
+            halo[wib][hr][c] = centred(mask[j], g[j]);
+        }
+        __syncwarp();
+        double win[WR][4];
+        uint32_t wmk[WR];  // the window rows' masks, 4 bytes
+        // raw loads of one row (issued a step ahead of their use, so a row's
+        // load latency hides behind the previous row's arithmetic)
+        auto fetch = [&](int y, T (&v)[4], uint32_t& m4) {
+            const size_t i = (size_t)(y & msk) * Ns + x0;
+            m4 = *reinterpret_cast<const uint32_t*>(mask + i);
+            load4(g, i, v);
+        };
+        auto put = [&](const T (&v)[4], uint32_t m4, double (&w)[4], uint32_t& mk) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) w[j] = centred((m4 >> (8 * j)) & 0xff, v[j]);
+            mk = m4;
+        };
+#pragma unroll
+        for (int r = 1; r < WR; ++r) {
+            T v[4];
+            uint32_t m4;
+            fetch(y0 - R + r - 1, v, m4);
+            put(v, m4, win[r], wmk[r]);
+        }
+        T nv[4], np[4];
+        uint32_t nm;
+        fetch(y0 + R, nv, nm);
+        if constexpr (DOTS) load4(gprev, (size_t)y0 * Ns + x0, np);
+        for (int k = 0; k < kSwRows; ++k) {
+#pragma unroll
+            for (int r = 0; r + 1 < WR; ++r) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) win[r][j] = win[r + 1][j];
+                wmk[r] = wmk[r + 1];
+            }
+            put(nv, nm, win[WR - 1], wmk[WR - 1]);
+            T gp[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) gp[j] = np[j];
+            if (k + 1 < kSwRows) {
+                fetch(y0 + k + 1 + R, nv, nm);
+                if constexpr (DOTS) load4(gprev, (size_t)(y0 + k + 1) * Ns + x0, np);
+            }
+            // value at column offset d (in [-R, 3 + R]) of window row r
+            auto at = [&](int r, int d) -> double {
+                if (d >= 0 && d < 4) return win[r][d];
+                double own, v;
+                if (d < 0) {
+                    own = win[r][4 + d];  // lane-1 holds it at index 4 + d
+                    v = __shfl_up_sync(0xffffffffu, own, 1);
+                    if (lane == 0) v = halo[wib][k + r][R + d];
+                } else {
+                    own = win[r][d - 4];  // lane+1 holds it at index d - 4
+                    v = __shfl_down_sync(0xffffffffu, own, 1);
+                    if (lane == 31) v = halo[wib][k + r][R + (d - 4)];
+                }
+                return v;
+            };
+            const int y = y0 + k;
+            const size_t i = (size_t)y * Ns + x0;
+            double a[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int dy = -R; dy <= R; ++dy) {
+#pragma unroll
+                for (int dx = -R; dx <= R; ++dx) {
+                    if (dx * dx + dy * dy > R * R) continue;
+                    const double w = W.w[dy < 0 ? -dy : dy][dx < 0 ? -dx : dx];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) a[j] += w * at(R + dy, j + dx);
+                }
+            }
+            const uint32_t mc = wmk[R];
+            T zo[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const bool on = (mc >> (8 * j)) & 0xff;
+                zo[j] = on ? (T)a[j] : T(0);
+                if (on) acc[0] += a[j];
+            }
+            if constexpr (sizeof(T) == 4) {
+                *reinterpret_cast<float4*>(z + i) = make_float4(zo[0], zo[1], zo[2], zo[3]);
+            } else {
+                *reinterpret_cast<double2*>(z + i) = make_double2(zo[0], zo[1]);
+                *reinterpret_cast<double2*>(z + i + 2) = make_double2(zo[2], zo[3]);
+            }
+            if constexpr (DOTS) {
+                T gv[4];
+                load4(g, i, gv);  // loaded R rows ago: a cache hit
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (!((mc >> (8 * j)) & 0xff)) continue;
+                    const T gi = LAZY ? (T)(gv[j] - aT) : gv[j];
+                    const double gd = (double)gi, dg = (double)(T)(gi - gp[j]);
+                    acc[1] += (double)zo[j] * gd;
+                    acc[2] += gd;
+                    acc[3] += (double)zo[j] * dg;
+                    acc[4] += dg;
+                    acc[5] += gd * gd;
+                }
+            }
+        }
+        __syncwarp();  // the halo buffer is refilled by the next strip
+    }
+    int kinds[DOTS ? 6 : 1];
+#pragma unroll
+    for (int i = 0; i < (DOTS ? 6 : 1); ++i) kinds[i] = 0;
+    if (grid_reduce_last<DOTS ? 6 : 1>(acc, kinds, part, &st->counter[2]) && threadIdx.x == 0) {
+        const double zmean = st->nc ? (double)(T)(acc[0] / st->nc) : 0.0;
+        st->zmean = zmean;
+        st->pc++;
+        if constexpr (DOTS) {
+            beta_update(P, st, acc[1] - zmean * acc[2], acc[3] - zmean * acc[4], acc[5]);
+            st->beta = (double)((T)st->delta * (T)st->bv);
+        }
+    }
+}
+
 inline int stencil_grid(int Ns) {
     const int n = ((Ns + kStX - 1) / kStX) * ((Ns + kStY - 1) / kStY);
     return n < kMaxRowBlocks ? n : kMaxRowBlocks;
@@ -409,9 +583,24 @@ StencilW stencil_weights(const StencilTaps& taps) {
 
 // launch of k_stencil_t for the runtime radius R in [1, kMaxR]
 template <typename T, bool LAZY, bool DOTS>
-void launch_stencil(int R, dim3 grid, cudaStream_t s, const PkParams* Pp, PkState* st,
+void launch_stencil(int R, int Ns, dim3 grid, cudaStream_t s, const PkParams* Pp, PkState* st,
                     const StencilW& W, const T* g, const T* gprev, const uint8_t* mask, T* z,
                     double* part, int gated) {
+    if (Ns >= kSwSeg) {
+        const int strips = (Ns / kSwSeg) * (Ns / kSwRows);
+        int nb = (strips + kSwWarps - 1) / kSwWarps;
+        if (nb > kMaxRowBlocks) nb = kMaxRowBlocks;
+        const dim3 gw(nb, grid.y);
+        switch (R) {
+            case 1: k_stencil_w<T, 1, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+            case 2: k_stencil_w<T, 2, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+            case 3: k_stencil_w<T, 3, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+            case 4: k_stencil_w<T, 4, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+            default: throw Error(ASPHER_EINVAL, "stencil radius must be in [1, 4]");
+        }
+        count_launches(1);
+        return;
+    }
     switch (R) {
         case 1: k_stencil_t<T, 1, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
         case 2: k_stencil_t<T, 2, LAZY, DOTS><<<grid, 256, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
@@ -952,7 +1141,7 @@ struct SolverCtx : SolverCtxBase {
             ++n;
         }
         if (precond == 1) {
-            launch_stencil<T, true, true>(radius, dim3(stencil_grid(op.Ns), B), s, Pd, st, W, g,
+            launch_stencil<T, true, true>(radius, op.Ns, dim3(stencil_grid(op.Ns), B), s, Pd, st, W, g,
                                           gprev, mask, z, part, 1);
             ++n;
         } else {
@@ -1751,7 +1940,7 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
     if (precond == 1) {
         StencilTaps taps = make_stencil_taps(op.Ns, radius);
-        launch_stencil<T, false, false>(radius, dim3(stencil_grid(op.Ns)), s, Pd, st,
+        launch_stencil<T, false, false>(radius, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st,
                                         stencil_weights(taps), g, nullptr, mask, z, part, 0);
     } else {
         fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
@@ -2030,7 +2219,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
         for (int k = 0; k < 16; ++k) {  // kernels return at entry once halted
             const T* zz = r;
             if (precond == ASPHER_PRECOND_STENCIL) {
-                launch_stencil<T, false, false>(radius, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
+                launch_stencil<T, false, false>(radius, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
                                                 nullptr, mask, z, part, 1);
                 zz = z;
             }

@@ -129,20 +129,22 @@ def test_periodic_matrix_properties_and_alias():
     assert torch.linalg.norm(x - ref) <= 1e-15 * torch.linalg.norm(ref)
 
 
-@pytest.mark.parametrize("kind", ["stencil", "fourier-fft"])
-@pytest.mark.parametrize("Ns", [64, 512])
-def test_preconditioners_match_oracle(kind, Ns):
+@pytest.mark.parametrize("kind,radius", [("stencil", 1), ("stencil", 2), ("stencil", 3),
+                                          ("stencil", 4), ("fourier-fft", 2)])
+@pytest.mark.parametrize("Ns", [64, 128, 512])
+def test_preconditioners_match_oracle(kind, radius, Ns):
+    # Ns = 64 runs the tiled stencil kernel, Ns >= 128 the register-window one
     rng = np.random.default_rng(11)
     g = rng.standard_normal(Ns * Ns)
     c = (rng.random(Ns * Ns) < 0.35).astype(np.uint8)
     op = _op("periodic", Ns)
-    P = StencilPreconditioner(Ns, 2) if kind == "stencil" else FourierPreconditioner(Ns)
+    P = StencilPreconditioner(Ns, radius) if kind == "stencil" else FourierPreconditioner(Ns)
     for dt, tol in ((torch.float64, 1e-13), (torch.float32, 2e-6)):
         npdt = np.float64 if dt == torch.float64 else np.float32
         gd = torch.as_tensor(g.astype(npdt), device="cuda")
         cd = torch.as_tensor(c, device="cuda")
         z = torch.empty_like(gd)
-        op.precond_("stencil" if kind == "stencil" else "fft", gd, cd, z)
+        op.precond_("stencil" if kind == "stencil" else "fft", gd, cd, z, radius=radius)
         torch.cuda.synchronize()
         ref = P.apply(g.astype(npdt), c.astype(bool), npdt).astype(np.float64)
         got = z.cpu().numpy().astype(np.float64)
