@@ -409,7 +409,8 @@ template <typename T, int R, bool LAZY, bool DOTS>
 __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __restrict__ Pp,
                                                              PkState* st, StencilW W, const T* g,
                                                              const T* gprev, const uint8_t* mask,
-                                                             T* z, double* part, int gated) {
+                                                             T* z, double* part, int gated,
+                                                             int rows) {
     Pp += blockIdx.y;
     st += blockIdx.y;
     part += (size_t)blockIdx.y * kPartStride;
@@ -421,13 +422,13 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
     const PkParams& P = *Pp;
     if (gated && st->halt) return;
     constexpr int WR = 2 * R + 1;            // window rows
-    constexpr int HR = kSwRows + 2 * R;      // halo rows of a strip
+    constexpr int HR = kSwRows + 2 * R;      // halo rows of the longest strip
     __shared__ double halo[kSwWarps][HR][2 * R];
     const int Ns = P.Ns, msk = Ns - 1;
     const double gmean = st->nc ? st->gcs / st->nc : 0.0;
     const T aT = LAZY ? (T)st->alpha : T(0);
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nseg = Ns / kSwSeg, nstrips = nseg * (Ns / kSwRows);
+    const int nseg = Ns / kSwSeg, nstrips = nseg * (Ns / rows);
     auto centred = [&](uint8_t m, T v) -> double {
         return m ? (double)(LAZY ? (T)(v - aT) : v) - gmean : 0.0;
     };
@@ -445,10 +446,10 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
 #pragma unroll
     for (int i = 0; i < (DOTS ? 6 : 1); ++i) acc[i] = 0.0;
     for (int sw = blockIdx.x * kSwWarps + wib; sw < nstrips; sw += gridDim.x * kSwWarps) {
-        const int seg = sw % nseg, y0 = (sw / nseg) * kSwRows;
+        const int seg = sw % nseg, y0 = (sw / nseg) * rows;
         const int xs = seg * kSwSeg, x0 = xs + 4 * lane;
         // the strip's halo columns (R left of the segment, R right), centred
-        for (int e = lane; e < HR * 2 * R; e += 32) {
+        for (int e = lane; e < (rows + 2 * R) * 2 * R; e += 32) {
             const int hr = e / (2 * R), c = e - hr * (2 * R);
             const int x = (c < R ? xs - R + c : xs + kSwSeg + (c - R)) & msk;
             const size_t j = (size_t)((y0 - R + hr) & msk) * Ns + x;
@@ -480,7 +481,7 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
         uint32_t nm;
         fetch(y0 + R, nv, nm);
         if constexpr (DOTS) load4(gprev, (size_t)y0 * Ns + x0, np);
-        for (int k = 0; k < kSwRows; ++k) {
+        for (int k = 0; k < rows; ++k) {
 #pragma unroll
             for (int r = 0; r + 1 < WR; ++r) {
 #pragma unroll
@@ -491,7 +492,7 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
             T gp[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) gp[j] = np[j];
-            if (k + 1 < kSwRows) {
+            if (k + 1 < rows) {
                 fetch(y0 + k + 1 + R, nv, nm);
                 if constexpr (DOTS) load4(gprev, (size_t)(y0 + k + 1) * Ns + x0, np);
             }
@@ -569,6 +570,13 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
     }
 }
 
+inline int num_sms() {
+    int dev = 0, n = 0;
+    ASB_CUDA(cudaGetDevice(&dev));
+    ASB_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+    return n > 0 ? n : 1;
+}
+
 inline int stencil_grid(int Ns) {
     const int n = ((Ns + kStX - 1) / kStX) * ((Ns + kStY - 1) / kStY);
     return n < kMaxRowBlocks ? n : kMaxRowBlocks;
@@ -581,21 +589,27 @@ StencilW stencil_weights(const StencilTaps& taps) {
     return W;
 }
 
-// launch of k_stencil_t for the runtime radius R in [1, kMaxR]
+// launch of the stencil pass for the runtime radius R in [1, kMaxR]: the
+// register-window kernel for Ns >= 128, the tile kernel below that
 template <typename T, bool LAZY, bool DOTS>
 void launch_stencil(int R, int Ns, dim3 grid, cudaStream_t s, const PkParams* Pp, PkState* st,
                     const StencilW& W, const T* g, const T* gprev, const uint8_t* mask, T* z,
                     double* part, int gated) {
     if (Ns >= kSwSeg) {
-        const int strips = (Ns / kSwSeg) * (Ns / kSwRows);
+        // strips of 32, 16 or 8 rows: the longest that still gives every
+        // SM about 16 resident warps (a shorter strip re-reads more halo rows)
+        int rows = kSwRows;
+        const long want = 16L * num_sms();
+        while (rows > 8 && (long)(Ns / kSwSeg) * (Ns / rows) * grid.y < want) rows /= 2;
+        const int strips = (Ns / kSwSeg) * (Ns / rows);
         int nb = (strips + kSwWarps - 1) / kSwWarps;
         if (nb > kMaxRowBlocks) nb = kMaxRowBlocks;
         const dim3 gw(nb, grid.y);
         switch (R) {
-            case 1: k_stencil_w<T, 1, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
-            case 2: k_stencil_w<T, 2, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
-            case 3: k_stencil_w<T, 3, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
-            case 4: k_stencil_w<T, 4, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated); break;
+            case 1: k_stencil_w<T, 1, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated, rows); break;
+            case 2: k_stencil_w<T, 2, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated, rows); break;
+            case 3: k_stencil_w<T, 3, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated, rows); break;
+            case 4: k_stencil_w<T, 4, LAZY, DOTS><<<gw, 32 * kSwWarps, 0, s>>>(Pp, st, W, g, gprev, mask, z, part, gated, rows); break;
             default: throw Error(ASPHER_EINVAL, "stencil radius must be in [1, 4]");
         }
         count_launches(1);
