@@ -403,17 +403,44 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             const bool full = nr == RB;
             const int lchunk = lct + ilog2c(RB);
             const cplx<T>* base = ld.base + blockIdx.y * ld.bs + (size_t)row0 * ct;
-            for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
-                const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
-                const int rr = e >> lct, c = e & (ct - 1);
-                const int k = j * ct + c;
-                if (k > LR) continue;
-                cplx<T>* d = &dst[smaddr(k, 1, rr * sm_len(LR + 1))];
-                const cplx<T>* g = &base[(size_t)j * ld.nrows * ct + e];
-                if constexpr (STAGED) cp_async_cplx<T>(d, g);
-                else *d = *g;
+            const int total = ntiles * chunk;
+            if constexpr (STAGED) {
+                for (int f = threadIdx.x; f < total; f += blockDim.x) {
+                    const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+                    const int rr = e >> lct, c = e & (ct - 1);
+                    const int k = j * ct + c;
+                    if (k > LR) continue;
+                    cp_async_cplx<T>(&dst[smaddr(k, 1, rr * sm_len(LR + 1))],
+                                     &base[(size_t)j * ld.nrows * ct + e]);
+                }
+                cp_async_commit();
+            } else {
+                // U loads in flight per thread before their stores: the
+                // chunks come from L2 / HBM, and one dependent load at a time
+                // left the kernel waiting on load latency
+                constexpr int U = 8;
+                for (int f0 = threadIdx.x; f0 < total; f0 += U * blockDim.x) {
+                    cplx<T> val[U];
+                    int at[U];
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int f = f0 + u * (int)blockDim.x;
+                        at[u] = -1;
+                        if (f < total) {
+                            const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+                            const int rr = e >> lct, c = e & (ct - 1);
+                            const int k = j * ct + c;
+                            if (k <= LR) {
+                                at[u] = smaddr(k, 1, rr * sm_len(LR + 1));
+                                val[u] = base[(size_t)j * ld.nrows * ct + e];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < U; ++u)
+                        if (at[u] >= 0) dst[at[u]] = val[u];
+                }
             }
-            if constexpr (STAGED) cp_async_commit();
         }
     };
     // split step from `src` (padded rows), transform and store of group grp
