@@ -82,7 +82,7 @@ class Operators:
 
 def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max_iter=5000,
                precision="float_then_double", concurrent=True, operators=None,
-               device=None):
+               device=None, float_tol=None):
     """Solve ``problems`` (dicts with backend, grid_size, p_nominal) with the
     matching ``gaps`` (device tensors or arrays of Ns^2 FP64 values).
     Returns the ContactResults in problem order (pressures on the device).
@@ -129,7 +129,8 @@ def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max
                                         dtype=torch.float64, keep_best=False,
                                         pressures_out=outputs[key])
             else:
-                rs, _ = solve_device_batch_mixed(op, g, pn, tol=tol, max_iter=max_iter,
+                rs, _ = solve_device_batch_mixed(op, g, pn, tol=tol, float_tol=float_tol,
+                                                 max_iter=max_iter,
                                                  precond=precond, keep_best=False,
                                                  polish=precision == "float_then_double",
                                                  polish_tol=polish_tol,
