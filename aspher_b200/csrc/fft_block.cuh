@@ -100,6 +100,19 @@ __host__ __device__ constexpr int num_stages(int L, int RMAX) {
 
 __device__ __forceinline__ int smaddr(int i, int S, int off) { return (i + (i >> 4)) * S + off; }
 
+// smaddr(i0 + m * STEP) as a per-thread base plus a compile-time offset where
+// the padding term splits.  For STEP a multiple of 16, (i0 + m STEP) >> 4 =
+// (i0 >> 4) + m STEP / 16.  RUN is the length (a power of two) of the
+// RUN-aligned group that every i0 + m STEP stays in; for RUN <= 16 that group
+// lies inside one 16-element block, so the padding term does not change
+// with m.
+template <int STEP, int RUN>
+__device__ __forceinline__ int smaddr_run(int i0, int m, int S, int off) {
+    if constexpr (STEP % 16 == 0) return smaddr(i0, S, off) + m * (STEP + STEP / 16) * S;
+    else if constexpr (RUN <= 16) return smaddr(i0, S, off) + m * STEP * S;
+    else return smaddr(i0 + m * STEP, S, off);
+}
+
 // a * w (forward) or a * conj(w) (inverse), w from the exp(-2 pi i k/L) table
 template <int DIR, typename V>
 __device__ __forceinline__ V tw_apply(V a, V w) {
@@ -169,13 +182,13 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
             } else {
                 const int base = (j / SPAN) * SPAN * R + (j % SPAN);
 #pragma unroll
-                for (int r = 0; r < R; ++r) sm[smaddr(base + r * SPAN, S, off)] = a[r];
+                for (int r = 0; r < R; ++r) sm[smaddr_run<SPAN, SPAN * R>(base, r, S, off)] = a[r];
             }
         }
         if constexpr (!LAST) {
             __syncthreads();
 #pragma unroll
-            for (int m = 0; m < RPT; ++m) v[m] = sm[smaddr(t + m * TT, S, off)];
+            for (int m = 0; m < RPT; ++m) v[m] = sm[smaddr_run<TT, 1 << 30>(t, m, S, off)];
             __syncthreads();
             fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R>(v, t, sm, off, tw);
         }

@@ -286,7 +286,7 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         const bool valid = row < nrows;
         block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
 #pragma unroll
-        for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, 1, off)] = v[m];
+        for (int m = 0; m < RPT; ++m) sm[smaddr_run<TT, 1 << 30>(t, m, 1, off)] = v[m];
         __syncthreads();
         if constexpr (Store::kTiled) {
             // each output reads Z[k] and Z[-k] from shared memory and goes
