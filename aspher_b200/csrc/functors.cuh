@@ -34,6 +34,49 @@ struct StoreRealRows {
     __device__ void finish(double*) const {}
 };
 
+// FP64 rows in, FP32 pairs out: x - x0 (x0 optional), rounded once.  The
+// defect-corrected FP64 apply (Operator::matvec_defect) transforms this
+// difference in FP32.
+struct LoadDiffRows {
+    static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
+    const double* x;
+    const double* x0;
+    int pitch;
+    long bs;
+    __device__ __forceinline__ cplx<float> operator()(int row, int n) const {
+        const size_t i = blockIdx.y * bs + (size_t)row * pitch + 2 * n;
+        double2 v = *reinterpret_cast<const double2*>(x + i);
+        if (x0) {
+            const double2 w = *reinterpret_cast<const double2*>(x0 + i);
+            v.x -= w.x;
+            v.y -= w.y;
+        }
+        return mk<float>((float)v.x, (float)v.y);
+    }
+};
+
+// FP32 pairs in, FP64 rows out: y = y0 + z (y0 optional).
+struct StoreAddRows {
+    static constexpr bool kFinish = false;
+    static constexpr bool kTiled = false;
+    double* y;
+    const double* y0;
+    int pitch;
+    long bs;
+    __device__ __forceinline__ void operator()(int row, int n, cplx<float> z) const {
+        const size_t i = blockIdx.y * bs + (size_t)row * pitch + 2 * n;
+        double2 o = make_double2((double)z.x, (double)z.y);
+        if (y0) {
+            const double2 w = *reinterpret_cast<const double2*>(y0 + i);
+            o.x += w.x;
+            o.y += w.y;
+        }
+        *reinterpret_cast<double2*>(y + i) = o;
+    }
+    __device__ void finish(double*) const {}
+};
+
 template <typename T>
 struct StoreTiled {
     cplx<T>* base;

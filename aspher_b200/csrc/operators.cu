@@ -777,6 +777,22 @@ void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const in
     }
 }
 
+void Operator::matvec_defect(const double* x, const double* x0, double* y, const double* y0,
+                             cudaStream_t s, const int* gate, int B, void* spec_b) {
+    void* spec = spec_b ? spec_b : spectrum(false, s);
+    const long bx = (long)Ns * Ns;
+    if (kind == OP_FFT) {
+        ASB_SIZE_SWITCH(Ns, FreeImpl<float, NS>::apply(*this, LoadDiffRows{x, x0, NS, bx},
+                                                       StoreAddRows{y, y0, NS, bx},
+                                                       (float2*)spec, s, gate, B));
+    } else {
+        ASB_SIZE_SWITCH(Ns, PeriodicImpl<float, NS>::apply(
+                                rowv[0], colv[0], LoadDiffRows{x, x0, NS, bx},
+                                PeriodicMult<float>{scale, NS}, StoreAddRows{y, y0, NS, bx},
+                                (float2*)spec, s, gate, B));
+    }
+}
+
 template <typename T>
 void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
                         double* part, cudaStream_t s, const int* gate, int B, void* spec) {

@@ -106,6 +106,14 @@ struct Operator {
     // instance b.
     void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr,
                 int B = 1, void* spec_b = nullptr);
+    // Defect-corrected FP64 apply: y = y0 + S_32(x - x0) with x, x0, y, y0
+    // FP64 fields (x0, y0 optional) and the transform in FP32.  With
+    // y0 = S x0 exact, the result carries the FP32 rounding of S only on the
+    // difference x - x0, i.e. FP64-level accuracy while x stays near x0.
+    // Batched as matvec (spec_b: B * spectrum_bytes(false) at least).
+    void matvec_defect(const double* x, const double* x0, double* y, const double* y0,
+                       cudaStream_t s, const int* gate = nullptr, int B = 1,
+                       void* spec_b = nullptr);
     void* spectrum(bool dbl, cudaStream_t s);
     int col_tile(bool dbl, int cv) const;
     void set_variants(bool dbl, int rv, int cv);

@@ -1031,6 +1031,17 @@ int red_grid(long N) {
     return (int)g;
 }
 
+// The FP64 polish stage of a mixed solve runs its loop applies
+// defect-corrected (Operator::matvec_defect: FP32 transforms of p - p0 and of
+// t around one exact FP64 apply of p0); ASPHER_POLISH_EXACT=1 keeps them FP64.
+static bool polish_defect() {
+    static const bool d = [] {
+        const char* v = std::getenv("ASPHER_POLISH_EXACT");
+        return !(v && v[0] == '1');
+    }();
+    return d;
+}
+
 // Per-operator, per-precision solver context: the CG workspace of up to
 // `cap` instances (fields back to back), the device parameter and state
 // blocks, and the instantiated loop graph (a while-conditional node whose
@@ -1055,10 +1066,17 @@ struct SolverCtx : SolverCtxBase {
     StencilW W{};
     int precond = -1, radius = -1;
     int grid = 1;
-    int graph_B = 0;
     bool with_hist = false;  // the loop body records pk per iteration (k_evalpk)
-    cudaGraphExec_t exec = nullptr;
-    cudaGraph_t graph = nullptr;
+    // Defect-corrected applies (FP64 contexts, the polish stage of a mixed
+    // solve): u = u0 + S_32(p - p0) and r = S_32(t), with p0 the stage's
+    // starting pressure and u0 = S p0 from one exact FP64 apply.
+    bool defect = false;
+    double* p0 = nullptr;
+    double* u0 = nullptr;
+    // one instantiated loop graph per apply mode (plain, defect-corrected)
+    cudaGraphExec_t exec_m[2] = {nullptr, nullptr};
+    cudaGraph_t graph_m[2] = {nullptr, nullptr};
+    int graph_B_m[2] = {0, 0};
     // Private non-blocking stream: the loop graph is captured and launched
     // here (the legacy NULL stream a caller may pass cannot be captured);
     // entry and exit are fenced to the caller's stream with events.
@@ -1090,9 +1108,8 @@ struct SolverCtx : SolverCtxBase {
     }
     ~SolverCtx() override {
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd, spec};
+        drop_graph();
+        void* all[] = {p, t, u, g, gprev, z, r, best, g0c, mask, part, hist, st, Pd, spec, p0, u0};
         for (void* v : all)
             if (v) cudaFree(v);
         if (ev_in) cudaEventDestroy(ev_in);
@@ -1113,11 +1130,25 @@ struct SolverCtx : SolverCtxBase {
         drop_graph();  // the graph bakes the history pointer
     }
     void drop_graph() {
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        exec = nullptr;
-        graph = nullptr;
-        graph_B = 0;
+        for (int m = 0; m < 2; ++m) {
+            if (exec_m[m]) cudaGraphExecDestroy(exec_m[m]);
+            if (graph_m[m]) cudaGraphDestroy(graph_m[m]);
+            exec_m[m] = nullptr;
+            graph_m[m] = nullptr;
+            graph_B_m[m] = 0;
+        }
+    }
+    // switch the loop's applies between exact and defect-corrected (FP64
+    // contexts only); allocates p0 / u0 on first use, outside any capture
+    void set_defect(bool on) {
+        if (on && sizeof(T) != 8) throw Error(ASPHER_EINVAL, "defect correction needs FP64");
+        if (on && !p0) {
+            std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+            ASB_CUDA(cudaMalloc((void**)&p0, (size_t)cap * N * sizeof(double)));
+            ASB_CUDA(cudaMalloc((void**)&u0, (size_t)cap * N * sizeof(double)));
+            (void)op.spectrum(false, nullptr);  // the FP32 scratch of unbatched applies
+        }
+        defect = on;
     }
     void set_hist(bool on) {
         if (on == with_hist) return;
@@ -1144,10 +1175,29 @@ struct SolverCtx : SolverCtxBase {
     // per instance on the device:
     //   [apply p->u] eval (evalpk) | stencil+dots  or  [precond] dots |
     //   tupd [apply t->r] rden | pupd rescale
+    // the loop's two applies: u = S p (gated by skip_mv1) and r = S t
+    void apply_u(cudaStream_t s, int B) {
+        if constexpr (sizeof(T) == 8) {
+            if (defect) {
+                op.matvec_defect(p, p0, u, u0, s, &st->skip_mv1, B, B > 1 ? spec : nullptr);
+                return;
+            }
+        }
+        apply(p, u, &st->skip_mv1, s, B);
+    }
+    void apply_r(cudaStream_t s, int B) {
+        if constexpr (sizeof(T) == 8) {
+            if (defect) {
+                op.matvec_defect(t, nullptr, r, nullptr, s, &st->halt, B, B > 1 ? spec : nullptr);
+                return;
+            }
+        }
+        apply(t, r, &st->halt, s, B);
+    }
     void enqueue_iteration(cudaStream_t s, int B) {
         const dim3 gr(grid, B);
         int n = 0;
-        apply(p, u, &st->skip_mv1, s, B);
+        apply_u(s, B);
         k_eval<T><<<gr, kRedThreads, 0, s>>>(Pd, st, u, g0c, p, g, mask, part, 0);
         ++n;
         if (with_hist) {
@@ -1165,12 +1215,12 @@ struct SolverCtx : SolverCtxBase {
             k_dots<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
             ++n;
         }
-        if (fused_t()) {
+        if (fused_t() && !defect) {
             pk_apply_t<T>(op, z, g, gprev, t, mask, p, best, st, part, precond, s, &st->halt, B,
                           B > 1 ? spec : nullptr);
         } else {
             k_tupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
-            apply(t, r, &st->halt, s, B);
+            apply_r(s, B);
             k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
             n += 2;
         }
@@ -1189,7 +1239,13 @@ struct SolverCtx : SolverCtxBase {
         ASB_CUDA(cudaGetLastError());
     }
     void build_graph(cudaStream_t s, int B) {
-        drop_graph();
+        const int m = defect;
+        if (exec_m[m]) cudaGraphExecDestroy(exec_m[m]);
+        if (graph_m[m]) cudaGraphDestroy(graph_m[m]);
+        exec_m[m] = nullptr;
+        graph_m[m] = nullptr;
+        graph_B_m[m] = 0;
+        cudaGraph_t& graph = graph_m[m];
         ASB_CUDA(cudaGraphCreate(&graph, 0));
         cudaGraphConditionalHandle h;
         ASB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
@@ -1216,8 +1272,8 @@ struct SolverCtx : SolverCtxBase {
         }
         cudaGraph_t captured = nullptr;
         ASB_CUDA(cudaStreamEndCapture(s, &captured));
-        ASB_CUDA(cudaGraphInstantiate(&exec, graph, 0));
-        graph_B = B;
+        ASB_CUDA(cudaGraphInstantiate(&exec_m[defect], graph_m[defect], 0));
+        graph_B_m[defect] = B;
     }
     // (Re)build the loop graph if needed.  Before capturing, one fully gated
     // iteration runs eagerly (every kernel returns at entry) so that all
@@ -1226,7 +1282,7 @@ struct SolverCtx : SolverCtxBase {
     // The capture holds setup_mutex(): no other host thread may synchronise
     // the device (a set-up call) while this stream is capturing.
     void ensure_graph(cudaStream_t s, int B) {
-        if (exec && graph_B == B) return;
+        if (exec_m[defect] && graph_B_m[defect] == B) return;
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         std::vector<PkState> gated(B);
         std::memset(gated.data(), 0, B * sizeof(PkState));
@@ -1240,7 +1296,7 @@ struct SolverCtx : SolverCtxBase {
         build_graph(s, B);
     }
     void launch_graph(cudaStream_t s) {
-        ASB_CUDA(cudaGraphLaunch(exec, s));
+        ASB_CUDA(cudaGraphLaunch(exec_m[defect], s));
         count_launches(1);
     }
     // ASPHER_EAGER_LOOP=1: enqueue iterations as plain launches instead of the
@@ -1405,7 +1461,8 @@ struct Solver {
     void run(const aspher_solve_opts& o, const T* const* g0s, const double* p_bars,
              const T* const* p_inits, double* const* pressures, double* disp, double* gap,
              double* hist_host, int hist_cap, aspher_result* res,
-             const double* datum_b = nullptr, const double* gref_b = nullptr) {
+             const double* datum_b = nullptr, const double* gref_b = nullptr,
+             bool defect = false) {
         const auto t_start = std::chrono::steady_clock::now();
         const int Ns = c.op.Ns;
         const long N = (long)Ns * Ns;
@@ -1513,6 +1570,17 @@ struct Solver {
             H.halt = o.max_iter > 0 ? H_RUN : H_FINAL;
             H.skip_mv1 = H.halt ? 1 : 0;
         }
+        // defect-corrected applies (a polish stage): p0 = the starting
+        // pressures, u0 = S p0 by one exact FP64 apply of all instances
+        c.set_defect(defect);
+        if constexpr (sizeof(T) == 8) {
+            if (defect) {
+                ASB_CUDA(cudaMemcpyAsync(c.p0, c.p, (size_t)B * N * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, s));
+                c.apply(c.p0, c.u0, nullptr, s, B);
+                for (int b = 0; b < B; ++b) ih[b].mv_host += 1;
+            }
+        }
         if (!SolverCtx<T>::eager_loop()) c.ensure_graph(s, B);
         write_states();
 
@@ -1589,8 +1657,11 @@ struct Solver {
                     I.returned_best = true;
                 }
             }
-            if (!H.u_fresh) H.mv++;
-            H.skip_mv1 = H.u_fresh ? 1 : 0;  // gates the final apply per instance
+            // the certificate is evaluated from an exact apply: a
+            // defect-corrected u is recomputed
+            const bool fresh = H.u_fresh && !c.defect;
+            if (!fresh) H.mv++;
+            H.skip_mv1 = fresh ? 1 : 0;  // gates the final apply per instance
             H.halt = H_FINAL;
         }
         write_states();
@@ -1868,7 +1939,7 @@ void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, dou
         Solver<double> S(cd, s);
         const double* pw = pressure;
         S.run(od, &g0, &p_bar, &pw, &pressure, disp, gap, nullptr, 0, &res, datum.data(),
-              gref.data());
+              gref.data(), polish_defect());
     }
     add_stage(res, rf);
 }
@@ -1928,7 +1999,7 @@ void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const do
         Solver<double> S(cd, s, B);
         std::vector<const double*> pw(pressures, pressures + B);
         S.run(od, g0s, p_bars, pw.data(), pressures, nullptr, nullptr, nullptr, 0, res,
-              datum.data(), gref.data());
+              datum.data(), gref.data(), polish_defect());
     }
     for (int b = 0; b < B; ++b) add_stage(res[b], rf[b]);
 }

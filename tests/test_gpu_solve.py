@@ -164,3 +164,22 @@ def test_history_and_counts():
     assert len(r.error_history) == r.iterations
     assert r.matvec_count >= 2 * r.iterations
     assert r.precond_count >= 1
+
+
+@pytest.mark.parametrize("backend", ["fft", "periodic"])
+def test_polish_reaches_fp64_certificates(backend):
+    """The FP64 polish stage applies S defect-corrected (FP32 transforms of
+    p - p0 and of the direction around one exact FP64 apply of p0); it still
+    certifies FP64 tolerances, and the result matches a tight FP64 solve."""
+    from aspher_b200 import Operator, solve_device, solve_device_mixed
+    Ns, pbar = 256, 0.005
+    op = Operator(backend, Ns)
+    g0 = torch.as_tensor(_rough(Ns), device="cuda")
+    ref = solve_device(op, g0, pbar, tol=1e-12, precond="fourier", dtype=torch.float64,
+                       max_iter=20000)
+    assert ref.status == "converged"
+    r, rf = solve_device_mixed(op, g0, pbar, tol=1e-10, float_tol=1e-5, precond="fourier")
+    assert rf.status == "converged" and rf.fw_error <= 1e-5
+    assert r.status == "converged", (r.status, r.status_reason)
+    assert r.fw_error <= 1e-10 and r.penetration_error <= 1e-10
+    assert rel(r.pressure, ref.pressure) <= 1e-8
