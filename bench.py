@@ -492,6 +492,7 @@ def large_single(dev, Ns=8192, pbar=0.005):
                                           seed=SEED)).to(dev)
     asb.solve_nested(1024, gs, pbar, **kw)
     torch.cuda.synchronize()
+    torch.cuda.empty_cache()  # the earlier legs' cached blocks back to the driver
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
