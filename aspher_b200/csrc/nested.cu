@@ -272,7 +272,7 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
                     od.datum_mode = ASPHER_DATUM_SOLVER;
                     od.dtype = ASPHER_F64;
                     solve_impl<double>(*op, od, glvl, p_bar, p_lvl, p_lvl, dout, gout, hout,
-                                       hist_cap, r, s);
+                                       hist_cap, r, s, /*polish_stage=*/true);
                     record("polish:" + std::to_string(n), "double", np.tol, np.tol, r);
                     r.iterations += rf.iterations;
                     r.matvec_count += rf.matvec_count;

@@ -1829,18 +1829,20 @@ StencilTaps make_stencil_taps(int Ns, int R) {
 template <typename T>
 void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
-                int hist_cap, aspher_result& res, cudaStream_t s) {
+                int hist_cap, aspher_result& res, cudaStream_t s, bool polish_stage) {
     Solver<T> S(get_ctx<T>(op), s);
     const T* g = (const T*)g0;
     const T* pi = (const T*)p_init;
-    S.run(o, &g, &p_bar, &pi, &pressure, disp, gap, hist, hist_cap, &res);
+    const bool defect = sizeof(T) == 8 && polish_stage && p_init && polish_defect();
+    S.run(o, &g, &p_bar, &pi, &pressure, disp, gap, hist, hist_cap, &res, nullptr, nullptr,
+          defect);
 }
 template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*, double,
                                 const void*, double*, double*, double*, double*, int,
-                                aspher_result&, cudaStream_t);
+                                aspher_result&, cudaStream_t, bool);
 template void solve_impl<double>(Operator&, const aspher_solve_opts&, const void*, double,
                                  const void*, double*, double*, double*, double*, int,
-                                 aspher_result&, cudaStream_t);
+                                 aspher_result&, cudaStream_t, bool);
 
 namespace {
 // FP64 min / max / non-finite count of B FP64 gaps (validation before any

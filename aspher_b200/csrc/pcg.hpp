@@ -39,10 +39,13 @@ void pk_apply_t(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint
                 const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
                 const int* gate, int B = 1, void* spec = nullptr);
 
+// polish_stage: the solve refines p_init (the FP64 stage of a mixed or
+// nested float_then_double solve); its loop applies may then be
+// defect-corrected (see Operator::matvec_defect)
 template <typename T>
 void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
-                int hist_cap, aspher_result& res, cudaStream_t s);
+                int hist_cap, aspher_result& res, cudaStream_t s, bool polish_stage = false);
 
 void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
                  const double* p_init, double float_tol, int polish, double* pressure,
