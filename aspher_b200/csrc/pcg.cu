@@ -20,6 +20,8 @@
 #include "reduce.cuh"
 
 #include <algorithm>
+#include <map>
+#include <utility>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
@@ -1012,13 +1014,16 @@ __global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, cons
 }
 
 // ---- device-side loop control -------------------------------------------------------
-// Last kernel of the graph body: keep looping while any instance is running.
-__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st, int B) {
-    // one warp: keep looping while any instance is still running
+// Last kernel of the graph body: keep looping while at least min_run
+// instances are running (a batch graph hands its last running instance to
+// that instance's own loop graph, whose kernels launch no gated blocks).
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st, int B, int min_run) {
+    // one warp: count the running instances
     int run = 0;
-    for (int b = threadIdx.x; b < B; b += 32) run |= (st[b].halt == H_RUN);
-    run = __any_sync(0xffffffffu, run);
-    if (threadIdx.x == 0) cudaGraphSetConditional(h, run ? 1u : 0u);
+    for (int b = threadIdx.x; b < B; b += 32) run += (st[b].halt == H_RUN);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) run += __shfl_xor_sync(0xffffffffu, run, o);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, run >= min_run ? 1u : 0u);
 }
 
 // ---- host driver -----------------------------------------------------------------
@@ -1073,10 +1078,15 @@ struct SolverCtx : SolverCtxBase {
     bool defect = false;
     double* p0 = nullptr;
     double* u0 = nullptr;
-    // one instantiated loop graph per apply mode (plain, defect-corrected)
-    cudaGraphExec_t exec_m[2] = {nullptr, nullptr};
-    cudaGraph_t graph_m[2] = {nullptr, nullptr};
-    int graph_B_m[2] = {0, 0};
+    // instantiated loop graphs, keyed by (apply mode: plain / defect-
+    // corrected, instance): instance -1 is the graph of all B instances,
+    // instance b >= 0 the graph of instance b alone
+    struct LoopGraph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        int B = 0;
+    };
+    std::map<std::pair<int, int>, LoopGraph> graphs;
     // Private non-blocking stream: the loop graph is captured and launched
     // here (the legacy NULL stream a caller may pass cannot be captured);
     // entry and exit are fenced to the caller's stream with events.
@@ -1130,14 +1140,42 @@ struct SolverCtx : SolverCtxBase {
         drop_graph();  // the graph bakes the history pointer
     }
     void drop_graph() {
-        for (int m = 0; m < 2; ++m) {
-            if (exec_m[m]) cudaGraphExecDestroy(exec_m[m]);
-            if (graph_m[m]) cudaGraphDestroy(graph_m[m]);
-            exec_m[m] = nullptr;
-            graph_m[m] = nullptr;
-            graph_B_m[m] = 0;
+        for (auto& kv : graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
         }
+        graphs.clear();
     }
+    // The context seen as instance b0 alone: every per-instance pointer
+    // offset to b0 (restored on destruction), so enqueue_iteration(s, 1)
+    // captures instance b0's iteration with gridDim.y = 1.
+    struct InstanceView {
+        SolverCtx& c;
+        T *p, *t, *u, *g, *gprev, *z, *r, *best, *g0c;
+        uint8_t* mask;
+        double *part, *p0, *u0;
+        PkState* st;
+        PkParams* Pd;
+        InstanceView(SolverCtx& cx, int b0)
+            : c(cx), p(cx.p), t(cx.t), u(cx.u), g(cx.g), gprev(cx.gprev), z(cx.z), r(cx.r),
+              best(cx.best), g0c(cx.g0c), mask(cx.mask), part(cx.part), p0(cx.p0), u0(cx.u0),
+              st(cx.st), Pd(cx.Pd) {
+            const size_t o = (size_t)b0 * cx.N;
+            T** vs[] = {&cx.p, &cx.t, &cx.u, &cx.g, &cx.gprev, &cx.z, &cx.r, &cx.best, &cx.g0c};
+            for (T** v : vs) *v += o;
+            cx.mask += o;
+            cx.part += (size_t)b0 * kPartStride;
+            if (cx.p0) cx.p0 += o;
+            if (cx.u0) cx.u0 += o;
+            cx.st += b0;
+            cx.Pd += b0;
+        }
+        ~InstanceView() {
+            c.p = p; c.t = t; c.u = u; c.g = g; c.gprev = gprev; c.z = z; c.r = r;
+            c.best = best; c.g0c = g0c; c.mask = mask; c.part = part; c.p0 = p0; c.u0 = u0;
+            c.st = st; c.Pd = Pd;
+        }
+    };
     // switch the loop's applies between exact and defect-corrected (FP64
     // contexts only); allocates p0 / u0 on first use, outside any capture
     void set_defect(bool on) {
@@ -1238,30 +1276,35 @@ struct SolverCtx : SolverCtxBase {
         count_launches(1);
         ASB_CUDA(cudaGetLastError());
     }
-    void build_graph(cudaStream_t s, int B) {
-        const int m = defect;
-        if (exec_m[m]) cudaGraphExecDestroy(exec_m[m]);
-        if (graph_m[m]) cudaGraphDestroy(graph_m[m]);
-        exec_m[m] = nullptr;
-        graph_m[m] = nullptr;
-        graph_B_m[m] = 0;
-        cudaGraph_t& graph = graph_m[m];
-        ASB_CUDA(cudaGraphCreate(&graph, 0));
+    // capture the loop graph of all B instances (b0 < 0) or of instance b0
+    // alone; the caller holds setup_mutex()
+    void build_graph(cudaStream_t s, int B, int b0) {
+        LoopGraph& lg = graphs[std::make_pair((int)defect, b0)];
+        if (lg.exec) cudaGraphExecDestroy(lg.exec);
+        if (lg.graph) cudaGraphDestroy(lg.graph);
+        lg = LoopGraph{};
+        ASB_CUDA(cudaGraphCreate(&lg.graph, 0));
         cudaGraphConditionalHandle h;
-        ASB_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+        ASB_CUDA(cudaGraphConditionalHandleCreate(&h, lg.graph, 1, cudaGraphCondAssignDefault));
         cudaGraphNodeParams cp = {};
         cp.type = cudaGraphNodeTypeConditional;
         cp.conditional.handle = h;
         cp.conditional.type = cudaGraphCondTypeWhile;
         cp.conditional.size = 1;
         cudaGraphNode_t node;
-        ASB_CUDA(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+        ASB_CUDA(cudaGraphAddNode(&node, lg.graph, nullptr, 0, &cp));
         cudaGraph_t body = cp.conditional.phGraph_out[0];
         ASB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeRelaxed));
         try {
-            enqueue_iteration(s, B);
-            k_loop_cond<<<1, 32, 0, s>>>(h, st, B);
+            if (b0 >= 0) {
+                InstanceView view(*this, b0);
+                enqueue_iteration(s, 1);
+                k_loop_cond<<<1, 32, 0, s>>>(h, st, 1, 1);
+            } else {
+                enqueue_iteration(s, B);
+                k_loop_cond<<<1, 32, 0, s>>>(h, st, B, B > 1 ? 2 : 1);
+            }
         } catch (...) {
             // leave no capture open on the stream, then report the failure
             cudaGraph_t partial = nullptr;
@@ -1272,31 +1315,43 @@ struct SolverCtx : SolverCtxBase {
         }
         cudaGraph_t captured = nullptr;
         ASB_CUDA(cudaStreamEndCapture(s, &captured));
-        ASB_CUDA(cudaGraphInstantiate(&exec_m[defect], graph_m[defect], 0));
-        graph_B_m[defect] = B;
+        ASB_CUDA(cudaGraphInstantiate(&lg.exec, lg.graph, 0));
+        lg.B = B;
     }
-    // (Re)build the loop graph if needed.  Before capturing, one fully gated
+    // (Re)build a loop graph if needed.  Before capturing, one fully gated
     // iteration runs eagerly (every kernel returns at entry) so that all
-    // function attributes are set outside the capture.  Clobbers st; the
-    // caller writes the initial states afterwards.
-    // The capture holds setup_mutex(): no other host thread may synchronise
-    // the device (a set-up call) while this stream is capturing.
-    void ensure_graph(cudaStream_t s, int B) {
-        if (exec_m[defect] && graph_B_m[defect] == B) return;
+    // function attributes are set outside the capture.  Clobbers the device
+    // states of the instances it covers; the caller writes the states
+    // afterwards.  The capture holds setup_mutex(): no other host thread may
+    // synchronise the device (a set-up call) while this stream is capturing.
+    void ensure_graph(cudaStream_t s, int B, int b0 = -1) {
+        auto it = graphs.find(std::make_pair((int)defect, b0));
+        if (it != graphs.end() && it->second.exec && it->second.B == B) return;
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
-        std::vector<PkState> gated(B);
-        std::memset(gated.data(), 0, B * sizeof(PkState));
+        const int nb = b0 >= 0 ? 1 : B;
+        std::vector<PkState> gated(nb);
+        std::memset(gated.data(), 0, nb * sizeof(PkState));
         for (auto& x : gated) {
             x.halt = H_FINAL;
             x.skip_mv1 = 1;
         }
-        ASB_CUDA(cudaMemcpyAsync(st, gated.data(), B * sizeof(PkState), cudaMemcpyHostToDevice, s));
-        enqueue_iteration(s, B);
+        ASB_CUDA(cudaMemcpyAsync(st + (b0 >= 0 ? b0 : 0), gated.data(), nb * sizeof(PkState),
+                                 cudaMemcpyHostToDevice, s));
+        if (b0 >= 0) {
+            InstanceView view(*this, b0);
+            enqueue_iteration(s, 1);
+        } else {
+            enqueue_iteration(s, B);
+        }
         ASB_CUDA(cudaStreamSynchronize(s));
-        build_graph(s, B);
+        build_graph(s, B, b0);
     }
-    void launch_graph(cudaStream_t s) {
-        ASB_CUDA(cudaGraphLaunch(exec_m[defect], s));
+    bool has_graph(int b0) const {
+        auto it = graphs.find(std::make_pair((int)defect, b0));
+        return it != graphs.end() && it->second.exec;
+    }
+    void launch_graph(cudaStream_t s, int b0 = -1) {
+        ASB_CUDA(cudaGraphLaunch(graphs.at(std::make_pair((int)defect, b0)).exec, s));
         count_launches(1);
     }
     // ASPHER_EAGER_LOOP=1: enqueue iterations as plain launches instead of the
@@ -1594,7 +1649,21 @@ struct Solver {
             if (SolverCtx<T>::eager_loop()) {
                 for (int k = 0; k < 8; ++k) c.enqueue_iteration(s, B);
             } else {
-                c.launch_graph(s);
+                // the batch graph runs while two or more instances run; the
+                // last one continues in its own graph, whose kernels launch
+                // no blocks for the halted instances
+                int nrun = 0, last = -1;
+                for (int b = 0; b < B; ++b)
+                    if (h[b].halt == H_RUN) { ++nrun; last = b; }
+                if (B > 1 && nrun == 1) {
+                    if (!c.has_graph(last)) {
+                        c.ensure_graph(s, 1, last);  // clobbers st[last]
+                        write_states();
+                    }
+                    c.launch_graph(s, last);
+                } else {
+                    c.launch_graph(s);
+                }
             }
             read_states();
             bool changed = false;
