@@ -21,6 +21,7 @@
 
 #include <algorithm>
 #include <map>
+#include <tuple>
 #include <utility>
 #include <chrono>
 #include <cmath>
@@ -1014,16 +1015,14 @@ __global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, cons
 }
 
 // ---- device-side loop control -------------------------------------------------------
-// Last kernel of the graph body: keep looping while at least min_run
-// instances are running (a batch graph hands its last running instance to
-// that instance's own loop graph, whose kernels launch no gated blocks).
-__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st, int B, int min_run) {
-    // one warp: count the running instances
-    int run = 0;
-    for (int b = threadIdx.x; b < B; b += 32) run += (st[b].halt == H_RUN);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) run += __shfl_xor_sync(0xffffffffu, run, o);
-    if (threadIdx.x == 0) cudaGraphSetConditional(h, run >= min_run ? 1u : 0u);
+// Last kernel of the graph body of instances [0, n) (a range of the batch):
+// keep looping while both end instances are running.  When an end instance
+// halts the host continues with the loop graph of the smaller range that
+// covers the instances still running, so halted instances at the ends stop
+// costing gated blocks.
+__global__ void k_loop_cond(cudaGraphConditionalHandle h, const PkState* st, int n) {
+    if (threadIdx.x == 0)
+        cudaGraphSetConditional(h, (st[0].halt == H_RUN && st[n - 1].halt == H_RUN) ? 1u : 0u);
 }
 
 // ---- host driver -----------------------------------------------------------------
@@ -1079,14 +1078,13 @@ struct SolverCtx : SolverCtxBase {
     double* p0 = nullptr;
     double* u0 = nullptr;
     // instantiated loop graphs, keyed by (apply mode: plain / defect-
-    // corrected, instance): instance -1 is the graph of all B instances,
-    // instance b >= 0 the graph of instance b alone
+    // corrected, first instance, number of instances): the graph of the
+    // instance range [lo, lo + n) of a batch
     struct LoopGraph {
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
-        int B = 0;
     };
-    std::map<std::pair<int, int>, LoopGraph> graphs;
+    std::map<std::tuple<int, int, int>, LoopGraph> graphs;
     // Private non-blocking stream: the loop graph is captured and launched
     // here (the legacy NULL stream a caller may pass cannot be captured);
     // entry and exit are fenced to the caller's stream with events.
@@ -1146,9 +1144,9 @@ struct SolverCtx : SolverCtxBase {
         }
         graphs.clear();
     }
-    // The context seen as instance b0 alone: every per-instance pointer
-    // offset to b0 (restored on destruction), so enqueue_iteration(s, 1)
-    // captures instance b0's iteration with gridDim.y = 1.
+    // The context seen from instance b0 on: every per-instance pointer
+    // offset to b0 (restored on destruction), so enqueue_iteration(s, n)
+    // captures the iteration of instances [b0, b0 + n) with gridDim.y = n.
     struct InstanceView {
         SolverCtx& c;
         T *p, *t, *u, *g, *gprev, *z, *r, *best, *g0c;
@@ -1276,10 +1274,10 @@ struct SolverCtx : SolverCtxBase {
         count_launches(1);
         ASB_CUDA(cudaGetLastError());
     }
-    // capture the loop graph of all B instances (b0 < 0) or of instance b0
-    // alone; the caller holds setup_mutex()
-    void build_graph(cudaStream_t s, int B, int b0) {
-        LoopGraph& lg = graphs[std::make_pair((int)defect, b0)];
+    // capture the loop graph of instances [lo, lo + n); the caller holds
+    // setup_mutex()
+    void build_graph(cudaStream_t s, int lo, int n) {
+        LoopGraph& lg = graphs[std::make_tuple((int)defect, lo, n)];
         if (lg.exec) cudaGraphExecDestroy(lg.exec);
         if (lg.graph) cudaGraphDestroy(lg.graph);
         lg = LoopGraph{};
@@ -1297,14 +1295,9 @@ struct SolverCtx : SolverCtxBase {
         ASB_CUDA(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
                                                cudaStreamCaptureModeRelaxed));
         try {
-            if (b0 >= 0) {
-                InstanceView view(*this, b0);
-                enqueue_iteration(s, 1);
-                k_loop_cond<<<1, 32, 0, s>>>(h, st, 1, 1);
-            } else {
-                enqueue_iteration(s, B);
-                k_loop_cond<<<1, 32, 0, s>>>(h, st, B, B > 1 ? 2 : 1);
-            }
+            InstanceView view(*this, lo);
+            enqueue_iteration(s, n);
+            k_loop_cond<<<1, 32, 0, s>>>(h, st, n);
         } catch (...) {
             // leave no capture open on the stream, then report the failure
             cudaGraph_t partial = nullptr;
@@ -1316,42 +1309,38 @@ struct SolverCtx : SolverCtxBase {
         cudaGraph_t captured = nullptr;
         ASB_CUDA(cudaStreamEndCapture(s, &captured));
         ASB_CUDA(cudaGraphInstantiate(&lg.exec, lg.graph, 0));
-        lg.B = B;
     }
-    // (Re)build a loop graph if needed.  Before capturing, one fully gated
-    // iteration runs eagerly (every kernel returns at entry) so that all
-    // function attributes are set outside the capture.  Clobbers the device
-    // states of the instances it covers; the caller writes the states
-    // afterwards.  The capture holds setup_mutex(): no other host thread may
-    // synchronise the device (a set-up call) while this stream is capturing.
-    void ensure_graph(cudaStream_t s, int B, int b0 = -1) {
-        auto it = graphs.find(std::make_pair((int)defect, b0));
-        if (it != graphs.end() && it->second.exec && it->second.B == B) return;
+    // Build the loop graph of instances [lo, lo + n) if needed.  Before
+    // capturing, one fully gated iteration of those instances runs eagerly
+    // (every kernel returns at entry) so that all function attributes are set
+    // outside the capture: it clobbers their device states, which the caller
+    // writes afterwards.  The capture holds setup_mutex(): no other host
+    // thread may synchronise the device (a set-up call) while this stream is
+    // capturing.
+    bool has_graph(int lo, int n) const {
+        auto it = graphs.find(std::make_tuple((int)defect, lo, n));
+        return it != graphs.end() && it->second.exec;
+    }
+    void ensure_graph(cudaStream_t s, int lo, int n) {
+        if (has_graph(lo, n)) return;
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
-        const int nb = b0 >= 0 ? 1 : B;
-        std::vector<PkState> gated(nb);
-        std::memset(gated.data(), 0, nb * sizeof(PkState));
+        std::vector<PkState> gated(n);
+        std::memset(gated.data(), 0, n * sizeof(PkState));
         for (auto& x : gated) {
             x.halt = H_FINAL;
             x.skip_mv1 = 1;
         }
-        ASB_CUDA(cudaMemcpyAsync(st + (b0 >= 0 ? b0 : 0), gated.data(), nb * sizeof(PkState),
+        ASB_CUDA(cudaMemcpyAsync(st + lo, gated.data(), n * sizeof(PkState),
                                  cudaMemcpyHostToDevice, s));
-        if (b0 >= 0) {
-            InstanceView view(*this, b0);
-            enqueue_iteration(s, 1);
-        } else {
-            enqueue_iteration(s, B);
+        {
+            InstanceView view(*this, lo);
+            enqueue_iteration(s, n);
         }
         ASB_CUDA(cudaStreamSynchronize(s));
-        build_graph(s, B, b0);
+        build_graph(s, lo, n);
     }
-    bool has_graph(int b0) const {
-        auto it = graphs.find(std::make_pair((int)defect, b0));
-        return it != graphs.end() && it->second.exec;
-    }
-    void launch_graph(cudaStream_t s, int b0 = -1) {
-        ASB_CUDA(cudaGraphLaunch(graphs.at(std::make_pair((int)defect, b0)).exec, s));
+    void launch_graph(cudaStream_t s, int lo, int n) {
+        ASB_CUDA(cudaGraphLaunch(graphs.at(std::make_tuple((int)defect, lo, n)).exec, s));
         count_launches(1);
     }
     // ASPHER_EAGER_LOOP=1: enqueue iterations as plain launches instead of the
@@ -1636,7 +1625,7 @@ struct Solver {
                 for (int b = 0; b < B; ++b) ih[b].mv_host += 1;
             }
         }
-        if (!SolverCtx<T>::eager_loop()) c.ensure_graph(s, B);
+        if (!SolverCtx<T>::eager_loop()) c.ensure_graph(s, 0, B);
         write_states();
 
         // ---- the loop: device-driven, the host services rare branches
@@ -1649,21 +1638,21 @@ struct Solver {
             if (SolverCtx<T>::eager_loop()) {
                 for (int k = 0; k < 8; ++k) c.enqueue_iteration(s, B);
             } else {
-                // the batch graph runs while two or more instances run; the
-                // last one continues in its own graph, whose kernels launch
-                // no blocks for the halted instances
-                int nrun = 0, last = -1;
+                // the loop graph of the smallest instance range that covers
+                // every running instance: halted instances outside it launch
+                // no (gated) blocks
+                int lo = -1, hi = -1;
                 for (int b = 0; b < B; ++b)
-                    if (h[b].halt == H_RUN) { ++nrun; last = b; }
-                if (B > 1 && nrun == 1) {
-                    if (!c.has_graph(last)) {
-                        c.ensure_graph(s, 1, last);  // clobbers st[last]
-                        write_states();
+                    if (h[b].halt == H_RUN) {
+                        if (lo < 0) lo = b;
+                        hi = b;
                     }
-                    c.launch_graph(s, last);
-                } else {
-                    c.launch_graph(s);
+                const int n = hi - lo + 1;
+                if (!c.has_graph(lo, n)) {
+                    c.ensure_graph(s, lo, n);  // clobbers st[lo, lo + n)
+                    write_states();
                 }
+                c.launch_graph(s, lo, n);
             }
             read_states();
             bool changed = false;
