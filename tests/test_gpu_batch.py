@@ -47,6 +47,27 @@ def test_batch_equals_single(backend, dtype):
         assert abs(r.contact_area - r1.contact_area) <= 1e-12
 
 
+@pytest.mark.parametrize("loads", [[0.03, 0.002, 0.01, 0.03], [0.002, 0.03, 0.03, 0.01]])
+def test_batch_any_halting_order(loads):
+    """The loop graph covers the smallest instance range holding every
+    running instance, and shrinks it as end instances halt: instances that
+    halt in the middle of the range, at its ends, or in either order keep
+    the single-solve results."""
+    from aspher_b200 import Operator, solve_device, solve_device_batch
+    Ns = 64
+    op = Operator("periodic", Ns)
+    gaps = [torch.as_tensor(_rough(Ns, 60 + i), device="cuda") for i in range(len(loads))]
+    rb = solve_device_batch(op, gaps, loads, tol=1e-9, precond="fourier")
+    its = []
+    for g, pn, r in zip(gaps, loads, rb):
+        r1 = solve_device(op, g, pn, tol=1e-9, precond="fourier", light=True, keep_best=True)
+        assert r.status == r1.status == "converged"
+        assert r.iterations == r1.iterations
+        assert rel(r.pressure, r1.pressure) <= 1e-12
+        its.append(r.iterations)
+    assert len(set(its)) > 1  # the instances do halt at different iterations
+
+
 def test_batch_with_identification_and_maxiter():
     from aspher_b200 import Operator, solve_device, solve_device_batch
     Ns = 16
