@@ -273,12 +273,14 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
     };
     // split step of the real transform: X[k] = E + w^k O with
     // E = (Z[k] + conj Z[-k])/2, O = (Z[k] - conj Z[-k])/(2i), k in [0, LR]
-    auto split = [&](cplx<T> zk, cplx<T> zn, int k) {
+    auto split_w = [&](cplx<T> zk, cplx<T> zn, cplx<T> w) {
         const cplx<T> A = mk<T>(zk.x + zn.x, zk.y - zn.y);
         const cplx<T> B = mk<T>(zk.x - zn.x, zk.y + zn.y);
         const cplx<T> O = mk<T>(B.y * T(0.5), -B.x * T(0.5));
-        const cplx<T> w = __ldg(&tw_2lr[k]);
         return cadd(cscale(A, T(0.5)), cmul(w, O));
+    };
+    auto split = [&](cplx<T> zk, cplx<T> zn, int k) {
+        return split_w(zk, zn, __ldg(&tw_2lr[k]));
     };
     // transform of group grp from the strided registers v, and its store
     auto body = [&](int grp, cplx<T> (&v)[RPT]) {
@@ -300,20 +302,42 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             const bool full = nr == RB;
             const int lchunk = lct + ilog2c(RB);
             cplx<T>* base = st.base + blockIdx.y * st.bs + (size_t)row0 * ct;
-            for (int f = threadIdx.x; f < ntiles * chunk; f += blockDim.x) {
-                const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
-                const int rr = e >> lct, c = e & (ct - 1);
-                const int k = j * ct + c;
-                if (k > LR) continue;
-                const int o = rr * sm_len(LR + 1);
-                const cplx<T> zk = sm[smaddr(k & (LR - 1), 1, o)];
-                cplx<T> X;
-                if (k == LR) {
-                    X = mk<T>(zk.x - zk.y, T(0));  // zk = Z[0]
-                } else {
-                    X = split(zk, sm[smaddr((LR - k) & (LR - 1), 1, o)], k);
+            const int total = ntiles * chunk;
+            // U outputs per thread at a time: their shared-memory reads and
+            // twiddle loads are all issued before the first is used (U = 1
+            // where the launch's register budget is below 96)
+            constexpr int REGCAP = 65536 / (row_threads<T>(LR, V) * row_minb<T>(LR, V));
+            constexpr int U = REGCAP < 96 ? 1 : (sizeof(T) == 4 ? 4 : 2);
+            for (int f0 = threadIdx.x; f0 < total; f0 += U * blockDim.x) {
+                cplx<T> zk[U], zn[U], w[U];
+                size_t at[U];
+                int kk[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int f = f0 + u * (int)blockDim.x;
+                    kk[u] = LR + 1;  // no output
+                    if (f < total) {
+                        const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
+                        const int rr = e >> lct, c = e & (ct - 1);
+                        const int k = j * ct + c;
+                        if (k <= LR) {
+                            const int o = rr * sm_len(LR + 1);
+                            kk[u] = k;
+                            at[u] = (size_t)j * st.nrows * ct + e;
+                            zk[u] = sm[smaddr(k & (LR - 1), 1, o)];
+                            zn[u] = sm[smaddr((LR - k) & (LR - 1), 1, o)];
+                            w[u] = __ldg(&tw_2lr[k < LR ? k : 0]);
+                        }
+                    }
                 }
-                base[(size_t)j * st.nrows * ct + e] = X;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    if (kk[u] > LR) continue;
+                    // k == LR: zk = Z[0], X = Re Z0 - Im Z0
+                    const cplx<T> X = kk[u] == LR ? mk<T>(zk[u].x - zk[u].y, T(0))
+                                                  : split_w(zk[u], zn[u], w[u]);
+                    base[at[u]] = X;
+                }
             }
         } else {
             const cplx<T> z0 = v[0];
