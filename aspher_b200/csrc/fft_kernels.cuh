@@ -472,11 +472,15 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         const int row = grp * RB + r;
         const bool valid = row < nrows;
         cplx<T> v[RPT];
+        // padded-layout addresses of Z[k] and Z[LR - k]: per-thread bases
+        // plus compile-time steps when TT is a multiple of 16
+        constexpr int DSTEP = TT % 16 == 0 ? TT + TT / 16 : 0;
+        const int ak = smaddr(t, 1, off), an = smaddr(LR - t, 1, off);
 #pragma unroll
         for (int m = 0; m < RPT; ++m) {
             const int k = t + m * TT;
-            const cplx<T> xk = src[smaddr(k, 1, off)];
-            const cplx<T> xn = src[smaddr(LR - k, 1, off)];
+            const cplx<T> xk = src[DSTEP ? ak + m * DSTEP : smaddr(k, 1, off)];
+            const cplx<T> xn = src[DSTEP ? an - m * DSTEP : smaddr(LR - k, 1, off)];
             const cplx<T> A = mk<T>(xk.x + xn.x, xk.y - xn.y);
             const cplx<T> B = mk<T>(xk.x - xn.x, xk.y + xn.y);
             const cplx<T> Bw = cmulc(B, __ldg(&tw_2lr[k]));  // B * exp(+2 pi i k / 2LR)
