@@ -101,7 +101,7 @@ __device__ __forceinline__ T gc(T v, T aT) { return v - aT; }
 // Real difference; in FP64 to ~1e-16 relative).  pk = sum p |g| is not
 // linear; k_evalpk computes it when a history is recorded and at the end.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_eval(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_eval(const PkParams* __restrict__ Pp, PkState* st,
                                                       const T* u, const T* g0, const T* p, T* g,
                                                       uint8_t* mask, double* part,
                                                       int final_mode) {
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(kRedThreads) k_eval(const PkParams* __restrict
 // recorded in the history); runs after k_eval of a recorded iteration
 // (pk_due) or in final mode.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_evalpk(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_evalpk(const PkParams* __restrict__ Pp, PkState* st,
                                                         const T* p, const T* g, double* part,
                                                         double* hist, int final_mode) {
     Pp += blockIdx.y;
@@ -637,7 +637,7 @@ __device__ __forceinline__ T zfinal(const PkParams& P, T z, T g, T zm) {
 // dots for the unpreconditioned and the FFT-preconditioned loops (z from the
 // preconditioner; g centred on the fly)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict__ Pp, PkState* st, const T* z,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_dots(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, const T* gprev,
                                                       const uint8_t* mask, double* part) {
     // instance blockIdx.y of a batched solve (0 when unbatched)
@@ -682,7 +682,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dots(const PkParams* __restrict
 // copy_best) before the t apply; k_rden consumes r after it.  pk_apply_t is
 // the same pair fused into the apply's row kernels (ASPHER_FUSED_T=1).
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, T* gprev, T* t,
                                                       const uint8_t* mask, const T* p, T* best) {
     // instance blockIdx.y of a batched solve (0 when unbatched)
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(kRedThreads) k_tupd(const PkParams* __restrict
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_rden(const PkParams* __restrict__ Pp, PkState* st, const T* r,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_rden(const PkParams* __restrict__ Pp, PkState* st, const T* r,
                                                       const T* g, const T* t,
                                                       const uint8_t* mask, double* part) {
     // instance blockIdx.y of a batched solve (0 when unbatched)
@@ -762,7 +762,7 @@ __global__ void __launch_bounds__(kRedThreads) k_rden(const PkParams* __restrict
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict__ Pp, PkState* st, T* p, const T* t,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_pupd(const PkParams* __restrict__ Pp, PkState* st, T* p, const T* t,
                                                       const T* g, double* part) {
     // instance blockIdx.y of a batched solve (0 when unbatched)
     Pp += blockIdx.y;
@@ -811,7 +811,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pupd(const PkParams* __restrict
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_rescale(const PkParams* __restrict__ Pp, PkState* st, T* p,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_rescale(const PkParams* __restrict__ Pp, PkState* st, T* p,
                                                          double* part) {
     // instance blockIdx.y of a batched solve (0 when unbatched)
     Pp += blockIdx.y;
@@ -846,7 +846,7 @@ __global__ void __launch_bounds__(kRedThreads) k_rescale(const PkParams* __restr
 //                    4: count/sum of x > theta
 //                    5: objective = sum p(0.5u + g0s)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_reduce(const PkParams* __restrict__ Pp, PkState* st, int mode,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_reduce(const PkParams* __restrict__ Pp, PkState* st, int mode,
                                                         const T* a, const T* b, const T* c,
                                                         const T* d, double theta,
                                                         double* part) {
@@ -905,7 +905,7 @@ __global__ void __launch_bounds__(kRedThreads) k_reduce(const PkParams* __restri
 
 // gd = sum double(g) * double(z - p)  (contact_solver.cpp:345-346)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_gd(const PkParams* __restrict__ Pp, PkState* st, const T* g,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_gd(const PkParams* __restrict__ Pp, PkState* st, const T* g,
                                                     const T* z, const T* p, double* part) {
     const PkParams& P = *Pp;
     double acc[1] = {0};
@@ -1002,7 +1002,7 @@ __global__ void k_sub_zmean(long N, T* z, const uint8_t* mask, const PkState* st
 
 // contact sum / count of g for the standalone preconditioner
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_gmean(long N, PkState* st, const T* g,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_gmean(long N, PkState* st, const T* g,
                                                        const uint8_t* mask, double* part) {
     double acc[2] = {0, 0};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
@@ -2124,7 +2124,7 @@ template void precond_apply_impl<double>(Operator&, int, int, const double*, con
 namespace {
 
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_init(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_init(const PkParams* __restrict__ Pp, PkState* st,
                                                           const double* p, const double* w,
                                                           uint8_t* mask, T* wT, double* part) {
     const PkParams& P = *Pp;
@@ -2148,7 +2148,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_init(const PkParams* __rest
 
 // r = Pi w, lam = d = 0, |r0|^2
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_r0(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_r0(const PkParams* __restrict__ Pp, PkState* st,
                                                         const uint8_t* mask, const T* wT, T* r,
                                                         T* lam, T* d, double* part) {
     const PkParams& P = *Pp;
@@ -2176,7 +2176,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_r0(const PkParams* __restri
 
 // rz = <Pi z, r>, beta = rz / rz_old; z = r when unpreconditioned
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_rz(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_rz(const PkParams* __restrict__ Pp, PkState* st,
                                                         const T* z, const T* r,
                                                         const uint8_t* mask, double* part) {
     const PkParams& P = *Pp;
@@ -2206,7 +2206,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_rz(const PkParams* __restri
 
 // d = Pi z + beta d on C
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_d(const PkParams* __restrict__ Pp, const PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_d(const PkParams* __restrict__ Pp, const PkState* st,
                                                        const T* z, const uint8_t* mask, T* d) {
     const PkParams& P = *Pp;
     if (st->halt) return;
@@ -2225,7 +2225,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_d(const PkParams* __restric
 
 // a = rz / <d, q>, qm = contact mean of q (q = S d)
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_dq(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_dq(const PkParams* __restrict__ Pp, PkState* st,
                                                         const T* d, const T* q,
                                                         const uint8_t* mask, double* part) {
     const PkParams& P = *Pp;
@@ -2255,7 +2255,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_dq(const PkParams* __restri
 
 // lam += a d; r -= a Pi q; convergence |r| <= tol |r0|
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_upd(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_upd(const PkParams* __restrict__ Pp, PkState* st,
                                                          const T* d, const T* q,
                                                          const uint8_t* mask, T* lam, T* r,
                                                          double* part) {
@@ -2299,7 +2299,7 @@ __global__ void __launch_bounds__(kRedThreads) k_adj_upd(const PkParams* __restr
 
 // mu = mean_C(S lam - w); grad_g0 = -lam on C (0 off C), FP64
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads) k_adj_out(const PkParams* __restrict__ Pp, PkState* st,
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_out(const PkParams* __restrict__ Pp, PkState* st,
                                                          const T* q, const T* wT, const T* lam,
                                                          const uint8_t* mask, double* grad,
                                                          double* part) {

@@ -9,6 +9,9 @@
 namespace asb {
 
 constexpr int kRedThreads = 256;
+// the vector passes run kMaxBlocks / 2 = 4 x 148 blocks: with at most 64
+// registers per thread all of them are resident at once (one wave)
+constexpr int kRedMinBlocks = 4;
 // upper bound on the grid of the vector-pass reducing kernels
 constexpr int kMaxBlocks = 1184;
 // partials per instance of a batched solve: 8 values for the largest grid of
