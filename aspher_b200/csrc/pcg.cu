@@ -599,10 +599,11 @@ void launch_stencil(int R, int Ns, dim3 grid, cudaStream_t s, const PkParams* Pp
                     const StencilW& W, const T* g, const T* gprev, const uint8_t* mask, T* z,
                     double* part, int gated) {
     if (Ns >= kSwSeg) {
-        // strips of 32, 16 or 8 rows: the longest that still gives every
-        // SM about 16 resident warps (a shorter strip re-reads more halo rows)
+        // strips of 32, 16 or 8 rows: the longest that still gives every SM
+        // 12 or more warps (a shorter strip re-reads more halo rows; at
+        // Ns=2048 16-row strips measured 1 % faster per solve than 8 or 32)
         int rows = kSwRows;
-        const long want = 16L * num_sms();
+        const long want = 12L * num_sms();
         while (rows > 8 && (long)(Ns / kSwSeg) * (Ns / rows) * grid.y < want) rows /= 2;
         const int strips = (Ns / kSwSeg) * (Ns / rows);
         int nb = (strips + kSwWarps - 1) / kSwWarps;
