@@ -424,7 +424,7 @@ def run_ours(args):
     # the FP64 solve
     adj = None
     if rank == 0 and not os.environ.get("BENCH_SKIP_ADJOINT"):
-        adj = adjoint_check(dev, n_dirs=int(os.environ.get("BENCH_ADJ_DIRS", "16")))
+        adj = adjoint_check(dev, n_dirs=int(os.environ.get("BENCH_ADJ_DIRS", "64")))
 
     if rank == 0:
         line = {
@@ -526,7 +526,10 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     contact-boundary points in and out of contact, so their central
     differences do not converge to the (one-sided) derivative at this step --
     the difference to the adjoint shrinks with the step (1.4e-2 -> 6e-4 from
-    1e-6 to 1e-8 rms) while smooth directions agree to 1e-7."""
+    1e-6 to 1e-8 rms) while smooth directions agree to 1e-7.  Surface-law
+    steps can move a few boundary cells as well; every direction reports how
+    many cells its +h and -h solves moved, and the per-direction 1e-4 gate
+    applies to the directions that moved none (at least half of them must)."""
     import numpy as np
     import torch
     import aspher_b200 as asb
@@ -569,10 +572,16 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     errn = {"f64": [], "f32": []}
     pairs = []
     dn = float(np.sqrt(N))  # |d| of a unit-RMS direction
+    c0 = p0 > 0
+    moved = []  # cells whose contact state differs from the base solve at +h / -h
     for k in range(n_dirs):
         d = torch.from_numpy(self_affine_gap(Ns, hurst=0.8, rms=1.0, seed=100 + k)).to(dev)
         d /= torch.sqrt(torch.mean(d ** 2))
-        fd = (L_of(g0 + h * d, warm=p0)[0] - L_of(g0 - h * d, warm=p0)[0]) / (2 * h)
+        Lp, rp = L_of(g0 + h * d, warm=p0)
+        Lm, rm = L_of(g0 - h * d, warm=p0)
+        fd = (Lp - Lm) / (2 * h)
+        moved.append(int(((rp.pressure_device > 0) != c0).sum()) +
+                     int(((rm.pressure_device > 0) != c0).sum()))
         for name in errs:
             ad = float(torch.dot(grads[name][0], d))
             errs[name].append(abs(ad - fd) / max(abs(fd), 1e-300))
@@ -581,17 +590,27 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
                 pairs.append([ad, fd])
     hp = 1e-6 * pbar
     fdp = (L_of(g0, pbar + hp, warm=p0)[0] - L_of(g0, pbar - hp, warm=p0)[0]) / (2 * hp)
+    # a step that moves contact-boundary cells crosses a kink of L(gap): its
+    # central difference is not the derivative there, so the per-direction
+    # gate applies to the directions whose +h and -h solves keep the base
+    # contact set (all of them are reported)
+    keep = [i for i in range(n_dirs) if moved[i] == 0]
     for name in errs:
         out[name]["n_within_1e-4"] = sum(e <= 1e-4 for e in errs[name])
+        out[name]["max_rel_err_fd_gap_same_set"] = max([errs[name][i] for i in keep], default=None)
         out[name]["max_rel_err_fd_gap"] = max(errs[name])
         out[name]["median_rel_err_fd_gap"] = float(np.median(errs[name]))
         out[name]["max_err_rel_grad_norm"] = max(errn[name])
         out[name]["rel_err_fd_pnominal"] = abs(grads[name][1] - fdp) / abs(fdp)
     out["f64_adjoint_vs_fd_pairs"] = pairs
     out["fd_directions"] = n_dirs
+    out["fd_same_contact_set"] = len(keep)
+    out["fd_cells_moved"] = moved
     out["fd_step"] = "1e-6 * rms(gap); directions: self-affine random fields (seeds 100..), unit RMS"
-    out["pass"] = all(out[n]["max_rel_err_fd_gap"] <= 1e-4 and
-                      out[n]["rel_err_fd_pnominal"] <= 1e-4 for n in errs)
+    out["pass"] = len(keep) >= n_dirs // 2 and all(
+        out[n]["max_rel_err_fd_gap_same_set"] <= 1e-4 and
+        out[n]["max_err_rel_grad_norm"] <= 1e-4 and
+        out[n]["rel_err_fd_pnominal"] <= 1e-4 for n in errs)
     return out
 
 
