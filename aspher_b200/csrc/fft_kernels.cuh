@@ -602,4 +602,53 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     }
 }
 
+// ---- split column (free space, the length-2LH column too long for one CTA) -------
+// The zero-padded column transform of length M = 2 LH is evaluated as two
+// length-LH halves.  With x[n] = 0 for n >= LH and w = exp(-2 pi i / M):
+//   X[2m] = FFT_LH(x)[m],   X[2m+1] = FFT_LH(w^n x)[m],
+// and for the kept outputs n < LH (unnormalised inverse, as col_kernel)
+//   y[n] = IFFT_LH(K[2m] X[2m])[n] + w^-n IFFT_LH(K[2m+1] X[2m+1])[n].
+// PARITY 0 writes its half to `acc` (a second spectrum-shaped buffer with the
+// same tiled layout); PARITY 1 adds it and writes the column in place.  Each
+// launch reads the untouched input column, so the two launches run back to
+// back on one stream.  One column tile per CTA; shared memory col_smem<T>(LH, CT).
+template <typename T, int LH, int NCM1, int V, int PARITY, class Mult>
+__global__ void __launch_bounds__(col_threads<T>(LH, NCM1, V), col_minb<T>(LH, NCM1, V))
+col_split_kernel(cplx<T>* __restrict__ spec, cplx<T>* __restrict__ acc, int nrows, Mult mul,
+                 const cplx<T>* __restrict__ tw_lh, const cplx<T>* __restrict__ tw_m,
+                 const int* __restrict__ gate) {
+    if (gate && gate[blockIdx.y * kGateStride]) return;
+    constexpr int RPT = col_rpt<T>(LH, V);
+    constexpr int CT = col_ct_v<T>(LH, NCM1, V);
+    constexpr int TT = LH / RPT;
+    constexpr int NTILES = NCM1 / CT + 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    const int c = threadIdx.x % CT, t = threadIdx.x / CT;
+    const size_t off = (size_t)blockIdx.y * NTILES * nrows * CT + (size_t)blockIdx.x * nrows * CT;
+    cplx<T>* base = spec + off;
+    cplx<T>* abase = acc + off;
+    cplx<T> v[RPT];
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        const int n = t + m * TT;
+        v[m] = base[(size_t)n * CT + c];
+        if constexpr (PARITY) v[m] = cmul(v[m], __ldg(&tw_m[n]));
+    }
+    block_fft<T, LH, RPT, -1, CT>(v, t, sm, c, tw_lh);
+    const int kx = blockIdx.x * CT + c;
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, 2 * (t + m * TT) + PARITY);
+    block_fft<T, LH, RPT, +1, CT>(v, t, sm, c, tw_lh);
+#pragma unroll
+    for (int m = 0; m < RPT; ++m) {
+        const size_t i = (size_t)(t + m * TT) * CT + c;
+        if constexpr (PARITY) {
+            base[i] = cadd(cmulc(v[m], __ldg(&tw_m[t + m * TT])), abase[i]);
+        } else {
+            abase[i] = v[m];
+        }
+    }
+}
+
 }  // namespace asb

@@ -23,6 +23,7 @@
 
 #include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -331,6 +332,23 @@ void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gat
     k<<<dim3(gx, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
 }
 
+// the two launches of the split column transform (variant 0 only): parity 0
+// writes its half to acc, parity 1 adds it and writes the column in place
+template <typename T, int LH, int NCM1, class Mult>
+void launch_col_split(cplx<T>* spec, cplx<T>* acc, int nrows, Mult m, cudaStream_t s,
+                      const int* gate, int B = 1) {
+    constexpr int V = vclamp(LH, 0);
+    constexpr int ct = col_ct_v<T>(LH, NCM1, V), thr = col_threads<T>(LH, NCM1, V);
+    constexpr int sm = col_smem<T>(LH, ct);
+    auto k0 = col_split_kernel<T, LH, NCM1, V, 0, Mult>;
+    auto k1 = col_split_kernel<T, LH, NCM1, V, 1, Mult>;
+    fft_attrs((const void*)k0, sm);
+    fft_attrs((const void*)k1, sm);
+    const dim3 grid(NCM1 / ct + 1, B);
+    k0<<<grid, thr, sm, s>>>(spec, acc, nrows, m, tw<T>(LH), tw<T>(2 * LH), gate);
+    k1<<<grid, thr, sm, s>>>(spec, acc, nrows, m, tw<T>(LH), tw<T>(2 * LH), gate);
+}
+
 #define ASB_V_SWITCH(VV, L, ...)                                                   \
     switch (VV) {                                                                  \
         case 0: { constexpr int V = vclamp(L, 0); __VA_ARGS__; } break;            \
@@ -366,30 +384,41 @@ int col_ct_rt(int v) {
 template <typename T, int NS>
 struct FreeImpl {
     static constexpr int LR = NS, LC = 2 * NS;
+    // the length-2Ns column in one CTA's shared memory (all sizes but FP64
+    // at Ns = 8192); otherwise the column pass runs as two length-Ns halves
+    // (col_split_kernel), instantiated for Ns >= kSplitMin
     static constexpr bool kFits = col_fits<T>(LC);
-    // spectrum sized for the widest tile (16 columns)
-    static size_t spec_elems() { return (size_t)(LR + 16) * NS; }
-    static int ct(int cv) { return col_ct_rt<T, LC, LR>(cv); }
+    static constexpr bool kSplitOK = NS >= kSplitMin;
+    static_assert(kFits || kSplitOK, "a column that does not fit must have the split form");
+    static bool split(const Operator& op) { return !kFits || (kSplitOK && op.split_cols); }
+    // spectrum sized for the widest tile (16 columns); the split form keeps
+    // its first half-column result in a second spectrum-shaped block after
+    // the B instances' spectra
+    static size_t spec_elems(bool sp) { return (size_t)(LR + 16) * NS * (sp ? 2 : 1); }
+    static int ct(int cv, bool sp) {
+        return sp ? col_ct_v<T>(LR, LR, vclamp(LR, 0)) : col_ct_rt<T, LC, LR>(cv);
+    }
 
     // row_fwd(ld) -> col(x Kh) -> row_inv(st); ld / st see the Ns x Ns field(s)
     template <class Load, class Store>
     static void apply(const Operator& op, Load ld, Store st, cplx<T>* spec, cudaStream_t s,
                       const int* gate, int B) {
-        if constexpr (!kFits) {
-            throw Error(-1, "free-space FP64 apply at grid_size 8192 is not supported (the "
-                            "16384-point FP64 column does not fit one CTA's shared memory); "
-                            "use FP32 or grid_size <= 4096");
+        const int dbl = sizeof(T) == 8;
+        const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
+        const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
+        const long bsp = (long)(LR / c + 1) * NS * c;
+        row_fwd_v<T, LR, true>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
+        if (split(op)) {
+            if constexpr (kSplitOK)
+                launch_col_split<T, LR, LR>(spec, spec + (size_t)B * bsp, NS,
+                                            KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
         } else {
-            const int dbl = sizeof(T) == 8;
-            const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
-            const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
-            const long bsp = (long)(LR / c + 1) * NS * c;
-            row_fwd_v<T, LR, true>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
-            col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
-            row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
-            count_launches(3);
-            ASB_CUDA(cudaGetLastError());
+            if constexpr (kFits)
+                col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
         }
+        row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
+        count_launches(split(op) ? 4 : 3);
+        ASB_CUDA(cudaGetLastError());
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
@@ -591,6 +620,13 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ASB_CUDA(cudaGetDevice(&device));
     (void)tw_table(false, 2);
+    {
+        // ASPHER_SPLIT_COLUMNS=1: the free-space column pass in its split
+        // (two half-length) form at every size >= kSplitMin, the form that
+        // FP64 at Ns = 8192 needs (for cross-checks against the one-CTA form)
+        const char* e = std::getenv("ASPHER_SPLIT_COLUMNS");
+        split_cols = kind == OP_FFT && Ns >= kSplitMin && e && std::atoi(e) != 0;
+    }
     if (kind == OP_PERIODIC) {
         scale = L / (M_PI * E_star * (double)Ns * Ns);
     } else {
@@ -630,8 +666,8 @@ Operator::~Operator() {
 int Operator::col_tile(bool dbl, int cv) const {
     int c = 1;
     if (kind == OP_FFT) {
-        if (dbl) { ASB_SIZE_SWITCH(Ns, c = FreeImpl<double, NS>::ct(cv)); }
-        else { ASB_SIZE_SWITCH(Ns, c = FreeImpl<float, NS>::ct(cv)); }
+        if (dbl) { ASB_SIZE_SWITCH(Ns, c = FreeImpl<double, NS>::ct(cv, FreeImpl<double, NS>::split(*this))); }
+        else { ASB_SIZE_SWITCH(Ns, c = FreeImpl<float, NS>::ct(cv, FreeImpl<float, NS>::split(*this))); }
     } else {
         if (dbl) { ASB_SIZE_SWITCH(Ns, c = PeriodicImpl<double, NS>::ct(cv)); }
         else { ASB_SIZE_SWITCH(Ns, c = PeriodicImpl<float, NS>::ct(cv)); }
@@ -720,8 +756,8 @@ double Operator::autotune(bool dbl, int reps, int& best_rv, int& best_cv) {
 size_t Operator::spectrum_bytes(bool dbl) const {
     size_t n = 0;
     if (kind == OP_FFT) {
-        if (dbl) { ASB_SIZE_SWITCH(Ns, n = FreeImpl<double, NS>::spec_elems() * sizeof(double2)); }
-        else { ASB_SIZE_SWITCH(Ns, n = FreeImpl<float, NS>::spec_elems() * sizeof(float2)); }
+        if (dbl) { ASB_SIZE_SWITCH(Ns, n = FreeImpl<double, NS>::spec_elems(FreeImpl<double, NS>::split(*this)) * sizeof(double2)); }
+        else { ASB_SIZE_SWITCH(Ns, n = FreeImpl<float, NS>::spec_elems(FreeImpl<float, NS>::split(*this)) * sizeof(float2)); }
     } else {
         if (dbl) { ASB_SIZE_SWITCH(Ns, n = PeriodicImpl<double, NS>::spec_elems() * sizeof(double2)); }
         else { ASB_SIZE_SWITCH(Ns, n = PeriodicImpl<float, NS>::spec_elems() * sizeof(float2)); }

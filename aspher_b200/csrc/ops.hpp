@@ -53,6 +53,10 @@ tw(int L) {
 
 enum OpKind : int { OP_FFT = 0, OP_PERIODIC = 1 };
 
+// smallest grid with the split free-space column pass (two length-Ns halves
+// of the length-2Ns column; required for FP64 at Ns = 8192)
+constexpr int kSplitMin = 256;
+
 bool is_pow2(long v);
 
 // launch variants chosen for (kind, precision, Ns): the autotuned entry of
@@ -83,6 +87,9 @@ struct Operator {
     // launch variants per precision [F32, F64] and the column tile width
     // (half-spectrum layout) they imply
     int rowv[2] = {0, 0}, colv[2] = {0, 0}, ct[2] = {0, 0};
+    // free space: the column pass as two half-length transforms even where
+    // the full column fits one CTA (set from ASPHER_SPLIT_COLUMNS at creation)
+    bool split_cols = false;
     // periodic: symbol scale L / (pi E* Ns^2)
     double scale = 0.0;
     // scratch half spectra per precision (lazily sized)

@@ -1,0 +1,115 @@
+"""Free-space operator with the split column pass (B200).
+
+The zero-padded column of length 2 Ns is transformed as two length-Ns halves
+(even and odd frequencies).  That is the only form an FP64 column of 16384
+points can take (it does not fit one CTA's shared memory), so FP64 applies at
+Ns = 8192 use it; ASPHER_SPLIT_COLUMNS=1 forces it at smaller sizes, where it
+is checked against the oracle and against the one-CTA column pass.  The FP64
+apply at Ns = 8192 is checked through point loads, whose response is the
+Love table itself (the aperiodic convolution of a unit load at a corner
+cell), against the FP32 apply, and for symmetry.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from oracle.operators import FFTOperator as OFFT  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def _op(Ns, split=False):
+    from aspher_b200 import Operator
+    if not split:
+        return Operator("fft", Ns)
+    os.environ["ASPHER_SPLIT_COLUMNS"] = "1"
+    try:
+        return Operator("fft", Ns)
+    finally:
+        del os.environ["ASPHER_SPLIT_COLUMNS"]
+
+
+def _mv(op, x, dtype):
+    xt = torch.as_tensor(np.ascontiguousarray(x), dtype=dtype, device="cuda")
+    y = torch.empty_like(xt)
+    op.matvec_(xt, y)
+    torch.cuda.synchronize()
+    return y.cpu().numpy().astype(np.float64)
+
+
+def rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("Ns", [256, 1024])
+def test_split_columns_match_oracle_and_one_cta_form(Ns):
+    ops, op = _op(Ns, split=True), _op(Ns)
+    x = np.random.default_rng(11).standard_normal(Ns * Ns)
+    ref = OFFT(Ns, 1.0, 1.0).matvec(x)
+    ys = _mv(ops, x, torch.float64)
+    assert rel(ys, ref) < 1e-13
+    assert rel(ys, _mv(op, x, torch.float64)) < 1e-14
+    x32 = x.astype(np.float32)
+    ref32 = OFFT(Ns, 1.0, 1.0).matvec(x32.astype(np.float64))
+    ys32 = _mv(ops, x32, torch.float32)
+    assert rel(ys32, ref32) < 2e-6
+    # repeat calls bitwise equal (test_fft.cpp:46-59)
+    assert np.array_equal(ys, _mv(ops, x, torch.float64))
+
+
+def test_split_columns_batched_solve():
+    import aspher_b200 as asb
+    from aspher_b200.surfaces import self_affine_gap
+    Ns = 256
+    ops, op = _op(Ns, split=True), _op(Ns)
+    gs = [torch.from_numpy(self_affine_gap(Ns, hurst=0.8, rms=0.002, seed=s)).cuda()
+          for s in (3, 4, 5)]
+    loads = [0.002, 0.005, 0.02]
+    rb = asb.solve_device_batch(ops, gs, loads, tol=1e-10, precond="fourier",
+                                dtype=torch.float64)
+    for g, p, r in zip(gs, loads, rb):
+        r1 = asb.solve_device(op, g, p, tol=1e-10, precond="fourier", dtype=torch.float64,
+                              light=True)
+        assert r.status == "converged" and r1.status == "converged"
+        assert rel(r.pressure.ravel(), r1.pressure.ravel()) < 1e-8
+        assert abs(r.contact_area - r1.contact_area) <= 1e-4
+
+
+def test_fp64_apply_at_8192():
+    Ns = 8192
+    N = Ns * Ns
+    op = _op(Ns)
+    T = op.love_table()
+    # unit loads at the two opposite corners: u(iy, ix) = T(|iy - jy|, |ix - jx|)
+    for (jy, jx) in ((0, 0), (Ns - 1, Ns - 1)):
+        x = np.zeros(N)
+        x[jy * Ns + jx] = 1.0
+        u = _mv(op, x, torch.float64).reshape(Ns, Ns)
+        ref = T if jy == 0 else T[::-1, ::-1]
+        assert rel(u.ravel(), ref.ravel()) < 1e-13
+        assert np.max(np.abs(u - ref)) < 1e-13 * T[0, 0]
+    del T
+    rng = np.random.default_rng(5)
+    x, w = rng.standard_normal(N), rng.standard_normal(N)
+    y = _mv(op, x, torch.float64)
+    assert rel(y, _mv(op, x.astype(np.float32), torch.float32)) < 2e-6
+    sx, sw = np.dot(w, y), np.dot(x, _mv(op, w, torch.float64))
+    assert abs(sx - sw) < 1e-12 * np.linalg.norm(y) * np.linalg.norm(w)
+
+
+def test_fp64_solve_runs_at_8192():
+    import aspher_b200 as asb
+    from aspher_b200.surfaces import self_affine_gap
+    Ns = 8192
+    op = _op(Ns)
+    g = torch.from_numpy(self_affine_gap(Ns, hurst=0.8, rms=0.002, seed=42)).cuda()
+    r = asb.solve_device(op, g, 0.005, tol=1e-6, max_iter=8, precond="fourier",
+                         dtype=torch.float64, light=True)
+    assert r.iterations == 8 and r.status == "max_iterations"
+    p = r.pressure_device
+    assert torch.isfinite(p).all() and float(p.min()) >= 0.0
+    assert abs(float(p.mean()) / 0.005 - 1.0) < 1e-12
