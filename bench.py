@@ -13,7 +13,9 @@ solves/s with the gaps resident in HBM; ``e2e`` = the same solves one at a
 time through ``ContactSolver.solve`` with the gap copied from pinned host
 memory and the pressure read back every solve.  The same mixed solves one
 at a time, the plain FP64 GPU solve, a 96-problem uneven batch and the
-adjoint's finite-difference check are measured beside it.  Ranks solve disjoint
+adjoint's finite-difference check are measured beside it, and so are the
+fft rows of the reference's backend x precision study (nested solves at
+Ns 2048-8192, double and float, next to its published CPU wall times).  Ranks solve disjoint
 problem sets (seed 42 + 1000*rank): weak scaling, no collective on the
 data path.
 
@@ -420,6 +422,12 @@ def run_ours(args):
     if rank == 0 and not os.environ.get("BENCH_SKIP_LARGE"):
         large = large_single(dev)
 
+    # the reference's own backend x precision study (fft rows), same settings
+    # and surface law, next to its published CPU wall times
+    study = None
+    if rank == 0 and not os.environ.get("BENCH_SKIP_STUDY"):
+        study = precision_study(dev)
+
     # the adjoint (FP32 and FP64 CG), checked against central differences of
     # the FP64 solve
     adj = None
@@ -453,6 +461,7 @@ def run_ours(args):
             "uneven_batch": uneven,
             "adjoint": adj,
             "large_single": large,
+            "precision_study": study,
             "fp64_gpu": {"value": value64, "unit": "solves/s",
                          "ratio_mixed_over_fp64": value / value64,
                          "iterations": [r.iterations for r in last64]},
@@ -514,6 +523,61 @@ def large_single(dev, Ns=8192, pbar=0.005):
             "finest_iterations": r.iterations, "fw_error": r.fw_error,
             "penetration_error": r.penetration_error, "contact_area": r.contact_area,
             "stages": [[st["name"], st["iterations"], st["seconds"]] for st in r.stage_stats]}
+
+
+# the reference's published fft rows of its backend x precision study
+# (doc/backend_precision_study/summary.md:19-30; i7-13700H, 20 threads):
+# (precision, Ns) -> (wall seconds, iterations, contact area)
+STUDY_REF = {("double", 2048): (11.90, 16, 0.00086), ("double", 4096): (40.67, 22, 0.00068),
+             ("double", 8192): (432.61, 46, 0.00055), ("float", 2048): (4.23, 11, 0.00086),
+             ("float", 4096): (14.51, 17, 0.00068), ("float", 8192): (122.90, 28, 0.00055)}
+
+
+def precision_study(dev, sizes=(2048, 4096, 8192)):
+    """The reference's backend x precision study for backend='fft'
+    (bench_backend_precision_study.py:26-32,70-76): solve_nested with
+    p_nominal 0.002, coarsest 64, precond, tol 1e-8, coarse_tol 1e-4,
+    single_precision + allow_tolerance_relaxation for 'float', on a
+    self-affine surface with H 0.8, rms 0.02, |k| in [12, 0.33 Ns] cycles per
+    domain, seed 42 (this project's random-phase generator standing in for
+    the reference's surface package: same law, another realisation).  The
+    gap is a host array, as in the reference's call; wall time of the whole
+    call (operator builds of every level included), one run after an untimed
+    one at Ns=512."""
+    import numpy as np
+    import torch
+    import aspher_b200 as asb
+    from aspher_b200.surfaces import self_affine_gap
+
+    def run(Ns, precision):
+        g = self_affine_gap(Ns, hurst=0.8, rms=0.02, k_lo=12.0, k_hi=0.33 * Ns, seed=42)
+        single = precision == "float"
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = asb.solve_nested(Ns, g, 0.002, coarsest=64, precond=True, tol=1e-8, coarse_tol=1e-4,
+                             max_iter=20000, single_precision=single,
+                             allow_tolerance_relaxation=single, light_result=True,
+                             backend="fft")
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, r
+
+    run(512, "double")
+    run(512, "float")
+    rows = []
+    for precision in ("double", "float"):
+        for Ns in sizes:
+            sec, r = run(Ns, precision)
+            ref = STUDY_REF.get((precision, Ns))
+            rows.append({"precision": precision, "Ns": Ns, "seconds": sec, "status": r.status,
+                         "iterations": r.iterations, "final_error": r.error,
+                         "contact_area": r.contact_area,
+                         "reference_cpu": None if ref is None else
+                         {"seconds": ref[0], "iterations": ref[1], "contact_area": ref[2]}})
+            torch.cuda.empty_cache()
+    return {"workload": "reference's backend x precision study, fft rows: solve_nested "
+                        "p_nominal 0.002, coarsest 64, tol 1e-8 (float: relaxed to its floor), "
+                        "H 0.8, rms 0.02, |k| in [12, 0.33 Ns] cycles/domain, host gap",
+            "rows": rows}
 
 
 def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
