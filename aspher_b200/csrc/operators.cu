@@ -194,6 +194,59 @@ struct StoreRealTracked {
 // The functors are passed by value; StoreRealTracked keeps per-thread maxima
 // in mutable members initialised to zero by the host copy.
 
+// Split form of the two Kh passes, for rows of M = 2 Ns reals whose complex
+// FFT (length Ns) does not fit one CTA (FP64 at Ns > 8192): the real DFT of
+// a row is assembled from the real DFTs of its even and odd samples,
+//   X[k] = E[k] + w_M^k O[k],  k in [0, Ns],  w_M = exp(-2 pi i / M),
+// with E[Ns - k] = conj E[k] (and O likewise) for the upper half.  The first
+// pass stores E (row_fwd of the even samples, StoreCplxRows), the second
+// transforms the odd samples and combines while storing (StoreSplitCombine).
+struct LoadEmbeddedPar {  // z[n] = (x[4n + p], x[4n + 2 + p]) of an embedded row
+    static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
+    LoadEmbedded e;
+    int p;
+    __device__ __forceinline__ double2 operator()(int row, int n) const {
+        return make_double2(e.at(row, 4 * n + p), e.at(row, 4 * n + 2 + p));
+    }
+};
+struct LoadRealRowsPar {  // the same sampling of plain rows
+    static constexpr bool kTiled = false;
+    static constexpr bool kRaw = false;
+    const double* x;
+    int pitch, p;
+    __device__ __forceinline__ double2 operator()(int row, int n) const {
+        const double* r = x + (size_t)row * pitch;
+        return make_double2(r[4 * n + p], r[4 * n + 2 + p]);
+    }
+};
+struct StoreCplxRows {
+    static constexpr bool kFinish = false;
+    static constexpr bool kTiled = false;
+    double2* out;
+    int pitch;
+    __device__ __forceinline__ void operator()(int row, int k, double2 X) const {
+        out[(size_t)row * pitch + k] = X;
+    }
+    __device__ void finish(double*) const {}
+};
+struct StoreSplitCombine {
+    static constexpr bool kFinish = true;
+    static constexpr bool kTiled = false;
+    const double2* E;     // even-sample half spectra, pitch entries per row
+    int pitch;
+    const double2* twm;   // exp(-2 pi i k / M), k < M
+    int half;             // M / 2 = Ns
+    StoreRealTracked inner;
+    __device__ __forceinline__ void operator()(int row, int k, double2 O) const {
+        const double2 e = E[(size_t)row * pitch + k];
+        inner(row, k, cadd(e, cmul(O, __ldg(&twm[k]))));
+        const int k2 = half - k;
+        inner(row, k2, cadd(cconj(e), cmul(cconj(O), __ldg(&twm[k2]))));
+    }
+    __device__ void finish(double* scratch) const { inner.finish(scratch); }
+};
+
 // ----------------------------------------------------------------------------
 // launch-variant selection: a default per (backend, precision, Ns), overridden
 // process-wide by the autotuner (Operator::autotune) or set per operator
@@ -358,17 +411,31 @@ void launch_col_split(cplx<T>* spec, cplx<T>* acc, int nrows, Mult m, cudaStream
         default: throw Error(-1, "FFT launch variant out of range");              \
     }
 
-template <typename T, int LR, bool PAD, class Load, class Store>
+// ALLV = false: launch variant 0 whatever v is (one instantiation per pass;
+// the grids above kMaxVariantNs)
+template <typename T, int LR, bool PAD, bool ALLV = true, class Load, class Store>
 void row_fwd_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B) {
-    ASB_V_SWITCH(v, LR, (launch_row_fwd<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
+    if constexpr (!ALLV) {
+        launch_row_fwd<T, LR, PAD, vclamp(LR, 0), Load, Store>(ld, st, nrows, s, gate, B);
+    } else {
+        ASB_V_SWITCH(v, LR, (launch_row_fwd<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
+    }
 }
-template <typename T, int LR, bool PAD, class Load, class Store>
+template <typename T, int LR, bool PAD, bool ALLV = true, class Load, class Store>
 void row_inv_v(int v, Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B) {
-    ASB_V_SWITCH(v, LR, (launch_row_inv<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
+    if constexpr (!ALLV) {
+        launch_row_inv<T, LR, PAD, vclamp(LR, 0), Load, Store>(ld, st, nrows, s, gate, B);
+    } else {
+        ASB_V_SWITCH(v, LR, (launch_row_inv<T, LR, PAD, V, Load, Store>(ld, st, nrows, s, gate, B)));
+    }
 }
-template <typename T, int LC, int NCM1, bool PAD, class Mult>
+template <typename T, int LC, int NCM1, bool PAD, bool ALLV = true, class Mult>
 void col_v(int v, cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate, int B) {
-    ASB_V_SWITCH(v, LC, (launch_col<T, LC, NCM1, PAD, V, Mult>(spec, nrows, m, s, gate, B)));
+    if constexpr (!ALLV) {
+        launch_col<T, LC, NCM1, PAD, vclamp(LC, 0), Mult>(spec, nrows, m, s, gate, B);
+    } else {
+        ASB_V_SWITCH(v, LC, (launch_col<T, LC, NCM1, PAD, V, Mult>(spec, nrows, m, s, gate, B)));
+    }
 }
 // tile width of column variant v (runtime view of the constexpr table)
 template <typename T, int LC, int NCM1>
@@ -388,37 +455,46 @@ struct FreeImpl {
     // at Ns = 8192); otherwise the column pass runs as two length-Ns halves
     // (col_split_kernel), instantiated for Ns >= kSplitMin
     static constexpr bool kFits = col_fits<T>(LC);
-    static constexpr bool kSplitOK = NS >= kSplitMin;
-    static_assert(kFits || kSplitOK, "a column that does not fit must have the split form");
+    static constexpr bool kSplitOK = NS >= kSplitMin && col_fits<T>(LR);
+    // rows and columns in one CTA each (every size but FP64 above 8192)
+    static constexpr bool kSupported = row_smem_v<T>(LR, 0) <= kSmemPerSM && (kFits || kSplitOK);
+    static constexpr bool kAllV = NS <= kMaxVariantNs;
     static bool split(const Operator& op) { return !kFits || (kSplitOK && op.split_cols); }
     // spectrum sized for the widest tile (16 columns); the split form keeps
     // its first half-column result in a second spectrum-shaped block after
     // the B instances' spectra
     static size_t spec_elems(bool sp) { return (size_t)(LR + 16) * NS * (sp ? 2 : 1); }
     static int ct(int cv, bool sp) {
-        return sp ? col_ct_v<T>(LR, LR, vclamp(LR, 0)) : col_ct_rt<T, LC, LR>(cv);
+        if (sp) return col_ct_v<T>(LR, LR, vclamp(LR, 0));
+        return kAllV ? col_ct_rt<T, LC, LR>(cv) : col_ct_v<T>(LC, LR, vclamp(LC, 0));
     }
 
     // row_fwd(ld) -> col(x Kh) -> row_inv(st); ld / st see the Ns x Ns field(s)
     template <class Load, class Store>
     static void apply(const Operator& op, Load ld, Store st, cplx<T>* spec, cudaStream_t s,
                       const int* gate, int B) {
-        const int dbl = sizeof(T) == 8;
-        const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
-        const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
-        const long bsp = (long)(LR / c + 1) * NS * c;
-        row_fwd_v<T, LR, true>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
-        if (split(op)) {
-            if constexpr (kSplitOK)
-                launch_col_split<T, LR, LR>(spec, spec + (size_t)B * bsp, NS,
-                                            KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
+        if constexpr (!kSupported) {
+            throw Error(-1, "free-space FP64 apply above grid_size 8192 is not supported (its "
+                            "rows and half columns do not fit one CTA's shared memory); use FP32");
         } else {
-            if constexpr (kFits)
-                col_v<T, LC, LR, true>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
+            const int dbl = sizeof(T) == 8;
+            const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
+            const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
+            const long bsp = (long)(LR / c + 1) * NS * c;
+            row_fwd_v<T, LR, true, kAllV>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
+            if (split(op)) {
+                if constexpr (kSplitOK)
+                    launch_col_split<T, LR, LR>(spec, spec + (size_t)B * bsp, NS,
+                                                KhMult<T>{kh, NS + 1, LC, c}, s, gate, B);
+            } else {
+                if constexpr (kFits)
+                    col_v<T, LC, LR, true, kAllV>(cv, spec, NS, KhMult<T>{kh, NS + 1, LC, c}, s,
+                                                  gate, B);
+            }
+            row_inv_v<T, LR, true, kAllV>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
+            count_launches(split(op) ? 4 : 3);
+            ASB_CUDA(cudaGetLastError());
         }
-        row_inv_v<T, LR, true>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
-        count_launches(split(op) ? 4 : 3);
-        ASB_CUDA(cudaGetLastError());
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
@@ -431,19 +507,29 @@ struct FreeImpl {
 template <typename T, int NS>
 struct PeriodicImpl {
     static constexpr int LR = NS / 2, LC = NS;
+    // rows and columns in one CTA each (every size but FP64 above 8192)
+    static constexpr bool kSupported = row_smem_v<T>(LR, 0) <= kSmemPerSM && col_fits<T>(LC);
+    static constexpr bool kAllV = NS <= kMaxVariantNs;
     static size_t spec_elems() { return (size_t)(LR + 16) * NS; }
-    static int ct(int cv) { return col_ct_rt<T, LC, LR>(cv); }
+    static int ct(int cv) {
+        return kAllV ? col_ct_rt<T, LC, LR>(cv) : col_ct_v<T>(LC, LR, vclamp(LC, 0));
+    }
 
     template <class Load, class Mult, class Store>
     static void apply(int rv, int cv, Load ld, Mult mult, Store st, cplx<T>* spec, cudaStream_t s,
                       const int* gate, int B) {
-        const int c = ct(cv);
-        const long bsp = (long)(LR / c + 1) * NS * c;
-        row_fwd_v<T, LR, false>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
-        col_v<T, LC, LR, false>(cv, spec, NS, mult, s, gate, B);
-        row_inv_v<T, LR, false>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
-        count_launches(3);
-        ASB_CUDA(cudaGetLastError());
+        if constexpr (!kSupported) {
+            throw Error(-1, "periodic FP64 apply above grid_size 8192 is not supported (its "
+                            "column does not fit one CTA's shared memory); use FP32");
+        } else {
+            const int c = ct(cv);
+            const long bsp = (long)(LR / c + 1) * NS * c;
+            row_fwd_v<T, LR, false, kAllV>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
+            col_v<T, LC, LR, false, kAllV>(cv, spec, NS, mult, s, gate, B);
+            row_inv_v<T, LR, false, kAllV>(rv, LoadTiled<T>{spec, NS, c, bsp}, st, NS, s, gate, B);
+            count_launches(3);
+            ASB_CUDA(cudaGetLastError());
+        }
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
@@ -542,6 +628,15 @@ struct FourierImpl {
 // spectrum kh_canon[ky * (Ns+1) + kx], ky, kx in [0, Ns].
 template <int NS>
 struct KhBuild {
+    // the split form (see StoreSplitCombine) where the FP64 row does not fit
+    // one CTA, or where ASPHER_SPLIT_KH=1 asks for it (cross-checks), for
+    // Ns >= kSplitMin
+    static constexpr bool kRowFits = row_smem_v<double>(NS, 0) <= kSmemPerSM;
+    static bool split() {
+        if (!kRowFits) return true;
+        const char* e = std::getenv("ASPHER_SPLIT_KH");
+        return NS >= kSplitMin && e && std::atoi(e) != 0;
+    }
     static void run(Operator& op) {
         constexpr int LR = NS, M = 2 * NS;
         const size_t nk = (size_t)(NS + 1) * (NS + 1);
@@ -551,17 +646,45 @@ struct KhBuild {
         ASB_CUDA(cudaMalloc(&yt, (size_t)(NS + 1) * M * sizeof(double)));
         ASB_CUDA(cudaMalloc(&mx, 4 * sizeof(unsigned long long)));
         ASB_CUDA(cudaMemset(mx, 0, 4 * sizeof(unsigned long long)));
-        // pass A over the M rows of the embedded table (real by evenness in ix)
         StoreRealTracked sa{yt, M, nullptr, nullptr, 0, 0, 0, 0.0, mx, 0.0, 0.0};
-        launch_row_fwd<double, LR, false, 0>(LoadEmbedded{op.table, NS, M}, sa, M, nullptr,
-                                             nullptr);
-        ASB_CUDA(cudaGetLastError());
-        // pass B over the Ns+1 rows of the transposed buffer (each M long)
         StoreRealTracked sb{nullptr, M, op.kh_canon, nullptr, NS + 1, 0, 0,
                             1.0 / ((double)M * (double)M), mx + 2, 0.0, 0.0};
-        launch_row_fwd<double, LR, false, 0>(LoadRealRows<double>{yt, M, 0}, sb, NS + 1, nullptr,
-                                             nullptr);
-        ASB_CUDA(cudaGetLastError());
+        const LoadEmbedded emb{op.table, NS, M};
+        if (split()) {
+            if constexpr (NS >= kSplitMin) {
+                constexpr int LH = NS / 2;  // real length Ns per parity
+                double2* E = nullptr;
+                ASB_CUDA(cudaMalloc(&E, (size_t)M * (LH + 1) * sizeof(double2)));
+                const double2* twm = tw<double>(M);
+                // pass A over the M rows of the embedded table
+                launch_row_fwd<double, LH, false, 0>(LoadEmbeddedPar{emb, 0},
+                                                     StoreCplxRows{E, LH + 1}, M, nullptr, nullptr);
+                launch_row_fwd<double, LH, false, 0>(
+                    LoadEmbeddedPar{emb, 1}, StoreSplitCombine{E, LH + 1, twm, NS, sa}, M, nullptr,
+                    nullptr);
+                ASB_CUDA(cudaGetLastError());
+                // pass B over the Ns+1 rows of the transposed buffer
+                launch_row_fwd<double, LH, false, 0>(LoadRealRowsPar{yt, M, 0},
+                                                     StoreCplxRows{E, LH + 1}, NS + 1, nullptr,
+                                                     nullptr);
+                launch_row_fwd<double, LH, false, 0>(
+                    LoadRealRowsPar{yt, M, 1}, StoreSplitCombine{E, LH + 1, twm, NS, sb}, NS + 1,
+                    nullptr, nullptr);
+                ASB_CUDA(cudaGetLastError());
+                ASB_CUDA(cudaDeviceSynchronize());
+                ASB_CUDA(cudaFree(E));
+            }
+        } else {
+            if constexpr (kRowFits) {
+                // pass A over the M rows of the embedded table (real by evenness in ix)
+                launch_row_fwd<double, LR, false, 0>(emb, sa, M, nullptr, nullptr);
+                ASB_CUDA(cudaGetLastError());
+                // pass B over the Ns+1 rows of the transposed buffer (each M long)
+                launch_row_fwd<double, LR, false, 0>(LoadRealRows<double>{yt, M, 0}, sb, NS + 1,
+                                                     nullptr, nullptr);
+                ASB_CUDA(cudaGetLastError());
+            }
+        }
         unsigned long long h[4];
         ASB_CUDA(cudaMemcpy(h, mx, sizeof(h), cudaMemcpyDeviceToHost));
         ASB_CUDA(cudaFree(yt));
@@ -607,14 +730,15 @@ __global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
         case 2048: { constexpr int NS = 2048; __VA_ARGS__; } break; \
         case 4096: { constexpr int NS = 4096; __VA_ARGS__; } break; \
         case 8192: { constexpr int NS = 8192; __VA_ARGS__; } break; \
-        default: throw Error(-1, "grid_size must be a power of two in [16, 8192]"); \
+        case 16384: { constexpr int NS = 16384; __VA_ARGS__; } break; \
+        default: throw Error(-1, "grid_size must be a power of two in [16, 16384]"); \
     }
 
 Operator::Operator(int kind_, int Ns_, double L_, double E_)
     : kind(kind_), Ns(Ns_), L(L_), E_star(E_) {
     if (kind != OP_FFT && kind != OP_PERIODIC) throw Error(-1, "unknown operator kind");
-    if (!is_pow2(Ns) || Ns < 16 || Ns > 8192)
-        throw Error(-1, "grid_size must be a power of two in [16, 8192]");
+    if (!is_pow2(Ns) || Ns < 16 || Ns > kMaxNs)
+        throw Error(-1, "grid_size must be a power of two in [16, 16384]");
     if (!(L > 0.0) || !std::isfinite(L)) throw Error(-1, "domain_size must be positive");
     if (!(E_star > 0.0) || !std::isfinite(E_star)) throw Error(-1, "E_star must be positive");
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
@@ -637,9 +761,11 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
         ASB_CUDA(cudaGetLastError());
         ASB_SIZE_SWITCH(Ns, KhBuild<NS>::run(*this));
         const size_t nt = (size_t)(Ns + 16) * (Ns + 1);  // widest tiling
-        ASB_CUDA(cudaMalloc(&kh_d, nt * sizeof(double)));
+        if (supports(true)) {  // no FP64 copy where FP64 applies do not exist
+            ASB_CUDA(cudaMalloc(&kh_d, nt * sizeof(double)));
+            ASB_CUDA(cudaMemset(kh_d, 0, nt * sizeof(double)));
+        }
         ASB_CUDA(cudaMalloc(&kh_f, nt * sizeof(float)));
-        ASB_CUDA(cudaMemset(kh_d, 0, nt * sizeof(double)));
         ASB_CUDA(cudaMemset(kh_f, 0, nt * sizeof(float)));
     }
     for (int dbl = 0; dbl < 2; ++dbl) {
@@ -789,8 +915,23 @@ size_t Operator::resident_bytes() const {
     return n;
 }
 
+bool Operator::supports(bool dbl) const {
+    bool ok = true;
+    if (kind == OP_FFT) {
+        if (dbl) { ASB_SIZE_SWITCH(Ns, ok = FreeImpl<double, NS>::kSupported); }
+        else { ASB_SIZE_SWITCH(Ns, ok = FreeImpl<float, NS>::kSupported); }
+    } else {
+        if (dbl) { ASB_SIZE_SWITCH(Ns, ok = PeriodicImpl<double, NS>::kSupported); }
+        else { ASB_SIZE_SWITCH(Ns, ok = PeriodicImpl<float, NS>::kSupported); }
+    }
+    return ok;
+}
+
 void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate, int B,
                       void* spec_b) {
+    if (!supports(dbl))
+        throw Error(-1, "FP64 applies are not supported above grid_size 8192 (an FP64 row or "
+                        "column of 16384 points does not fit one CTA's shared memory); use FP32");
     void* spec = spec_b ? spec_b : spectrum(dbl, s);
     if (kind == OP_FFT) {
         if (dbl) {

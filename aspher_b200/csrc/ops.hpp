@@ -56,6 +56,11 @@ enum OpKind : int { OP_FFT = 0, OP_PERIODIC = 1 };
 // smallest grid with the split free-space column pass (two length-Ns halves
 // of the length-2Ns column; required for FP64 at Ns = 8192)
 constexpr int kSplitMin = 256;
+// largest grid; above kMaxVariantNs the pass kernels run launch variant 0
+// only, and only FP32 (an FP64 row or half column of 16384 points does not
+// fit one CTA's shared memory)
+constexpr int kMaxNs = 16384;
+constexpr int kMaxVariantNs = 8192;
 
 bool is_pow2(long v);
 
@@ -128,6 +133,9 @@ struct Operator {
     // keeps and records (process-wide) the fastest; returns its mean ms
     double autotune(bool dbl, int reps, int& best_rv, int& best_cv);
     size_t spectrum_bytes(bool dbl) const;
+    // whether applies of this precision exist at this size (false only for
+    // FP64 above 8192); checked before any allocation of that precision
+    bool supports(bool dbl) const;
     size_t resident_bytes() const;
 };
 

@@ -1108,8 +1108,12 @@ struct SolverCtx : SolverCtxBase {
         ASB_CUDA(cudaMemset(st, 0, (size_t)cap * sizeof(PkState)));
         ASB_CUDA(cudaMemset(z, 0, b));
         grid = red_grid(N);
-        (void)o.spectrum(sizeof(T) == 8, nullptr);  // allocate before any capture
-        if (cap > 1) {
+        // spectra allocated before any capture; none for a precision whose
+        // applies do not exist at this size (FP64 above 8192: this context
+        // then only holds the FP64 fields of a mixed solve)
+        const bool has_apply = o.supports(sizeof(T) == 8);
+        if (has_apply) (void)o.spectrum(sizeof(T) == 8, nullptr);
+        if (cap > 1 && has_apply) {
             const size_t sb = o.spectrum_bytes(sizeof(T) == 8) * (size_t)cap;
             ASB_CUDA(cudaMalloc(&spec, sb));
             ASB_CUDA(cudaMemset(spec, 0, sb));

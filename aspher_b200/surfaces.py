@@ -26,3 +26,26 @@ def self_affine_height(Ns, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=64.0, seed=42):
 def self_affine_gap(Ns, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=64.0, seed=42):
     """Flat (Ns*Ns,) float64 gap g0 = -h."""
     return np.ascontiguousarray((-self_affine_height(Ns, hurst, rms, k_lo, k_hi, seed)).ravel())
+
+
+def self_affine_gap_device(Ns, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=64.0, seed=42,
+                           device="cuda"):
+    """self_affine_gap synthesised on the device (for grids whose host-side
+    synthesis would take tens of GB): the same random phases (drawn on the
+    host from the same seed) and spectrum; the inverse FFT and the scaling
+    run in torch on `device`.  Returns a flat FP64 device tensor, equal to
+    self_affine_gap's array up to FFT rounding."""
+    import torch
+    rng = np.random.default_rng(seed)
+    ph = torch.from_numpy(rng.random((Ns, Ns))).to(device)
+    k = torch.fft.fftfreq(Ns, 1.0 / Ns, dtype=torch.float64, device=device)
+    kk = torch.hypot(k[:, None], k[None, :])
+    band = (kk >= k_lo) & (kk <= k_hi)
+    amp = torch.where(band, kk.clamp_min(1e-300) ** (-(1.0 + hurst)), torch.zeros_like(kk))
+    del kk, band
+    spec = torch.polar(amp, 2 * np.pi * ph)
+    del amp, ph
+    h = torch.fft.ifft2(spec).real
+    del spec
+    h *= rms / h.std(correction=0)
+    return (-h).reshape(-1).contiguous()

@@ -15,7 +15,8 @@ memory and the pressure read back every solve.  The same mixed solves one
 at a time, the plain FP64 GPU solve, a 96-problem uneven batch and the
 adjoint's finite-difference check are measured beside it, and so are the
 fft rows of the reference's backend x precision study (nested solves at
-Ns 2048-8192, double and float, next to its published CPU wall times).  Ranks solve disjoint
+Ns 2048-8192 in double and 2048-16384 in float, next to its published CPU
+wall times; at 16384 it ran out of memory).  Ranks solve disjoint
 problem sets (seed 42 + 1000*rank): weak scaling, no collective on the
 data path.
 
@@ -531,9 +532,12 @@ def large_single(dev, Ns=8192, pbar=0.005):
 STUDY_REF = {("double", 2048): (11.90, 16, 0.00086), ("double", 4096): (40.67, 22, 0.00068),
              ("double", 8192): (432.61, 46, 0.00055), ("float", 2048): (4.23, 11, 0.00086),
              ("float", 4096): (14.51, 17, 0.00068), ("float", 8192): (122.90, 28, 0.00055)}
+# rows the reference could not run (summary.md:32-34): fft at Ns=16384 ran out
+# of memory on its 32 GiB node (its h2 backend reached contact area 0.00046 there)
+STUDY_REF_FAILED = {("double", 16384): "oom (32 GiB node)", ("float", 16384): "oom (32 GiB node)"}
 
 
-def precision_study(dev, sizes=(2048, 4096, 8192)):
+def precision_study(dev, sizes=(2048, 4096, 8192), float_sizes=(2048, 4096, 8192, 16384)):
     """The reference's backend x precision study for backend='fft'
     (bench_backend_precision_study.py:26-32,70-76): solve_nested with
     p_nominal 0.002, coarsest 64, precond, tol 1e-8, coarse_tol 1e-4,
@@ -543,14 +547,21 @@ def precision_study(dev, sizes=(2048, 4096, 8192)):
     the reference's surface package: same law, another realisation).  The
     gap is a host array, as in the reference's call; wall time of the whole
     call (operator builds of every level included), one run after an untimed
-    one at Ns=512."""
+    one at Ns=512.  Ns=16384 (FP32 only; the reference's fft rows ran out of
+    memory there) synthesises the surface on the device, the same law and
+    phases, and hands the solve a host copy like the other rows."""
     import numpy as np
     import torch
     import aspher_b200 as asb
-    from aspher_b200.surfaces import self_affine_gap
+    from aspher_b200.surfaces import self_affine_gap, self_affine_gap_device
 
     def run(Ns, precision):
-        g = self_affine_gap(Ns, hurst=0.8, rms=0.02, k_lo=12.0, k_hi=0.33 * Ns, seed=42)
+        kw = dict(hurst=0.8, rms=0.02, k_lo=12.0, k_hi=0.33 * Ns, seed=42)
+        if Ns > 8192:
+            g = self_affine_gap_device(Ns, device=dev, **kw).cpu().numpy()
+            torch.cuda.empty_cache()
+        else:
+            g = self_affine_gap(Ns, **kw)
         single = precision == "float"
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -565,18 +576,20 @@ def precision_study(dev, sizes=(2048, 4096, 8192)):
     run(512, "float")
     rows = []
     for precision in ("double", "float"):
-        for Ns in sizes:
+        for Ns in (sizes if precision == "double" else float_sizes):
             sec, r = run(Ns, precision)
             ref = STUDY_REF.get((precision, Ns))
+            refd = ({"seconds": ref[0], "iterations": ref[1], "contact_area": ref[2]}
+                    if ref is not None else {"status": STUDY_REF_FAILED.get((precision, Ns))})
             rows.append({"precision": precision, "Ns": Ns, "seconds": sec, "status": r.status,
                          "iterations": r.iterations, "final_error": r.error,
-                         "contact_area": r.contact_area,
-                         "reference_cpu": None if ref is None else
-                         {"seconds": ref[0], "iterations": ref[1], "contact_area": ref[2]}})
+                         "contact_area": r.contact_area, "reference_cpu": refd})
+            del r
             torch.cuda.empty_cache()
     return {"workload": "reference's backend x precision study, fft rows: solve_nested "
                         "p_nominal 0.002, coarsest 64, tol 1e-8 (float: relaxed to its floor), "
-                        "H 0.8, rms 0.02, |k| in [12, 0.33 Ns] cycles/domain, host gap",
+                        "H 0.8, rms 0.02, |k| in [12, 0.33 Ns] cycles/domain, host gap; "
+                        "Ns 2048-8192 double and 2048-16384 float",
             "rows": rows}
 
 

@@ -73,7 +73,8 @@ typedef struct aspher_op aspher_op;
  * backend FFT and PeriodicFFTOperator(Ns, L, E*)
  * (include/periodic_fft_operator.hpp:26) for backend PERIODIC.  The Love
  * table and its FP64 spectrum are built on the device; synchronous.
- * grid_size must be a power of two in [16, 8192]. */
+ * grid_size must be a power of two in [16, 16384]; at 16384 only FP32
+ * applies and solves exist (FP64 ones return ASPHER_EINVAL). */
 int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
                      aspher_op** out);
 int aspher_op_destroy(aspher_op* op);

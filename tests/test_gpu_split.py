@@ -1,13 +1,17 @@
-"""Free-space operator with the split column pass (B200).
+"""Split transforms and the largest grids (B200).
 
-The zero-padded column of length 2 Ns is transformed as two length-Ns halves
-(even and odd frequencies).  That is the only form an FP64 column of 16384
-points can take (it does not fit one CTA's shared memory), so FP64 applies at
-Ns = 8192 use it; ASPHER_SPLIT_COLUMNS=1 forces it at smaller sizes, where it
-is checked against the oracle and against the one-CTA column pass.  The FP64
-apply at Ns = 8192 is checked through point loads, whose response is the
-Love table itself (the aperiodic convolution of a unit load at a corner
-cell), against the FP32 apply, and for symmetry.
+The zero-padded free-space column of length 2 Ns is transformed as two
+length-Ns halves (even and odd frequencies).  That is the only form an FP64
+column of 16384 points can take (it does not fit one CTA's shared memory), so
+FP64 applies at Ns = 8192 and FP32 applies at Ns = 16384 use it;
+ASPHER_SPLIT_COLUMNS=1 forces it at smaller sizes, where it is checked
+against the oracle and against the one-CTA column pass.  The FP64 Kh build
+likewise assembles rows of 2 Ns reals from the transforms of their even and
+odd samples where a row does not fit (Ns = 16384); ASPHER_SPLIT_KH=1 forces
+that form for the cross-check.  Applies at the large sizes are checked
+through point loads, whose response is the Love table itself (the aperiodic
+convolution of a unit load at a corner cell), through exact periodic Fourier
+modes, against the other precision, and for symmetry.
 """
 
 import os
@@ -22,15 +26,15 @@ from oracle.operators import FFTOperator as OFFT  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def _op(Ns, split=False):
+def _op(Ns, split=False, env="ASPHER_SPLIT_COLUMNS", backend="fft"):
     from aspher_b200 import Operator
     if not split:
-        return Operator("fft", Ns)
-    os.environ["ASPHER_SPLIT_COLUMNS"] = "1"
+        return Operator(backend, Ns)
+    os.environ[env] = "1"
     try:
-        return Operator("fft", Ns)
+        return Operator(backend, Ns)
     finally:
-        del os.environ["ASPHER_SPLIT_COLUMNS"]
+        del os.environ[env]
 
 
 def _mv(op, x, dtype):
@@ -113,3 +117,73 @@ def test_fp64_solve_runs_at_8192():
     p = r.pressure_device
     assert torch.isfinite(p).all() and float(p.min()) >= 0.0
     assert abs(float(p.mean()) / 0.005 - 1.0) < 1e-12
+
+
+@pytest.mark.parametrize("Ns", [256, 1024])
+def test_split_kh_build_matches_one_cta_build(Ns):
+    opk, op = _op(Ns, split=True, env="ASPHER_SPLIT_KH"), _op(Ns)
+    assert opk.info().max_im_ratio < 1e-10
+    x = np.random.default_rng(13).standard_normal(Ns * Ns)
+    y = _mv(op, x, torch.float64)
+    assert rel(_mv(opk, x, torch.float64), y) < 1e-14
+    assert rel(y, OFFT(Ns, 1.0, 1.0).matvec(x)) < 1e-13
+
+
+def test_fp32_free_space_at_16384():
+    Ns = 16384
+    N = Ns * Ns
+    op = _op(Ns)
+    assert op.info().max_im_ratio < 1e-10
+    T = op.love_table()
+    for (jy, jx) in ((0, 0), (Ns - 1, Ns - 1)):
+        x = torch.zeros(N, dtype=torch.float32, device="cuda")
+        x[jy * Ns + jx] = 1.0
+        y = torch.empty_like(x)
+        op.matvec_(x, y)
+        u = y.double().cpu().numpy().reshape(Ns, Ns)
+        ref = T if jy == 0 else T[::-1, ::-1]
+        assert rel(u.ravel(), ref.ravel()) < 2e-6
+        assert np.max(np.abs(u - ref)) < 2e-6 * T[0, 0]
+        del u
+    del T
+    with pytest.raises(Exception):
+        x = torch.zeros(N, dtype=torch.float64, device="cuda")
+        op.matvec_(x, torch.empty_like(x))
+    torch.cuda.synchronize()
+
+
+def test_fp32_periodic_modes_at_16384():
+    Ns, L, Es = 16384, 3.0, 2.5
+    from aspher_b200 import Operator
+    op = Operator("periodic", Ns, L, Es)
+    ix = torch.arange(Ns, dtype=torch.float64, device="cuda")
+    for mx, my in ((1, 0), (3, 7), (4000, 123)):
+        q = 2 * np.pi * np.hypot(mx, my) / L
+        p = torch.cos(2 * np.pi * ((mx * ix[None, :] + my * ix[:, None]) % Ns) / Ns)
+        p32 = p.float().reshape(-1).contiguous()
+        y = torch.empty_like(p32)
+        op.matvec_(p32, y)
+        ref = (2.0 / (Es * q)) * p32.double()
+        assert float(torch.linalg.norm(y.double() - ref) / torch.linalg.norm(ref)) < 2e-6
+        del p, p32, y, ref
+    torch.cuda.synchronize()
+
+
+def test_fp32_solves_at_16384():
+    import aspher_b200 as asb
+    Ns = 16384
+    # a wavy surface made on the device (a 16384^2 self-affine field would take
+    # tens of GB of host memory to synthesise)
+    x = torch.arange(Ns, dtype=torch.float64, device="cuda") / Ns
+    g = (-0.001 * (torch.cos(2 * np.pi * 3 * x)[None, :] + torch.cos(2 * np.pi * 5 * x)[:, None]
+                   + 0.3 * torch.sin(2 * np.pi * 17 * (x[None, :] + 2 * x[:, None])))).reshape(-1)
+    for backend in ("fft", "periodic"):
+        op = _op(Ns, backend=backend)
+        r = asb.solve_device(op, g, 0.005, tol=1e-6, max_iter=6, precond="fourier",
+                             dtype=torch.float32, light=True)
+        assert r.iterations == 6 and r.status == "max_iterations"
+        p = r.pressure_device
+        assert torch.isfinite(p).all() and float(p.min()) >= 0.0
+        assert abs(float(p.double().mean()) / 0.005 - 1.0) < 1e-6
+        del op, r, p
+        torch.cuda.empty_cache()
