@@ -56,7 +56,8 @@ class Result(C.Structure):
                 ("mem_cg_state", C.c_int64), ("mem_best_iterate", C.c_int64),
                 ("mem_contact_mask", C.c_int64), ("mem_output_arrays", C.c_int64),
                 ("mem_peak", C.c_int64), ("time_build", C.c_double),
-                ("time_coarse", C.c_double)]
+                ("time_coarse", C.c_double), ("active_rounds", C.c_int),
+                ("active_fallback", C.c_int), ("time_candidate", C.c_double)]
 
 
 class NestedOpts(C.Structure):
@@ -67,7 +68,10 @@ class NestedOpts(C.Structure):
                 ("coarse_tol", C.c_double), ("single_precision", C.c_int),
                 ("precision", C.c_int), ("float_floor", C.c_double),
                 ("allow_tolerance_relaxation", C.c_int), ("light_result", C.c_int),
-                ("record_error_history", C.c_int), ("active_set", C.c_int)]
+                ("record_error_history", C.c_int), ("active_set", C.c_int),
+                ("active_delta", C.c_double), ("active_halo", C.c_int),
+                ("active_max_rounds", C.c_int), ("active_all_levels", C.c_int),
+                ("active_occupancy_max", C.c_double)]
 
 
 class Stage(C.Structure):

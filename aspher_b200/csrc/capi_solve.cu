@@ -217,6 +217,11 @@ void aspher_nested_opts_default(aspher_nested_opts* o) {
     o->light_result = 0;
     o->record_error_history = 0;
     o->active_set = 0;
+    o->active_delta = 0.05;
+    o->active_halo = 2;
+    o->active_max_rounds = 5;
+    o->active_all_levels = 1;
+    o->active_occupancy_max = 0.4;
 }
 
 int aspher_solve_nested(int backend, int grid_size, double domain_size, double E_star,

@@ -69,6 +69,11 @@ def solve_nested(grid_size, gap, p_nominal, domain_size=1.0, E_star=1.0, coarses
     o.light_result = int(bool(light_result))
     o.record_error_history = int(bool(record_error_history))
     o.active_set = int(bool(active_set))
+    o.active_delta = float(active_delta)
+    o.active_halo = int(active_halo)
+    o.active_max_rounds = int(active_max_rounds)
+    o.active_all_levels = int(bool(active_all_levels))
+    o.active_occupancy_max = float(active_occupancy_max)
     Ns = int(grid_size)
     N = Ns * Ns
     dev = _dev()
@@ -98,4 +103,7 @@ def solve_nested(grid_size, gap, p_nominal, domain_size=1.0, E_star=1.0, coarses
                      for st in stages[:nst.value]]
     r.time_build = res.time_build
     r.time_coarse = res.time_coarse
+    r.time_candidate = res.time_candidate
+    r.active_rounds = res.active_rounds
+    r.active_fallback = bool(res.active_fallback)
     return r

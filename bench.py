@@ -422,6 +422,9 @@ def run_ours(args):
     large = None
     if rank == 0 and not os.environ.get("BENCH_SKIP_LARGE"):
         large = large_single(dev)
+        large["full_grid_levels"] = {k: v for k, v in large_single(dev, active=False).items()
+                                     if k in ("seconds", "status", "finest_iterations",
+                                              "contact_area", "fw_error")}
 
     # the reference's own backend x precision study (fft rows), same settings
     # and surface law, next to its published CPU wall times
@@ -496,17 +499,19 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def large_single(dev, Ns=8192, pbar=0.005):
-    """One nested FP32 solve of the free-space Ns=8192 problem (operator
-    built and graphs captured by an untimed run at Ns=1024 of the same
-    driver; the timed call includes the Ns=8192 operator build)."""
+def large_single(dev, Ns=8192, pbar=0.005, active=True):
+    """One nested FP32 solve of the free-space Ns=8192 problem with
+    active-set (restricted) levels (operator built and graphs captured by an
+    untimed run at Ns=1024 of the same driver; the timed call includes the
+    Ns=8192 operator build the first time); active=False: the same solve
+    with every level on the full grid."""
     import torch
     import aspher_b200 as asb
     from aspher_b200.surfaces import self_affine_gap
     g = torch.from_numpy(self_affine_gap(Ns, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=256.0,
                                          seed=SEED)).to(dev)
     kw = dict(backend="fft", coarsest=256, tol=1e-6, precision="float", float_floor=1e-6,
-              light_result=True)
+              light_result=True, active_set=active)
     gs = torch.from_numpy(self_affine_gap(1024, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=256.0,
                                           seed=SEED)).to(dev)
     asb.solve_nested(1024, gs, pbar, **kw)
@@ -519,8 +524,10 @@ def large_single(dev, Ns=8192, pbar=0.005):
     e1.record()
     torch.cuda.synchronize()
     return {"workload": "free-space Ns=8192, H=0.8, k in [4,256] cycles/domain, rms 0.002, "
-                        "p_nominal 0.005, nested from 256, FP32 (FP64 reductions), tol 1e-6",
+                        "p_nominal 0.005, nested from 256, FP32 (FP64 reductions), tol 1e-6, "
+                        + ("active-set levels" if active else "full-grid levels"),
             "seconds": e0.elapsed_time(e1) / 1e3, "status": r.status,
+            "active_rounds": r.active_rounds, "active_fallback": r.active_fallback,
             "finest_iterations": r.iterations, "fw_error": r.fw_error,
             "penetration_error": r.penetration_error, "contact_area": r.contact_area,
             "stages": [[st["name"], st["iterations"], st["seconds"]] for st in r.stage_stats]}

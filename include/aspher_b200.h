@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define ASPHER_B200_ABI_VERSION 1
+#define ASPHER_B200_ABI_VERSION 2
 
 /* ---- error codes ------------------------------------------------------- */
 #define ASPHER_OK 0
@@ -192,6 +192,9 @@ typedef struct {
     int64_t mem_peak;
     double time_build;       /* nested driver: operator construction, seconds */
     double time_coarse;      /* nested driver: coarse-level solves, seconds */
+    int active_rounds;       /* nested active set: restricted rounds of the finest level */
+    int active_fallback;     /* nested active set: the full-grid fallback solve ran */
+    double time_candidate;   /* nested active set: candidate-set work, seconds */
 } aspher_result;
 
 /* solve_contact_impl<Real> (include/contact_solver.hpp:244-249; reference
@@ -301,7 +304,13 @@ typedef struct {
     int allow_tolerance_relaxation;
     int light_result;
     int record_error_history;
-    int active_set;            /* rejected for fft/periodic, as in the reference */
+    int active_set;            /* restricted (active-set) levels; the reference
+                                  has them for h2 only (nested_solve.cpp:608-617) */
+    double active_delta;       /* candidates: coarse gap < delta * range(level gap) */
+    int active_halo;           /* Chebyshev dilation radius of candidates / violations */
+    int active_max_rounds;     /* restricted rounds before the full-grid fallback */
+    int active_all_levels;     /* restrict every level with a coarser one, not only the finest */
+    double active_occupancy_max; /* restrict only below this contact fraction */
 } aspher_nested_opts;
 
 /* ContactResult::Stage, reference include/contact_solver.hpp:100-113 */

@@ -20,7 +20,8 @@ oracle follows the reference sources line by line instead:
 * ``precond.py``   -- ``src/stencil_precond.cpp:19-109,199-220``,
                       ``src/fourier_precond.cpp:12-116``
 * ``solver.py``    -- ``src/contact_solver.cpp:31-60,69-99,150-587``
-* ``nested.py``    -- ``src/nested_solve.cpp:27-71,518-990`` (fft/periodic)
+* ``nested.py``    -- ``src/nested_solve.cpp:27-990`` (fft/periodic,
+                      with the active-set levels of ``:72-518``)
 * ``api.py``       -- ``python/bindings.cpp:115-234,362-432,637-879``
 
 FFT arithmetic: the reference runs pocketfft (vendored at

@@ -2,8 +2,13 @@
 
 Test infrastructure only (see ``oracle/__init__.py``).  Restates
 ``solve_contact_nested`` (src/nested_solve.cpp:518-990) without the H2
-backend and without the active-set branch (the reference only has the
-latter for h2: nested_solve.cpp:608-617).
+backend.  The active-set branch (``active_level``, nested_solve.cpp:72-518,
+and the restricted PK ``solve_contact_active_impl``,
+contact_solver.cpp:595-1040) is restated for the fft / periodic operators,
+which the reference itself only pairs with h2 (nested_solve.cpp:608-617): the
+restricted PK runs on the compressed candidate vectors, with the operator
+and the preconditioner applied on the full grid and read back at the
+candidates, and the full grid's load (``SolveOptions.n_grid``).
 """
 
 import time
@@ -40,6 +45,110 @@ def prolong_field(pc, Nc):
     return np.repeat(np.repeat(a, 2, axis=0), 2, axis=1).reshape(-1)
 
 
+def dilate_mask(m, Ns, r):
+    """Chebyshev (square) dilation by r, clamped at the edges: a max filter
+    along rows, then along columns (nested_solve.cpp:72-100)."""
+    m = np.asarray(m, dtype=bool).reshape(Ns, Ns)
+    if r <= 0:
+        return m.reshape(-1).copy()
+    tmp = np.zeros_like(m)
+    for d in range(-r, r + 1):
+        lo, hi = max(0, d), Ns + min(0, d)
+        tmp[:, lo - d:hi - d] |= m[:, lo:hi]
+    out = np.zeros_like(m)
+    for d in range(-r, r + 1):
+        lo, hi = max(0, d), Ns + min(0, d)
+        out[lo - d:hi - d, :] |= tmp[lo:hi, :]
+    return out.reshape(-1)
+
+
+def active_level(op, pobj, glvl, p_bar, lvl_tol, max_iter, use_pr, n, p_init, coarse_gap,
+                 g_ref, datum, dt, active_delta, active_halo, active_max_rounds,
+                 record_history, light):
+    """One restricted level (nested_solve.cpp:118-518): candidates from the
+    coarse contact and gap, restricted PK at tol/2 on the compressed
+    candidate vectors, the global check from a full-grid apply, dilated
+    violations added per round, a full-grid fallback solve when no round
+    certifies."""
+    N = n * n
+    R = np.dtype(dt).type
+    gmax, gmin = float(np.max(glvl)), float(np.min(glvl))
+    g_scale = gmax - gmin if gmax > gmin else 1.0
+    delta = active_delta * g_scale
+    vthresh = -lvl_tol * g_scale
+    cm = dilate_mask(np.asarray(p_init) > 0.0, n, active_halo)
+    cg = np.asarray(coarse_gap, dtype=np.float64).reshape(n // 2, n // 2)
+    cm |= (np.repeat(np.repeat(cg, 2, axis=0), 2, axis=1) < delta).reshape(-1)
+    g0c_full = (np.asarray(glvl, dtype=np.float64) - datum).astype(R)
+    pw = np.asarray(p_init, dtype=np.float64)
+    P_total = p_bar * N
+    it_total, rounds, certified, res, hist = 0, 0, False, None, []
+    while rounds < active_max_rounds:
+        rounds += 1
+        idx = np.nonzero(cm)[0]
+
+        def S_c(x, idx=idx):
+            xf = np.zeros(N, dtype=R)
+            xf[idx] = x
+            return op.matvec(xf, dt)[idx]
+
+        pc = None
+        if pobj is not None:
+            def pc(g_, c_, idx=idx):
+                gf = np.zeros(N, dtype=R)
+                gf[idx] = g_
+                cf = np.zeros(N, dtype=bool)
+                cf[idx] = c_
+                return pobj.apply(gf, cf, dt)[idx]
+
+        aopt = SolveOptions(tol=0.5 * lvl_tol, requested_tol=lvl_tol, max_iter=max_iter,
+                            use_pr=use_pr, record_history=record_history,
+                            allow_tolerance_relaxation=True, n_grid=N,
+                            scales=SolveScales(g_ref=g_ref, datum=datum, datum_mode="caller"))
+        res = solve_contact_impl(S_c, g0c_full[idx], p_bar, aopt, pc, pw[idx], dtype=dt)
+        it_total += res.iterations
+        hist += list(res.error_history or [])
+        pfull = np.zeros(N)
+        pfull[idx] = res.pressure
+        u = op.matvec(pfull.astype(R), dt).astype(np.float64)
+        v = u + g0c_full.astype(np.float64)
+        a = res.approach - datum
+        vmin_glob = float(v.min())
+        vmin_loc = float(v[idx].min())
+        viol = (~cm) & (v - a < vthresh)
+        G_glob = res.fw_gap + P_total * (vmin_loc - vmin_glob)
+        fw_glob = G_glob / (P_total * g_ref)
+        pen_glob = max(0.0, -(vmin_glob - a)) / g_ref
+        res.fw_gap, res.fw_error, res.penetration_error = G_glob, fw_glob, pen_glob
+        res.pressure = pfull
+        res.gap = None if light else v - a
+        if res.status == "converged" and not viol.any() and fw_glob <= lvl_tol \
+                and pen_glob <= lvl_tol:
+            certified = True
+            break
+        if not viol.any():
+            break
+        cm |= dilate_mask(viol, n, active_halo)
+        pw = pfull
+    fallback = False
+    if not certified:
+        fopt = SolveOptions(tol=lvl_tol, requested_tol=lvl_tol, max_iter=max_iter,
+                            use_pr=use_pr, light=light, record_history=record_history,
+                            keep_best=not light, allow_tolerance_relaxation=True,
+                            scales=SolveScales(g_ref=g_ref, datum=datum, datum_mode="caller"))
+        mv = (lambda x: op.matvec(x, dt))
+        pcf = None if pobj is None else (lambda g_, c_: pobj.apply(g_, c_, dt))
+        res = solve_contact_impl(mv, g0c_full, p_bar, fopt, pcf, res.pressure, dtype=dt)
+        it_total += res.iterations
+        hist += list(res.error_history or [])
+        fallback = True
+    res.iterations = it_total
+    res.error_history = hist
+    res.active_rounds = rounds
+    res.active_fallback = fallback
+    return res
+
+
 def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
                          use_pr=True, coarsest=64, precond=True,
                          precond_engine="auto", precond_radius=2,
@@ -47,7 +156,9 @@ def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
                          single_precision=False, precision="",
                          float_floor=2e-6, allow_tolerance_relaxation=False,
                          light_result=False, backend="fft",
-                         record_error_history=False, leaf_side=8, **_unused):
+                         record_error_history=False, leaf_side=8, active_set=False,
+                         active_delta=0.05, active_halo=2, active_max_rounds=5,
+                         active_all_levels=True, active_occupancy_max=0.4, **_unused):
     g0 = np.asarray(g0, dtype=np.float64).reshape(-1)
     if Ns <= 0:
         raise ValueError("solve_contact_nested: Ns must be positive")
@@ -82,6 +193,14 @@ def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
         raise ValueError("solve_contact_nested: Ns must equal coarsest * 2^k")
     if backend not in ("fft", "periodic"):
         raise ValueError("oracle nested driver: backend must be fft or periodic")
+    if active_set:
+        if active_halo < 0 or active_max_rounds < 1 or not (active_delta >= 0.0) \
+                or not (active_occupancy_max > 0.0):
+            raise ValueError("solve_contact_nested: bad active-set parameters")
+        if policy == "float_then_double":
+            raise ValueError("solve_contact_nested: float_then_double with active_set")
+        if len(levels) < 2:
+            raise ValueError("solve_contact_nested: active_set needs a coarse level")
 
     ncoarse = len(levels) - 1
     gap = [None] * ncoarse
@@ -94,6 +213,7 @@ def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
     g_ref = max(g_max_f - g_min_f, p_bar * L / E_star)
 
     p_init = None
+    coarse_gap = None
     prev_occupancy = -1.0
     stages = []
     res = None
@@ -121,7 +241,13 @@ def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
             lvl_tol = float_floor
         elif any_float:
             lvl_tol = max(lvl_tol, float_floor)
-        light = light_result if finest else True
+        gate_open_next = prev_occupancy < 0.0 or prev_occupancy < active_occupancy_max
+        keep_gap = bool(active_set and not finest and gate_open_next
+                        and (active_all_levels or li + 2 == len(levels)))
+        light = light_result if finest else not keep_gap
+        use_active = bool(active_set and p_init is not None and coarse_gap is not None
+                          and prev_occupancy < active_occupancy_max
+                          and (finest or active_all_levels))
         opt = SolveOptions(tol=lvl_tol, requested_tol=(tol if finest else coarse_tol),
                            max_iter=max_iter, use_pr=use_pr, light=light,
                            record_history=finest and record_error_history,
@@ -141,9 +267,16 @@ def solve_contact_nested(Ns, L, E_star, g0, p_bar, tol=1e-8, max_iter=20000,
         pc = None
         if pobj is not None:
             pc = (lambda g_, c_, pobj=pobj, dt=dt: pobj.apply(g_, c_, dt))
-        res = solve_contact_impl(mv, gl, p_bar, opt, pc, p_init, dtype=dt)
+        if use_active:
+            res = active_level(op, pobj, glvl, p_bar, lvl_tol, max_iter, use_pr, n, p_init,
+                               coarse_gap, g_ref, datum, dt, active_delta, active_halo,
+                               active_max_rounds, finest and record_error_history, light)
+        else:
+            res = solve_contact_impl(mv, gl, p_bar, opt, pc, p_init, dtype=dt)
+        coarse_gap = res.gap if keep_gap else None
         prev_occupancy = res.contact_fraction
-        stages.append(dict(name=("finest:" if finest else "coarse:") + str(n),
+        stages.append(dict(name=("finest:" if finest else "coarse:") + str(n)
+                           + ("(active)" if use_active else ""),
                            precision="float" if any_float else "double",
                            requested_tol=opt.requested_tol, effective_tol=opt.tol,
                            iterations=res.iterations, matvec_count=res.matvec_count,

@@ -45,6 +45,7 @@ class SolveOptions:
     stall_limit: int = 200
     precond_cost_gate: float = 0.0
     allow_tolerance_relaxation: bool = False
+    n_grid: int = 0  # > 0: the full grid's size when g0 holds a candidate subset
     scales: SolveScales = field(default_factory=SolveScales)
 
 
@@ -142,7 +143,10 @@ def solve_contact_impl(S: Callable, g0, p_bar, opt: SolveOptions,
     if not np.all(np.isfinite(g0)):
         raise ValueError("solve_contact: g0 contains non-finite values")
 
-    P_total = float(p_bar) * N
+    # restricted solves see the candidate subset but carry the full grid's
+    # load (contact_solver.cpp:628-630)
+    N_grid = opt.n_grid if opt.n_grid > 0 else N
+    P_total = float(p_bar) * N_grid
     gmin_v = float(g0.min())
     gmax_v = float(g0.max())
     g_ref = opt.scales.g_ref
@@ -165,6 +169,8 @@ def solve_contact_impl(S: Callable, g0, p_bar, opt: SolveOptions,
         datum = opt.scales.datum
         subtract = False
     gshift = R(datum) if subtract else R(0)
+    # uniform start: p_bar, or P_total / Nc on a candidate subset
+    p_unif = p_bar if N_grid == N else R(P_total / N)
     g0s = (g0 - gshift).astype(R)  # the Real expression g0(i) - gshift
 
     if p_init is not None:
@@ -176,9 +182,9 @@ def solve_contact_impl(S: Callable, g0, p_bar, opt: SolveOptions,
         if s > 0.0:
             p = (p * R(P_total / s)).astype(R)
         else:
-            p = np.full(N, p_bar, dtype=R)
+            p = np.full(N, p_unif, dtype=R)
     else:
-        p = np.full(N, p_bar, dtype=R)
+        p = np.full(N, p_unif, dtype=R)
     t = np.zeros(N, dtype=R)
     u = np.zeros(N, dtype=R)
     g = np.zeros(N, dtype=R)
@@ -357,7 +363,7 @@ def solve_contact_impl(S: Callable, g0, p_bar, opt: SolveOptions,
                 if total > 0.0:
                     p = (p * R(P_total / total)).astype(R)
                 else:
-                    p = np.full(N, p_bar, dtype=R)
+                    p = np.full(N, p_unif, dtype=R)
                 did_cg = True
         if not did_cg:
             if not identification_step():
@@ -393,8 +399,8 @@ def solve_contact_impl(S: Callable, g0, p_bar, opt: SolveOptions,
                        0.5 * u.astype(np.float64) + g0s.astype(np.float64)))
     res.objective = obj + datum * P_total
     res.iterations = it
-    res.contact_fraction = d["nc"] / N
-    res.mean_pressure = d["psum"] / N
+    res.contact_fraction = d["nc"] / N_grid
+    res.mean_pressure = d["psum"] / N_grid
     res.status = status
     res.status_reason = reason
     res.converged = status == "converged"

@@ -56,12 +56,20 @@ def test_auto_engine_is_fft_on_periodic():
     assert runs["stencil"].iterations > runs["fft"].iterations
 
 
-def test_active_set_rejected_and_bad_arguments():
+def test_active_set_bad_arguments():
+    """nested_solve.cpp:567-580,593-597,608-617: the active-set argument
+    checks (the backend restriction to h2 excepted: this build restricts
+    the fft / periodic levels)."""
     import aspher_b200 as hc
     g = _rough(128)
-    with pytest.raises(ValueError):
-        hc.solve_nested(grid_size=128, gap=g, p_nominal=0.01, coarsest=32, backend="periodic",
-                        active_set=True)
+    for kw in (dict(precision="float_then_double"), dict(coarsest=128),
+               dict(active_halo=-1), dict(active_max_rounds=0), dict(active_delta=-0.1),
+               dict(active_occupancy_max=0.0)):
+        args = dict(coarsest=32)
+        args.update(kw)
+        with pytest.raises(ValueError):
+            hc.solve_nested(grid_size=128, gap=g, p_nominal=0.01, backend="periodic",
+                            active_set=True, **args)
     with pytest.raises(ValueError):
         hc.solve_nested(grid_size=128, gap=g, p_nominal=0.01, coarsest=48, backend="fft")
     with pytest.raises(ValueError):
@@ -121,3 +129,56 @@ def test_gap_datum_invariance_nested():
             assert r.status == "converged"
             assert abs(r.approach - ref.approach - shift) < 1e-6 * max(1.0, shift)
             assert rel(r.pressure, ref.pressure) < (1e-4 if single else 1e-5)
+
+
+@pytest.mark.parametrize("backend,precision", [("fft", "double"), ("fft", "float"),
+                                               ("periodic", "double"), ("periodic", "float")])
+def test_active_set_nested_matches_full_and_oracle(backend, precision):
+    """Restricted (active-set) levels: a certified restricted solve is a
+    certified solve of the full problem (global Frank-Wolfe gap and
+    penetration from a full-grid apply), so it agrees with the full nested
+    solve and with the oracle's restricted driver within the certified
+    tolerance."""
+    import aspher_b200 as hc
+    from oracle.nested import solve_contact_nested as onested
+    ns, pbar = 256, 0.005
+    tol = 1e-7 if precision == "double" else 2e-6
+    g = hc.self_affine_gap(ns, hurst=0.8, rms=0.002, seed=42)
+    kw = dict(coarsest=64, tol=tol, precision=precision, backend=backend, light_result=False)
+    full = hc.solve_nested(ns, g, pbar, **kw)
+    act = hc.solve_nested(ns, g, pbar, active_set=True, **kw)
+    ora = onested(ns, 1.0, 1.0, g, pbar, active_set=True, **kw)
+    assert full.status == "converged" and act.status == "converged" and ora.status == "converged"
+    names = [st["name"] for st in act.stage_stats]
+    assert names == ["coarse:64", "coarse:128(active)", "finest:256(active)"], names
+    assert act.active_rounds >= 1 and not act.active_fallback
+    assert act.fw_error <= tol and act.penetration_error <= tol
+    assert rel(act.pressure, full.pressure) <= 20 * tol
+    assert rel(act.pressure, ora.pressure) <= 20 * tol
+    assert abs(act.contact_area - full.contact_area) <= 1e-4
+    assert abs(act.iterations - ora.iterations) <= max(3, ora.iterations // 4)
+    # the fields come from the certifying apply: gap = u + g0 - approach
+    gap = np.asarray(act.gap).ravel()
+    u = np.asarray(act.displacement).ravel()
+    assert np.max(np.abs(gap - (u + g - act.approach))) <= 1e-9 * np.max(np.abs(g))
+    assert gap.min() >= -tol * max(g.max() - g.min(), pbar) * 1.01
+
+
+def test_active_set_fallback_and_expansion():
+    """A candidate set that misses contact: no halo and delta 0 leave out
+    the points that the finer level brings into contact; one round then
+    fails the global check and the full-grid fallback solve certifies."""
+    import aspher_b200 as hc
+    ns, pbar, tol = 256, 0.02, 1e-7
+    g = hc.self_affine_gap(ns, hurst=0.8, rms=0.002, seed=5)
+    kw = dict(coarsest=64, tol=tol, backend="fft", light_result=True)
+    full = hc.solve_nested(ns, g, pbar, **kw)
+    one = hc.solve_nested(ns, g, pbar, active_set=True, active_halo=0, active_delta=0.0,
+                          active_max_rounds=1, **kw)
+    assert one.status == "converged" and one.active_fallback and one.active_rounds == 1
+    assert rel(one.pressure, full.pressure) <= 20 * tol
+    many = hc.solve_nested(ns, g, pbar, active_set=True, active_halo=0, active_delta=0.0,
+                           active_max_rounds=8, **kw)
+    assert many.status == "converged"
+    assert many.active_rounds > 1 or many.active_fallback
+    assert rel(many.pressure, full.pressure) <= 20 * tol
