@@ -183,3 +183,52 @@ def test_singleton_warm_start_repaired():
     assert got.status == "converged" and got.iterations > 0
     rel = np.linalg.norm(got.pressure - cold.pressure) / np.linalg.norm(cold.pressure)
     assert rel < 1e-6
+
+
+def test_dilate_mask_chebyshev_clamped():
+    """nested_solve.cpp:72-100: square (Chebyshev) dilation, clamped at the
+    grid edges (no wrap)."""
+    from oracle.nested import dilate_mask
+    n = 9
+    m = np.zeros(n * n, bool)
+    m[0] = True            # corner (0, 0)
+    m[4 * n + 6] = True    # (4, 6)
+    d = dilate_mask(m, n, 2).reshape(n, n)
+    ref = np.zeros((n, n), bool)
+    ref[0:3, 0:3] = True
+    ref[2:7, 4:9] = True
+    assert np.array_equal(d, ref)
+    assert np.array_equal(dilate_mask(m, n, 0), m)
+
+
+@pytest.mark.parametrize("backend", ["fft", "periodic"])
+def test_oracle_active_set_nested_matches_full(backend):
+    """The restricted (active-set) levels certify the full problem: the
+    result equals the full nested solve within the tolerance; a candidate
+    set without halo or gap margin needs an expansion round or the
+    fallback, and still certifies."""
+    from oracle.nested import solve_contact_nested
+    from aspher_b200.surfaces import self_affine_gap
+    ns, tol = 128, 1e-7
+    g = self_affine_gap(ns, hurst=0.8, rms=0.002, seed=42)
+    kw = dict(coarsest=32, tol=tol, backend=backend, light_result=True)
+    full = solve_contact_nested(ns, 1.0, 1.0, g, 0.005, **kw)
+    act = solve_contact_nested(ns, 1.0, 1.0, g, 0.005, active_set=True, **kw)
+    assert full.status == "converged" and act.status == "converged"
+    assert [s["name"] for s in act.stage_stats] == ["coarse:32", "coarse:64(active)",
+                                                    "finest:128(active)"]
+    assert act.fw_error <= tol and act.penetration_error <= tol
+    rel = np.linalg.norm(act.pressure - full.pressure) / np.linalg.norm(full.pressure)
+    assert rel <= 20 * tol
+    tight = solve_contact_nested(ns, 1.0, 1.0, g, 0.005, active_set=True, active_halo=0,
+                                 active_delta=0.0, active_max_rounds=1, **kw)
+    assert tight.status == "converged" and tight.active_rounds == 1
+    rel = np.linalg.norm(tight.pressure - full.pressure) / np.linalg.norm(full.pressure)
+    assert rel <= 20 * tol
+    # above active_occupancy_max (the coarse contact fraction) no level is restricted
+    gated = solve_contact_nested(ns, 1.0, 1.0, g, 0.005, active_set=True,
+                                 active_occupancy_max=1e-6, **kw)
+    assert not any("(active)" in s["name"] for s in gated.stage_stats)
+    with pytest.raises(ValueError):
+        solve_contact_nested(ns, 1.0, 1.0, g, 0.005, active_set=True,
+                             precision="float_then_double", **kw)
