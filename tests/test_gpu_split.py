@@ -187,3 +187,27 @@ def test_fp32_solves_at_16384():
         assert abs(float(p.double().mean()) / 0.005 - 1.0) < 1e-6
         del op, r, p
         torch.cuda.empty_cache()
+
+
+def test_fp32_nested_at_16384_and_fp64_rejected():
+    """solve_nested up to Ns = 16384 in FP32 (the size at which the
+    reference's fft rows ran out of memory); FP64 there is refused with
+    ValueError."""
+    import aspher_b200 as asb
+    from aspher_b200.surfaces import self_affine_gap_device
+    Ns, pbar = 16384, 0.002
+    g = self_affine_gap_device(Ns, hurst=0.8, rms=0.02, k_lo=12.0, k_hi=0.33 * Ns, seed=42)
+    r = asb.solve_nested(Ns, g, pbar, coarsest=4096, tol=1e-6, single_precision=True,
+                         allow_tolerance_relaxation=True, light_result=True, backend="fft")
+    assert r.status == "converged", (r.status, r.status_reason)
+    assert [st["name"] for st in r.stage_stats] == ["coarse:4096", "coarse:8192",
+                                                    "finest:16384"]
+    assert r.fw_error <= r.effective_tol and r.penetration_error <= r.effective_tol
+    p = r.pressure_device
+    assert float(p.min()) >= 0.0 and abs(float(p.mean()) / pbar - 1.0) < 1e-6
+    assert 0.0 < r.contact_area < 0.05
+    del p, r
+    torch.cuda.empty_cache()
+    with pytest.raises(ValueError):
+        asb.solve_nested(Ns, g, pbar, coarsest=8192, tol=1e-6, light_result=True,
+                         backend="fft", precision="double")
