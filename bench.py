@@ -21,10 +21,14 @@ wall times; at 16384 it ran out of memory).  Ranks solve disjoint
 problem sets (seed 42 + 1000*rank): weak scaling, no collective on the
 data path.
 
-``--impl reference`` times the reference algorithm's CPU implementation of
-the same workload (the oracle restatement, all host cores for its FFTs):
-each step runs a bounded sample of PCG iterations of one problem and scales
-it by that problem's oracle iteration count (tests/golden/bench_iterations.json).
+``--impl reference`` times the reference's own CPU implementation of the
+same workload: its unmodified hot-path C++ built here with OpenMP
+(oracle/_ref, see oracle/ref.py) on every host core.  Each step samples the
+six problems with two bounded solves each (stopped after 3 and 9 PCG
+iterations); a whole solve is the fitted fixed part plus the per-iteration
+slope times the reference's own iteration count
+(tests/golden/ref_ns2048.json), and one complete solve of the cheapest
+problem checks that prediction.
 """
 
 import argparse
@@ -157,20 +161,6 @@ def measured_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def profiled_traffic(name):
-    """dram bytes per launch of `name` from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "traffic.txt")
-    try:
-        with open(path) as f:
-            for line in f:
-                k, _, v = line.partition(":")
-                if k.strip() == name:
-                    return float(v.split()[0])
-    except OSError:
-        pass
-    return None
 
 
 # ---- our arm ----------------------------------------------------------------------
@@ -372,17 +362,28 @@ def run_ours(args):
     alg_bytes = 12 * 4 * N  # 12 b N, b = 4 (free-space apply model)
     achieved = alg_bytes / t_apply / 1e9
 
-    # whole-solve roofline: modelled bytes of every PCG iteration (two applies
-    # + stencil + vector passes: 2 B_op + (9 + 107) N bytes at FP32, scaled by
-    # b / 4 for the FP64 iterations) over the timed solve time
-    def iter_bytes(backend, b):
-        bop = (12 if backend == "fft" else 6) * b * N
-        return 2 * bop + (9 + 107) * N * b / 4
+    # whole-solve roofline: modelled bytes of every PCG iteration over the
+    # timed solve time.  FP32 stage: 2 B_op (12 b N free space, 6 b N
+    # periodic, b = 4) + the stencil and vector passes (9 + 107) N.  FP64
+    # polish stage: its loop applies run FP32 transforms with FP64 loads and
+    # stores (u = u0 + S32(p - p0): p, p0, u0 read and u written in FP64;
+    # r = S32(t): t read and r written in FP64), its vector passes are FP64
+    # (2 x 116 N), plus one exact FP64 apply at the stage start.
+    def iter_bytes_f32(backend):
+        return 2 * (48 if backend == "fft" else 24) * N + 116 * N
+
+    def iter_bytes_polish(backend):
+        tr = (24 if backend == "fft" else 8) * N  # FP32 transform interior
+        side = (8 if backend == "fft" else 4) * N  # FP32 spectrum written / read by the rows
+        u_apply = 16 * N + side + tr + side + 16 * N
+        r_apply = 8 * N + side + tr + side + 8 * N
+        return u_apply + r_apply + 232 * N
     solve_bytes = 0.0
     order = [b for b in BACKENDS for _ in by_backend[b]]
     for bk, (r, rf) in zip(order, last):
-        solve_bytes += rf.iterations * iter_bytes(bk, 4)
-        solve_bytes += (r.iterations - rf.iterations) * iter_bytes(bk, 8)
+        npol = r.iterations - rf.iterations
+        solve_bytes += rf.iterations * iter_bytes_f32(bk)
+        solve_bytes += npol * iter_bytes_polish(bk) + (96 if bk == "fft" else 48) * N
     solve_gbs = solve_bytes * args.steps * world / dt / 1e9
 
     # uneven batch: 96 problems (Ns 256..2048, both backends, loads
@@ -491,11 +492,13 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "kernel": "free-space apply FP32 Ns=2048 "
                          "(row_fwd+col+row_inv)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": profiled_traffic("fft_apply_f32_2048"),
+                         "traffic": None,
                          "alg_bytes": alg_bytes, "t_apply_ms": t_apply * 1e3},
             "solve_roofline": {"achieved": solve_gbs, "peak": peak, "unit": "GB/s",
                                "frac": solve_gbs / peak,
-                               "model": "per iteration 2 B_op + 116 b N / 4 bytes"},
+                               "model": "FP32 iterations 2 B_op(b=4) + 116 N; FP64 polish "
+                                        "iterations FP32 transforms with FP64 row I/O + "
+                                        "232 N vector passes; one FP64 apply per polish"},
             "gpu_launches": launches,
             "clocks": clocks,
             "wall_s_timed": wall,
@@ -503,7 +506,7 @@ def run_ours(args):
                         "fp64_gpu": step_ms[2], "e2e": step_ms[3]},
         }
         it64 = [r.iterations for r in last64]
-        line["cpu_baseline"] = (cpu_baseline(gpu_fp64_iterations=it64[1])
+        line["cpu_baseline"] = (cpu_baseline()
                                 if not os.environ.get("BENCH_SKIP_CPU")
                                 else {"value": None, "sample": "skipped (BENCH_SKIP_CPU)"})
         print(json.dumps(line), flush=True)
@@ -712,70 +715,135 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
     return out
 
 
-# ---- CPU baseline / reference arm (the oracle restatement) ----------------------------
-def _oracle_iterations():
-    with open(os.path.join(ROOT, "tests", "golden", "bench_iterations.json")) as f:
-        return json.load(f)["problems"]
+# ---- CPU baseline / reference arm ---------------------------------------------------
+# The reference's own C++ (oracle/_ref: the unmodified hot-path sources built
+# with OpenMP and the vendored pocketfft, see oracle/ref.py) on the host
+# cores; the numpy restatement of oracle/ only where that library is absent.
+def _ref_iterations():
+    """The reference's own iteration counts of the six Ns=2048 problems
+    (tests/golden/ref_ns2048.json, written by make_ref_fixtures.py from the
+    reference's solves)."""
+    with open(os.path.join(ROOT, "tests", "golden", "ref_ns2048.json")) as f:
+        probs = json.load(f)["problems"]
+    return {k: v["tol6"]["iterations"] for k, v in probs.items()}
 
 
-def _oracle_sample(backend, pbar, g, n_iter):
-    """Seconds per PCG iteration of the oracle on one problem (n_iter iterations)."""
+def _cpu_solver_factory():
+    from oracle import ref
+    if ref.available():
+        return (lambda b: ref.ContactSolver(NS, backend=b)), "reference", ref.threads()
     from oracle.api import ContactSolver
-    s = ContactSolver(NS, backend=backend)
+    from oracle import operators as oops
+    return (lambda b: ContactSolver(NS, backend=b)), "port", oops.WORKERS
+
+
+def _cpu_solve_seconds(solver, g, pbar, n_iter):
+    from oracle import ref
+    kw = dict(light=True) if isinstance(solver, ref.ContactSolver) else {}
     t0 = time.perf_counter()
-    r = s.solve(g, pbar, tol=TOL, max_iter=n_iter, precond="fourier")
-    dt = time.perf_counter() - t0
-    return dt / max(1, r.iterations), r.iterations
+    r = solver.solve(g, pbar, tol=TOL, max_iter=n_iter, precond="fourier", **kw)
+    return time.perf_counter() - t0, r
 
 
-def cpu_baseline(n_iter=6, gpu_fp64_iterations=None):
-    """Oracle FP64 solve of one problem (fft, p=0.005), n_iter iterations timed,
-    scaled to that problem's full oracle iteration count (or, when that count
-    is not recorded, to the FP64 GPU solve's count for the same problem)."""
-    try:
+class CpuSampler:
+    """Time of a whole CPU solve of each Ns=2048 benchmark problem from two
+    bounded samples: solves stopped after n1 and n2 PCG iterations give the
+    per-iteration slope (t2 - t1) / (n2 - n1) and the fixed part t1 - n1 slope
+    (set-up, first and final evaluation), and a solve of n iterations takes
+    fixed + n slope; n is the reference's own iteration count of the
+    problem."""
+
+    def __init__(self, n1=3, n2=9):
         from aspher_b200.surfaces import self_affine_gap
-        from oracle import operators as oops
-        g = self_affine_gap(NS, hurst=0.8, rms=0.002, seed=SEED)
-        try:
-            full = _oracle_iterations()["fft_0.005"]["iterations"]
-        except (OSError, KeyError):
-            full = gpu_fp64_iterations
-        if not full:
-            raise RuntimeError("no iteration count to scale the sample by")
-        spi, k = _oracle_sample("fft", 0.005, g, n_iter)
-        return {"value": 1.0 / (spi * full), "unit": "solves/s", "cores": oops.WORKERS,
-                "kind": "port",
-                "sample": "oracle FP64 solve, fft Ns=2048 p=0.005 stencil precond: %d PCG "
-                          "iterations timed (%.2f s/iteration), scaled to the oracle's full "
-                          "%d iterations; scipy pocketfft on %d threads, numpy vector passes "
-                          "single-threaded" % (k, spi, full, oops.WORKERS)}
+        self.n1, self.n2 = n1, n2
+        make, self.kind, self.cores = _cpu_solver_factory()
+        self.solvers = {b: make(b) for b in BACKENDS}
+        self.g = self_affine_gap(NS, hurst=0.8, rms=0.002, seed=SEED)
+        self.iters = _ref_iterations()
+        self.fits = {}
+
+    def sample(self, backend, pbar):
+        s = self.solvers[backend]
+        t1, _ = _cpu_solve_seconds(s, self.g, pbar, self.n1)
+        t2, _ = _cpu_solve_seconds(s, self.g, pbar, self.n2)
+        slope = max(t2 - t1, 0.0) / (self.n2 - self.n1)
+        fixed = max(t1 - self.n1 * slope, 0.0)
+        self.fits.setdefault((backend, pbar), []).append((slope, fixed))
+        return t1 + t2
+
+    def predicted(self, backend, pbar):
+        fits = self.fits[(backend, pbar)]
+        slope = statistics.mean(f[0] for f in fits)
+        fixed = statistics.mean(f[1] for f in fits)
+        return fixed + slope * self.iters["%s_%g" % (backend, pbar)]
+
+    def workload_seconds(self):
+        return sum(self.predicted(b, p) for b in BACKENDS for p in LOADS)
+
+    def validate(self, backend="periodic", pbar=0.001):
+        """One complete CPU solve of the cheapest problem, against the
+        prediction from its samples."""
+        if (backend, pbar) not in self.fits:
+            self.sample(backend, pbar)
+        sec, r = _cpu_solve_seconds(self.solvers[backend], self.g, pbar, 5000)
+        return {"problem": "%s p_nominal %g" % (backend, pbar), "status": r.status,
+                "iterations": r.iterations, "measured_s": round(sec, 3),
+                "predicted_s": round(self.predicted(backend, pbar), 3)}
+
+    def describe(self):
+        what = ("the reference's own C++ (unmodified src/ hot-path files, OpenMP, pocketfft)"
+                if self.kind == "reference" else "the oracle's numpy restatement")
+        return ("%s on %d host threads, FP64 solves of the six Ns=2048 problems (tol 1e-6, "
+                "stencil precond): each problem timed stopped after %d and after %d PCG "
+                "iterations, whole-solve time = fixed part + per-iteration slope x the "
+                "reference's own iteration count" % (what, self.cores, self.n1, self.n2))
+
+
+def cpu_baseline(**_unused):
+    """The CPU baseline of our arm's line (rank 0, N = 1): one sampling pass
+    over the six problems and one complete solve of the cheapest (about
+    10 s on 16 host threads)."""
+    try:
+        cs = CpuSampler()
+        for b in BACKENDS:
+            for p in LOADS:
+                cs.sample(b, p)
+        val = cs.validate()
+        sec = cs.workload_seconds()
+        return {"value": len(BACKENDS) * len(LOADS) / sec, "unit": "solves/s",
+                "cores": cs.cores, "kind": cs.kind, "sample": cs.describe(),
+                "validation": val}
     except Exception as e:  # the baseline must never sink the GPU line
         return {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": "unavailable: %s" % e}
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU implementation of the path
+    on the host cores, on our arm's workload and metric.  Each step samples
+    all six problems (two bounded solves each); the line's value is the
+    whole workload's solves/s from the per-problem fits; ms_per_step is the
+    time the step's samples actually took."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from aspher_b200.surfaces import self_affine_gap
-    from oracle import operators as oops
-    g = self_affine_gap(NS, hurst=0.8, rms=0.002, seed=SEED)
-    its = _oracle_iterations()
-    probs = [(b, p) for b in BACKENDS for p in LOADS]
-    n_iter = 4
+    cs = CpuSampler()
     for w in range(args.warmup):
-        b, p = probs[w % len(probs)]
-        _oracle_sample(b, p, g, 1)
-    per_solve = []
+        cs.sample(*[(b, p) for b in BACKENDS for p in LOADS][w % 6])
+    cs.fits.clear()
+    validation = cs.validate()
+    cs.fits.clear()
+    step_s = []
     t0 = time.perf_counter()
-    for s in range(args.steps):
-        b, p = probs[s % len(probs)]
-        spi, _ = _oracle_sample(b, p, g, n_iter)
-        per_solve.append(spi * its["%s_%g" % (b, p)]["iterations"])
+    for _ in range(args.steps):
+        s0 = time.perf_counter()
+        for b in BACKENDS:
+            for p in LOADS:
+                cs.sample(b, p)
+        step_s.append(time.perf_counter() - s0)
     wall = time.perf_counter() - t0
-    sec = statistics.mean(per_solve)
-    value = 1.0 / sec
+    value = len(BACKENDS) * len(LOADS) / cs.workload_seconds()
+    sample = cs.describe() + "; per step all six problems sampled"
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -784,22 +852,22 @@ def run_reference(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": sec * 1e3,
+        "ms_per_step": statistics.mean(step_s) * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded self-affine surfaces)",
         "config": {"workload": "Ns=2048 single solves: fft+periodic x p_nominal "
-                               "{0.001,0.005,0.02}, tol 1e-6, stencil precond",
+                               "{0.001,0.005,0.02}, tol 1e-6, stencil precond, FP64",
                    "grid_size": NS, "tol": TOL},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": oops.WORKERS,
-                         "kind": "port",
-                         "sample": "per step: %d oracle FP64 PCG iterations of one problem "
-                                   "(cycling the 6), scaled by its full oracle iteration "
-                                   "count" % n_iter},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cs.cores,
+                         "kind": cs.kind, "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "validation": validation,
+        "predicted_solve_seconds": {"%s_%g" % (b, p): round(cs.predicted(b, p), 3)
+                                    for b in BACKENDS for p in LOADS},
         "wall_s_timed": wall,
     }
     print(json.dumps(line), flush=True)

@@ -15,7 +15,6 @@ from oracle.precond import FourierPreconditioner, StencilPreconditioner
 from oracle.solver import SolveOptions, project_load_simplex, solve_contact_impl
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-REF_FIXTURE = "/root/reference/tests/data/love_reference.txt"
 
 # tests/test_stencil.cpp:21-33 (universal constants of w = F^-1|k| / w(0,0))
 STENCIL_GOLDEN = {(0, 0): 1.0, (1, 0): -0.180875, (1, 1): -0.032860, (2, 0): 0.021189,
@@ -30,17 +29,12 @@ def test_love_golden_fixture():
     assert rel.max() <= 1e-12  # test_kernel_stability.cpp:53-83 gate
 
 
-@pytest.mark.skipif(not os.path.exists(REF_FIXTURE), reason="reference tree not mounted")
 def test_love_reference_fixture():
-    """The reference's own 80-digit fixture (test_kernel_stability.cpp:53-83)."""
-    rows = []
-    with open(REF_FIXTURE) as f:
-        for line in f:
-            if line.startswith("#") or not line.strip():
-                continue
-            rows.append([float(v) for v in line.split()[:5]])
-    r = np.array(rows)
-    assert len(r) > 300
+    """The reference's own 80-digit fixture (tests/data/love_reference.txt,
+    read by test_kernel_stability.cpp:53-83), committed as
+    tests/golden/love_reference.txt by make_reference_fixtures_txt.py."""
+    r = np.loadtxt(os.path.join(GOLDEN, "love_reference.txt"))
+    assert len(r) == 472
     got = love_uz(r[:, 0], r[:, 1], r[:, 2], r[:, 3])
     rel = np.abs(got - r[:, 4]) / np.abs(r[:, 4])
     assert rel.max() <= 1e-12
