@@ -96,6 +96,8 @@ SIGNATURES = {
     "aspher_status_string": (C.c_char_p, [C.c_int]),
     "aspher_op_create": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double,
                                    C.POINTER(C.c_void_p)]),
+    "aspher_op_create_ex": (C.c_int, [C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
+                                      C.POINTER(C.c_void_p)]),
     "aspher_op_destroy": (C.c_int, [C.c_void_p]),
     "aspher_op_matvec": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_op_get_info": (C.c_int, [C.c_void_p, C.POINTER(OpInfo)]),

@@ -56,7 +56,13 @@ def _as_vector(a, expected, name="array"):
 class Operator:
     """Device operator handle (free-space FFT or periodic)."""
 
-    def __init__(self, backend, grid_size, domain_size=1.0, E_star=1.0):
+    # creation flags (aspher_op_create_ex): the split column pass and the
+    # split FP64 Kh build at sizes where the one-CTA forms fit, for
+    # cross-checks of the forms the largest grids need
+    SPLIT_COLUMNS = 1
+    SPLIT_KH = 2
+
+    def __init__(self, backend, grid_size, domain_size=1.0, E_star=1.0, flags=0):
         if backend not in L.BACKEND:
             raise ValueError("unknown backend: %s (this build implements 'fft' and "
                              "'periodic')" % backend)
@@ -67,8 +73,8 @@ class Operator:
         self.domain_size = float(domain_size)
         self.E_star = float(E_star)
         h = C.c_void_p()
-        L.check(L.lib().aspher_op_create(L.BACKEND[backend], self.Ns, self.domain_size,
-                                         self.E_star, C.byref(h)))
+        L.check(L.lib().aspher_op_create_ex(L.BACKEND[backend], self.Ns, self.domain_size,
+                                            self.E_star, int(flags), C.byref(h)))
         self._h = h
 
     def __del__(self):
@@ -160,6 +166,12 @@ class ContactResult:
         self.time_coarse = 0.0
         self.active_rounds = 0
         self.active_fallback = False
+        # accuracy of a float / float_then_double result against the plain
+        # FP64 solve of the same problem (ContactSolver.solve(...,
+        # reference_fp64=True)); None where it was not measured
+        self.pressure_rel_l2_vs_fp64 = None
+        self.contact_area_error_vs_fp64 = None
+        self.fp64_status = None
 
     def _grid(self, t):
         if t is None:
@@ -411,7 +423,8 @@ class ContactSolver:
         return y.cpu().numpy()
 
     def solve(self, gap, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precond="none",
-              p_init=None, *, precision="double", float_tol=None, polish_tol=None):
+              p_init=None, *, precision="double", float_tol=None, polish_tol=None,
+              reference_fp64=False):
         """Normal contact solve (bindings.cpp:186-234); always FP64 by default.
 
         ``precision`` (keyword-only extension): 'double' (reference),
@@ -419,6 +432,13 @@ class ContactSolver:
         'float_then_double' (FP32 to float_tol (default tol), then an FP64
         polish that certifies polish_tol (default tol); see
         solve_device_mixed).
+
+        ``reference_fp64`` (keyword-only, for 'float' / 'float_then_double'):
+        also run the plain FP64 solve of the same problem (same tol,
+        preconditioner and warm start) and state the result's accuracy
+        against it in ``pressure_rel_l2_vs_fp64`` (||p - p64|| / ||p64||),
+        ``contact_area_error_vs_fp64`` (|A - A64|) and ``fp64_status``;
+        without it those fields are None.
         """
         N = self.Ns * self.Ns
         if precond not in ("none", "", "fourier", "fourier-fft"):
@@ -437,6 +457,14 @@ class ContactSolver:
         else:
             raise ValueError("precision must be 'double', 'float' or 'float_then_double'")
         r.wall = time.perf_counter() - t0
+        if reference_fp64 and precision != "double":
+            rd = solve_device(self.op, g0d, p_nominal, tol, max_iter, use_pr, precond, p0,
+                              torch.float64, light=True)
+            pd = rd.pressure_device
+            r.pressure_rel_l2_vs_fp64 = float(torch.linalg.norm(r.pressure_device - pd) /
+                                              torch.linalg.norm(pd))
+            r.contact_area_error_vs_fp64 = abs(r.contact_area - rd.contact_area)
+            r.fp64_status = rd.status
         return r
 
     def hmatrix_info(self):

@@ -40,16 +40,19 @@ const char* aspher_last_error(void) { return asb::g_last_error.c_str(); }
 
 int64_t aspher_launch_count(void) { return (int64_t)asb::launch_count(); }
 
-int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
-                     aspher_op** out) {
+int aspher_op_create_ex(int backend, int grid_size, double domain_size, double E_star,
+                        int flags, aspher_op** out) {
     ASB_API_BEGIN
     if (!out) throw asb::Error(ASPHER_EINVAL, "aspher_op_create: out is NULL");
     *out = nullptr;
     if (backend != ASPHER_BACKEND_FFT && backend != ASPHER_BACKEND_PERIODIC)
         throw asb::Error(ASPHER_EINVAL, "unknown backend (expected fft or periodic)");
+    static_assert(ASPHER_OPF_SPLIT_COLUMNS == asb::OPF_SPLIT_COLUMNS &&
+                      ASPHER_OPF_SPLIT_KH == asb::OPF_SPLIT_KH,
+                  "flag values of the ABI and the operator agree");
     auto* op = new aspher_op{nullptr};
     try {
-        op->impl = new asb::Operator(backend, grid_size, domain_size, E_star);
+        op->impl = new asb::Operator(backend, grid_size, domain_size, E_star, flags);
     } catch (...) {
         delete op;
         throw;
@@ -57,6 +60,11 @@ int aspher_op_create(int backend, int grid_size, double domain_size, double E_st
     *out = op;
     return ASPHER_OK;
     ASB_API_END
+}
+
+int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
+                     aspher_op** out) {
+    return aspher_op_create_ex(backend, grid_size, domain_size, E_star, 0, out);
 }
 
 int aspher_op_destroy(aspher_op* op) {

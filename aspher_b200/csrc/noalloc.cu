@@ -15,11 +15,19 @@
 // Limits and contract:
 //   - grid_size is a power of two in [16, kNoAllocMaxNs] (1024); larger grids
 //     are rejected (the static scratch is sized for 1024: (512+16) x 1024
-//     double2 = 8.65 MB, held by every GPU that loads this library until the
-//     process exits; the FP32 path uses the same array);
-//   - the first call on a device sets that device up (symbol addresses and the
-//     twiddle tables, filled by a kernel); make that first call before any
-//     stream capture;
+//     double2 = 8.65 MB; the FP32 path uses the same array);
+//   - the 8.65 MB are device memory of this file's module: with CUDA's lazy
+//     module loading (the default since CUDA 12.2) the driver allocates them
+//     when the module is first used on a device, i.e. in the first call on
+//     that device, and holds them until the process exits.  A host whose
+//     allocator reserves the GPU's memory up front should make the first
+//     call before it reserves its pool (or run with CUDA_MODULE_LOADING=EAGER,
+//     which loads the module with the library);
+//   - the first call on a device sets that device up (symbol addresses, the
+//     twiddle tables filled by a kernel on the caller's stream, the kernels'
+//     shared-memory attributes per precision and size on their first use);
+//     make that first call before any stream capture;
+//   - `stream` must belong to the current device;
 //   - every call shares the one scratch array, which keeps the last call's
 //     contents: calls that overlap on the GPU (different streams, or
 //     different host threads without ordering) race on it.  Nothing in the
@@ -28,6 +36,7 @@
 #include "functors.cuh"
 #include "ops.hpp"
 
+#include <atomic>
 #include <cmath>
 #include <mutex>
 
@@ -47,6 +56,8 @@ struct NaDevice {
     void* spec = nullptr;
     double2* twd = nullptr;
     float2* twf = nullptr;
+    // kernel attributes set, one bit per (precision, log2 grid_size)
+    std::atomic<unsigned> attrs{0};
 };
 NaDevice g_na[64];
 std::mutex g_na_mu;
@@ -84,48 +95,68 @@ NaDevice& na_setup(cudaStream_t s) {
     return d;
 }
 
-void na_attrs(const void* func, int bytes) {
+void na_attr(const void* func, int bytes) {
     if (bytes > 48 * 1024)
         ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
 }
 
-// One periodic apply with launch variant 0 (the same kernels and layout as
-// the operator path), the static scratch and the static twiddles.
+// The three kernels of one periodic apply with launch variant 0 (the same
+// kernels and layout as the operator path).
 template <typename T, int NS>
-void na_apply(const NaDevice& d, double scale, const T* x, T* y, cudaStream_t s) {
-    constexpr int LR = NS / 2, LC = NS, V = 0;
+struct NaKernels {
+    static constexpr int LR = NS / 2, LC = NS, V = 0;
+    static constexpr auto fwd = row_fwd_kernel<T, LR, false, V, LoadRealRows<T>, StoreTiled<T>>;
+    static constexpr auto col = col_kernel<T, LC, LR, false, V, PeriodicMult<T>>;
+    static constexpr auto inv = row_inv_kernel<T, LR, false, V, LoadTiled<T>, StoreRealRows<T>>;
+    static constexpr int sm_fwd = row_fwd_smem<T, LR, false, V, LoadRealRows<T>>();
+    static constexpr int sm_col = col_smem_total<T, LC, LR, false, V>();
+    static constexpr int sm_inv = row_inv_smem<T, LR, false, V, LoadTiled<T>>();
+    // their shared-memory attributes, set once per device, precision and size
+    static void prepare(NaDevice& d) {
+        const unsigned bit = 1u << ((sizeof(T) == 8 ? 16 : 0) + ilog2c(NS));
+        if (d.attrs.load(std::memory_order_acquire) & bit) return;
+        std::lock_guard<std::mutex> lk(g_na_mu);
+        if (d.attrs.load(std::memory_order_relaxed) & bit) return;
+        na_attr((const void*)fwd, sm_fwd);
+        na_attr((const void*)col, sm_col);
+        na_attr((const void*)inv, sm_inv);
+        d.attrs.fetch_or(bit, std::memory_order_release);
+    }
+};
+
+// One periodic apply: the static scratch and the static twiddles.
+template <typename T, int NS>
+void na_apply(NaDevice& d, double scale, const T* x, T* y, cudaStream_t s) {
+    using K = NaKernels<T, NS>;
+    constexpr int LR = K::LR, LC = K::LC, V = K::V;
     constexpr int ct = col_ct_v<T>(LC, LR, V);
+    K::prepare(d);
     const cplx<T>* tw = reinterpret_cast<const cplx<T>*>(
         sizeof(T) == 8 ? (const void*)d.twd : (const void*)d.twf);
     cplx<T>* spec = static_cast<cplx<T>*>(d.spec);
     {
         constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-        constexpr int sm = row_fwd_smem<T, LR, false, V, LoadRealRows<T>>();
-        auto k = row_fwd_kernel<T, LR, false, V, LoadRealRows<T>, StoreTiled<T>>;
-        na_attrs((const void*)k, sm);
-        k<<<(NS + rb - 1) / rb, thr, sm, s>>>(LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, ct},
-                                              NS, tw + LR, tw + 2 * LR, nullptr);
+        K::fwd<<<(NS + rb - 1) / rb, thr, K::sm_fwd, s>>>(
+            LoadRealRows<T>{x, NS}, StoreTiled<T>{spec, NS, ct}, NS, tw + LR, tw + 2 * LR,
+            nullptr);
     }
     {
-        constexpr int thr = col_threads<T>(LC, LR, V), sm = col_smem_total<T, LC, LR, false, V>();
-        auto k = col_kernel<T, LC, LR, false, V, PeriodicMult<T>>;
-        na_attrs((const void*)k, sm);
-        k<<<LR / ct + 1, thr, sm, s>>>(spec, NS, PeriodicMult<T>{scale, NS}, tw + LC, nullptr);
+        constexpr int thr = col_threads<T>(LC, LR, V);
+        K::col<<<LR / ct + 1, thr, K::sm_col, s>>>(spec, NS, PeriodicMult<T>{scale, NS}, tw + LC,
+                                                   nullptr);
     }
     {
         constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-        constexpr int sm = row_inv_smem<T, LR, false, V, LoadTiled<T>>();
-        auto k = row_inv_kernel<T, LR, false, V, LoadTiled<T>, StoreRealRows<T>>;
-        na_attrs((const void*)k, sm);
-        k<<<(NS + rb - 1) / rb, thr, sm, s>>>(LoadTiled<T>{spec, NS, ct}, StoreRealRows<T>{y, NS},
-                                              NS, tw + LR, tw + 2 * LR, nullptr);
+        K::inv<<<(NS + rb - 1) / rb, thr, K::sm_inv, s>>>(
+            LoadTiled<T>{spec, NS, ct}, StoreRealRows<T>{y, NS}, NS, tw + LR, tw + 2 * LR,
+            nullptr);
     }
     count_launches(3);
     ASB_CUDA(cudaGetLastError());
 }
 
 template <typename T>
-void na_dispatch(int Ns, const NaDevice& d, double scale, const T* x, T* y, cudaStream_t s) {
+void na_dispatch(int Ns, NaDevice& d, double scale, const T* x, T* y, cudaStream_t s) {
     switch (Ns) {
         case 16: na_apply<T, 16>(d, scale, x, y, s); break;
         case 32: na_apply<T, 32>(d, scale, x, y, s); break;
@@ -158,17 +189,17 @@ extern "C" int aspher_periodic_matvec_noalloc(int grid_size, double domain_size,
         if (((uintptr_t)x_dev | (uintptr_t)y_dev) % 16)
             throw asb::Error(ASPHER_EINVAL,
                              "aspher_periodic_matvec_noalloc: buffers must be 16-byte aligned");
+        if (dtype != ASPHER_F64 && dtype != ASPHER_F32)
+            throw asb::Error(ASPHER_EINVAL, "aspher_periodic_matvec_noalloc: dtype must be F32 or F64");
         cudaStream_t s = static_cast<cudaStream_t>(stream);
-        const asb::NaDevice& d = asb::na_setup(s);
+        asb::NaDevice& d = asb::na_setup(s);
         // same symbol scale as PeriodicFFTOperator (periodic_fft_operator.cpp:11-24)
         const double scale =
             domain_size / (M_PI * E_star * (double)grid_size * (double)grid_size);
         if (dtype == ASPHER_F64)
             asb::na_dispatch<double>(grid_size, d, scale, (const double*)x_dev, (double*)y_dev, s);
-        else if (dtype == ASPHER_F32)
-            asb::na_dispatch<float>(grid_size, d, scale, (const float*)x_dev, (float*)y_dev, s);
         else
-            throw asb::Error(ASPHER_EINVAL, "aspher_periodic_matvec_noalloc: dtype must be F32 or F64");
+            asb::na_dispatch<float>(grid_size, d, scale, (const float*)x_dev, (float*)y_dev, s);
         return ASPHER_OK;
     } catch (const asb::Error& e) {
         asb::set_last_error(e.what());

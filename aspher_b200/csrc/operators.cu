@@ -18,7 +18,6 @@
 #include "functors.cuh"
 #include "ops.hpp"
 #include "pcg.hpp"
-#include "pk_fused.cuh"
 #include "reduce.cuh"
 
 #include <atomic>
@@ -629,13 +628,12 @@ struct FourierImpl {
 template <int NS>
 struct KhBuild {
     // the split form (see StoreSplitCombine) where the FP64 row does not fit
-    // one CTA, or where ASPHER_SPLIT_KH=1 asks for it (cross-checks), for
-    // Ns >= kSplitMin
+    // one CTA, or where the operator's creation flags ask for it
+    // (cross-checks), for Ns >= kSplitMin
     static constexpr bool kRowFits = row_smem_v<double>(NS, 0) <= kSmemPerSM;
-    static bool split() {
+    static bool split(const Operator& op) {
         if (!kRowFits) return true;
-        const char* e = std::getenv("ASPHER_SPLIT_KH");
-        return NS >= kSplitMin && e && std::atoi(e) != 0;
+        return NS >= kSplitMin && op.split_kh;
     }
     static void run(Operator& op) {
         constexpr int LR = NS, M = 2 * NS;
@@ -650,7 +648,7 @@ struct KhBuild {
         StoreRealTracked sb{nullptr, M, op.kh_canon, nullptr, NS + 1, 0, 0,
                             1.0 / ((double)M * (double)M), mx + 2, 0.0, 0.0};
         const LoadEmbedded emb{op.table, NS, M};
-        if (split()) {
+        if (split(op)) {
             if constexpr (NS >= kSplitMin) {
                 constexpr int LH = NS / 2;  // real length Ns per parity
                 double2* E = nullptr;
@@ -734,7 +732,7 @@ __global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
         default: throw Error(-1, "grid_size must be a power of two in [16, 16384]"); \
     }
 
-Operator::Operator(int kind_, int Ns_, double L_, double E_)
+Operator::Operator(int kind_, int Ns_, double L_, double E_, int flags)
     : kind(kind_), Ns(Ns_), L(L_), E_star(E_) {
     if (kind != OP_FFT && kind != OP_PERIODIC) throw Error(-1, "unknown operator kind");
     if (!is_pow2(Ns) || Ns < 16 || Ns > kMaxNs)
@@ -744,13 +742,12 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_)
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ASB_CUDA(cudaGetDevice(&device));
     (void)tw_table(false, 2);
-    {
-        // ASPHER_SPLIT_COLUMNS=1: the free-space column pass in its split
-        // (two half-length) form at every size >= kSplitMin, the form that
-        // FP64 at Ns = 8192 needs (for cross-checks against the one-CTA form)
-        const char* e = std::getenv("ASPHER_SPLIT_COLUMNS");
-        split_cols = kind == OP_FFT && Ns >= kSplitMin && e && std::atoi(e) != 0;
-    }
+    if (flags & ~(OPF_SPLIT_COLUMNS | OPF_SPLIT_KH)) throw Error(-1, "unknown operator flags");
+    // cross-check forms: the free-space column pass in its split (two
+    // half-length) form and the FP64 Kh build from even / odd row samples at
+    // every size >= kSplitMin, the forms FP64 at Ns = 8192 and 16384 need
+    split_cols = kind == OP_FFT && Ns >= kSplitMin && (flags & OPF_SPLIT_COLUMNS);
+    split_kh = kind == OP_FFT && Ns >= kSplitMin && (flags & OPF_SPLIT_KH);
     if (kind == OP_PERIODIC) {
         scale = L / (M_PI * E_star * (double)Ns * Ns);
     } else {
@@ -979,40 +976,5 @@ template void fourier_precond_pk<float>(Operator&, const float*, const uint8_t*,
                                         double*, cudaStream_t, const int*, int, void*);
 template void fourier_precond_pk<double>(Operator&, const double*, const uint8_t*, PkState*,
                                          double*, double*, cudaStream_t, const int*, int, void*);
-
-// r = S t inside the PK loop with the direction update in the forward row
-// load and the rsum / den sums in the inverse row store (pk_fused.cuh)
-template <typename T, int NS>
-struct FusedTApply {
-    static void run(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
-                    const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
-                    const int* gate, int B, void* spec_b) {
-        cplx<T>* spec = static_cast<cplx<T>*>(spec_b ? spec_b : op.spectrum(sizeof(T) == 8, s));
-        const long bx = (long)NS * NS;
-        LoadTupd<T> ld{z, g, gprev, t, mask, p, best, st, NS, precond, bx};
-        StoreRden<T> sr{g, t, mask, st, part, NS, bx, 0.0, 0.0, 0.0, 0.0};
-        if (op.kind == OP_FFT) {
-            FreeImpl<T, NS>::apply(op, ld, sr, spec, s, gate, B);
-        } else {
-            const int dbl = sizeof(T) == 8;
-            PeriodicImpl<T, NS>::apply(op.rowv[dbl], op.colv[dbl], ld,
-                                       PeriodicMult<T>{op.scale, NS}, sr, spec, s, gate, B);
-        }
-    }
-};
-
-template <typename T>
-void pk_apply_t(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
-                const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
-                const int* gate, int B, void* spec) {
-    ASB_SIZE_SWITCH(op.Ns, FusedTApply<T, NS>::run(op, z, g, gprev, t, mask, p, best, st, part,
-                                                   precond, s, gate, B, spec));
-}
-template void pk_apply_t<float>(Operator&, const float*, const float*, float*, float*,
-                                const uint8_t*, const float*, float*, PkState*, double*, int,
-                                cudaStream_t, const int*, int, void*);
-template void pk_apply_t<double>(Operator&, const double*, const double*, double*, double*,
-                                 const uint8_t*, const double*, double*, PkState*, double*, int,
-                                 cudaStream_t, const int*, int, void*);
 
 }  // namespace asb

@@ -52,6 +52,8 @@ tw(int L) {
 }
 
 enum OpKind : int { OP_FFT = 0, OP_PERIODIC = 1 };
+// operator creation flags (aspher_op_create_ex): cross-check forms
+enum OpFlags : int { OPF_SPLIT_COLUMNS = 1, OPF_SPLIT_KH = 2 };
 
 // smallest grid with the split free-space column pass (two length-Ns halves
 // of the length-2Ns column; required for FP64 at Ns = 8192)
@@ -93,8 +95,12 @@ struct Operator {
     // (half-spectrum layout) they imply
     int rowv[2] = {0, 0}, colv[2] = {0, 0}, ct[2] = {0, 0};
     // free space: the column pass as two half-length transforms even where
-    // the full column fits one CTA (set from ASPHER_SPLIT_COLUMNS at creation)
+    // the full column fits one CTA (creation flag ASPHER_OPF_SPLIT_COLUMNS,
+    // for cross-checks of the form Ns = 8192 FP64 needs)
     bool split_cols = false;
+    // free space: the FP64 Kh build from even / odd row samples even where a
+    // row fits one CTA (creation flag ASPHER_OPF_SPLIT_KH, for cross-checks)
+    bool split_kh = false;
     // periodic: symbol scale L / (pi E* Ns^2)
     double scale = 0.0;
     // scratch half spectra per precision (lazily sized)
@@ -106,7 +112,7 @@ struct Operator {
     // solver contexts per precision (workspace + loop graph), built lazily
     std::shared_ptr<SolverCtxBase> ctx_f, ctx_d;
 
-    Operator(int kind, int Ns, double L, double E_star);
+    Operator(int kind, int Ns, double L, double E_star, int flags = 0);
     ~Operator();
     Operator(const Operator&) = delete;
     Operator& operator=(const Operator&) = delete;

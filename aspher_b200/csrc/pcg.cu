@@ -16,7 +16,6 @@
 #include "ops.hpp"
 #include "pk_state.hpp"
 #include "pcg.hpp"
-#include "pk_fused.cuh"
 #include "reduce.cuh"
 
 #include <algorithm>
@@ -89,6 +88,35 @@ __device__ __forceinline__ void stm4(uint8_t* m, long i4, const uint8_t (&a)[4])
 // so centring costs no pass of its own.
 template <typename T>
 __device__ __forceinline__ T gc(T v, T aT) { return v - aT; }
+
+__device__ __forceinline__ void set_halt(PkState* st, int h) {
+    st->halt = h;
+    st->skip_mv1 = 1;
+}
+
+// Scalar tail of the rsum / den pass (thread 0 of the last block).
+// acc = {sum_C r, sum_C g t, sum_C r t, sum_C t};
+// den = sum_C Real(r - rm) t, linear in rm: sum_C r t - rm sum_C t.
+template <typename T>
+__device__ inline void rden_tail(PkState* st, const double (&acc)[4]) {
+    st->mv++;
+    if (st->copy_best) {
+        st->copy_best = 0;
+        st->have_best = 1;
+    }
+    st->rsum = acc[0];
+    st->num = acc[1];
+    st->rmean = (double)(T)(st->nc ? acc[0] / st->nc : 0.0);
+    const double den = acc[2] - st->rmean * acc[3], num = acc[1];
+    st->den = den;
+    if (den > 0.0 && isfinite(den) && isfinite(num)) {
+        const T tau = (T)(num / den);
+        st->tau = (double)tau;
+        st->tau_ov = st->gg > 0.0 ? (double)(T)(num * num / (den * st->gg)) : (double)tau;
+    } else {
+        set_halt(st, H_IDENT);  // no usable direction: identification step
+    }
+}
 
 // One pass for evaluate() (contact_solver.cpp:263-303): v -> g buffer, the
 // contact mask, and the sums whose last-block logic is the certificate, the
@@ -680,8 +708,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_dots(const PkPar
 }
 
 // Direction update t = chi_C(z_f + beta t), g_prev = g (and best = p when
-// copy_best) before the t apply; k_rden consumes r after it.  pk_apply_t is
-// the same pair fused into the apply's row kernels (ASPHER_FUSED_T=1).
+// copy_best) before the t apply; k_rden consumes r after it.
 template <typename T>
 __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_tupd(const PkParams* __restrict__ Pp, PkState* st, const T* z,
                                                       const T* g, T* gprev, T* t,
@@ -1038,14 +1065,7 @@ int red_grid(long N) {
 
 // The FP64 polish stage of a mixed solve runs its loop applies
 // defect-corrected (Operator::matvec_defect: FP32 transforms of p - p0 and of
-// t around one exact FP64 apply of p0); ASPHER_POLISH_EXACT=1 keeps them FP64.
-static bool polish_defect() {
-    static const bool d = [] {
-        const char* v = std::getenv("ASPHER_POLISH_EXACT");
-        return !(v && v[0] == '1');
-    }();
-    return d;
-}
+// t around one exact FP64 apply of p0).
 
 // Per-operator, per-precision solver context: the CG workspace of up to
 // `cap` instances (fields back to back), the device parameter and state
@@ -1256,15 +1276,10 @@ struct SolverCtx : SolverCtxBase {
             k_dots<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, mask, part);
             ++n;
         }
-        if (fused_t() && !defect) {
-            pk_apply_t<T>(op, z, g, gprev, t, mask, p, best, st, part, precond, s, &st->halt, B,
-                          B > 1 ? spec : nullptr);
-        } else {
-            k_tupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
-            apply_r(s, B);
-            k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
-            n += 2;
-        }
+        k_tupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, z, g, gprev, t, mask, p, best);
+        apply_r(s, B);
+        k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
+        n += 2;
         k_pupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
         k_rescale<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, part);
         count_launches(n + 2);
@@ -1347,27 +1362,6 @@ struct SolverCtx : SolverCtxBase {
     void launch_graph(cudaStream_t s, int lo, int n) {
         ASB_CUDA(cudaGraphLaunch(graphs.at(std::make_tuple((int)defect, lo, n)).exec, s));
         count_launches(1);
-    }
-    // ASPHER_EAGER_LOOP=1: enqueue iterations as plain launches instead of the
-    // loop graph (same kernels, same gating; for per-kernel profilers)
-    static bool eager_loop() {
-        static const bool e = [] {
-            const char* v = std::getenv("ASPHER_EAGER_LOOP");
-            return v && v[0] == '1';
-        }();
-        return e;
-    }
-    // ASPHER_FUSED_T=1: the direction update and the r sums inside the row
-    // kernels of the t apply (pk_apply_t) instead of two streaming passes
-    // around a plain apply.  Off by default: the row kernels are latency-bound
-    // and the extra loads in them cost more than the passes they save
-    // (measured on B200 at Ns=2048: 1-2 % slower per solve).
-    static bool fused_t() {
-        static const bool e = [] {
-            const char* v = std::getenv("ASPHER_FUSED_T");
-            return v && v[0] == '1';
-        }();
-        return e;
     }
 };
 
@@ -1630,7 +1624,7 @@ struct Solver {
                 for (int b = 0; b < B; ++b) ih[b].mv_host += 1;
             }
         }
-        if (!SolverCtx<T>::eager_loop()) c.ensure_graph(s, 0, B);
+        c.ensure_graph(s, 0, B);
         write_states();
 
         // ---- the loop: device-driven, the host services rare branches
@@ -1640,25 +1634,21 @@ struct Solver {
             return false;
         };
         while (any_running()) {
-            if (SolverCtx<T>::eager_loop()) {
-                for (int k = 0; k < 8; ++k) c.enqueue_iteration(s, B);
-            } else {
-                // the loop graph of the smallest instance range that covers
-                // every running instance: halted instances outside it launch
-                // no (gated) blocks
-                int lo = -1, hi = -1;
-                for (int b = 0; b < B; ++b)
-                    if (h[b].halt == H_RUN) {
-                        if (lo < 0) lo = b;
-                        hi = b;
-                    }
-                const int n = hi - lo + 1;
-                if (!c.has_graph(lo, n)) {
-                    c.ensure_graph(s, lo, n);  // clobbers st[lo, lo + n)
-                    write_states();
+            // the loop graph of the smallest instance range that covers
+            // every running instance: halted instances outside it launch
+            // no (gated) blocks
+            int lo = -1, hi = -1;
+            for (int b = 0; b < B; ++b)
+                if (h[b].halt == H_RUN) {
+                    if (lo < 0) lo = b;
+                    hi = b;
                 }
-                c.launch_graph(s, lo, n);
+            const int n = hi - lo + 1;
+            if (!c.has_graph(lo, n)) {
+                c.ensure_graph(s, lo, n);  // clobbers st[lo, lo + n)
+                write_states();
             }
+            c.launch_graph(s, lo, n);
             read_states();
             bool changed = false;
             for (int b = 0; b < B; ++b) {
@@ -1896,7 +1886,7 @@ void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double
     Solver<T> S(get_ctx<T>(op), s);
     const T* g = (const T*)g0;
     const T* pi = (const T*)p_init;
-    const bool defect = sizeof(T) == 8 && polish_stage && p_init && polish_defect();
+    const bool defect = sizeof(T) == 8 && polish_stage && p_init;
     S.run(o, &g, &p_bar, &pi, &pressure, disp, gap, hist, hist_cap, &res, nullptr, nullptr,
           defect);
 }
@@ -2004,7 +1994,7 @@ void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, dou
         Solver<double> S(cd, s);
         const double* pw = pressure;
         S.run(od, &g0, &p_bar, &pw, &pressure, disp, gap, nullptr, 0, &res, datum.data(),
-              gref.data(), polish_defect());
+              gref.data(), true);
     }
     add_stage(res, rf);
 }
@@ -2064,7 +2054,7 @@ void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const do
         Solver<double> S(cd, s, B);
         std::vector<const double*> pw(pressures, pressures + B);
         S.run(od, g0s, p_bars, pw.data(), pressures, nullptr, nullptr, nullptr, 0, res,
-              datum.data(), gref.data(), polish_defect());
+              datum.data(), gref.data(), true);
     }
     for (int b = 0; b < B; ++b) add_stage(res[b], rf[b]);
 }

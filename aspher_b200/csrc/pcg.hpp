@@ -30,15 +30,6 @@ void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* 
                         double* part, cudaStream_t s, const int* gate, int B = 1,
                         void* spec = nullptr);
 
-// r = S t of the PK loop with the direction update t = chi_C(z_f + beta t)
-// (and g_prev = g, best = p when copy_best) fused into the forward row load
-// and the rsum / num / den sums of r fused into the inverse row store; r is
-// not written.  Defined in operators.cu (functors in pk_fused.cuh).
-template <typename T>
-void pk_apply_t(Operator& op, const T* z, const T* g, T* gprev, T* t, const uint8_t* mask,
-                const T* p, T* best, PkState* st, double* part, int precond, cudaStream_t s,
-                const int* gate, int B = 1, void* spec = nullptr);
-
 // polish_stage: the solve refines p_init (the FP64 stage of a mixed or
 // nested float_then_double solve); its loop applies may then be
 // defect-corrected (see Operator::matvec_defect)

@@ -77,6 +77,18 @@ typedef struct aspher_op aspher_op;
  * applies and solves exist (FP64 ones return ASPHER_EINVAL). */
 int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
                      aspher_op** out);
+/* The same with creation flags (the survey's aspher_op_create(kind, Ns, L,
+ * Estar, flags, ...)): ASPHER_OPF_SPLIT_COLUMNS computes the free-space
+ * column pass as two half-length transforms and ASPHER_OPF_SPLIT_KH builds
+ * the FP64 kernel spectrum from even / odd row samples at every grid_size
+ * >= 256 -- the forms that FP64 at 8192 and 16384 need, selectable at
+ * smaller sizes so that they can be checked against the one-CTA forms.
+ * Results equal aspher_op_create's to rounding; flags = 0 is
+ * aspher_op_create.  Unknown flag bits return ASPHER_EINVAL. */
+#define ASPHER_OPF_SPLIT_COLUMNS 1
+#define ASPHER_OPF_SPLIT_KH 2
+int aspher_op_create_ex(int backend, int grid_size, double domain_size, double E_star,
+                        int flags, aspher_op** out);
 int aspher_op_destroy(aspher_op* op);
 
 /* y = S x over Ns*Ns values of `dtype` (F64: FFTOperator::matvec_into,
@@ -274,11 +286,15 @@ int aspher_adjoint(aspher_op* op, int dtype, const double* p_dev, const double* 
  * allocator owns all GPU memory.  Same
  * result as aspher_op_matvec on a PERIODIC operator of the same grid_size,
  * domain_size and E_star, without an operator handle: the scratch is a
- * static 8.65 MB device array (held by every GPU that loads the library)
- * and grid_size must be a power of two in [16, 1024]; larger sizes return
- * ASPHER_EINVAL.  The first call on a device sets it up (make it before any
- * stream capture).  All calls share the scratch: calls that overlap on the
- * GPU race.  x_dev and y_dev must not alias.  Async on `stream`. */
+ * static 8.65 MB device array and grid_size must be a power of two in
+ * [16, 1024]; larger sizes return ASPHER_EINVAL.  With CUDA's lazy module
+ * loading (the default since CUDA 12.2) the 8.65 MB are allocated by the
+ * driver in the first call on each device and held until the process exits:
+ * make that first call before a host allocator reserves the GPU's memory, or
+ * set CUDA_MODULE_LOADING=EAGER.  The first call on a device also sets it up
+ * (make it before any stream capture).  `stream` must belong to the current
+ * device.  All calls share the scratch: calls that overlap on the GPU race.
+ * x_dev and y_dev must not alias.  Async on `stream`. */
 int aspher_periodic_matvec_noalloc(int grid_size, double domain_size, double E_star, int dtype,
                                    const void* x_dev, void* y_dev, void* stream);
 

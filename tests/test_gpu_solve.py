@@ -183,3 +183,23 @@ def test_polish_reaches_fp64_certificates(backend):
     assert r.status == "converged", (r.status, r.status_reason)
     assert r.fw_error <= 1e-10 and r.penetration_error <= 1e-10
     assert rel(r.pressure, ref.pressure) <= 1e-8
+
+
+@pytest.mark.parametrize("precision", ["float", "float_then_double"])
+def test_mixed_result_states_its_accuracy_vs_fp64(precision):
+    """solve(..., reference_fp64=True) runs the plain FP64 solve beside the
+    float / float_then_double one and reports the pressure rel-L2 and the
+    contact-area error against it; without the flag the fields are None."""
+    Ns, pbar, tol = 256, 0.005, 1e-6
+    g0 = _rough(Ns)
+    s = _solver(Ns, "fft")
+    r = s.solve(g0, pbar, tol, precond="fourier", precision=precision, reference_fp64=True)
+    rd = s.solve(g0, pbar, tol, precond="fourier")
+    assert r.status == "converged" and r.fp64_status == rd.status == "converged"
+    assert r.pressure_rel_l2_vs_fp64 == pytest.approx(rel(r.pressure, rd.pressure), rel=1e-6,
+                                                      abs=1e-12)
+    assert r.contact_area_error_vs_fp64 == pytest.approx(abs(r.contact_area - rd.contact_area),
+                                                         abs=1e-12)
+    assert r.pressure_rel_l2_vs_fp64 <= 1e-4 and r.contact_area_error_vs_fp64 <= 1e-4
+    plain = s.solve(g0, pbar, tol, precond="fourier", precision=precision)
+    assert plain.pressure_rel_l2_vs_fp64 is None and plain.contact_area_error_vs_fp64 is None

@@ -3,18 +3,16 @@
 The zero-padded free-space column of length 2 Ns is transformed as two
 length-Ns halves (even and odd frequencies).  That is the only form an FP64
 column of 16384 points can take (it does not fit one CTA's shared memory), so
-FP64 applies at Ns = 8192 and FP32 applies at Ns = 16384 use it;
-ASPHER_SPLIT_COLUMNS=1 forces it at smaller sizes, where it is checked
+FP64 applies at Ns = 8192 and FP32 applies at Ns = 16384 use it; the
+operator creation flag SPLIT_COLUMNS forces it at smaller sizes, where it is checked
 against the oracle and against the one-CTA column pass.  The FP64 Kh build
 likewise assembles rows of 2 Ns reals from the transforms of their even and
-odd samples where a row does not fit (Ns = 16384); ASPHER_SPLIT_KH=1 forces
+odd samples where a row does not fit (Ns = 16384); the flag SPLIT_KH forces
 that form for the cross-check.  Applies at the large sizes are checked
 through point loads, whose response is the Love table itself (the aperiodic
 convolution of a unit load at a corner cell), through exact periodic Fourier
 modes, against the other precision, and for symmetry.
 """
-
-import os
 
 import numpy as np
 import pytest
@@ -26,15 +24,9 @@ from oracle.operators import FFTOperator as OFFT  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 
-def _op(Ns, split=False, env="ASPHER_SPLIT_COLUMNS", backend="fft"):
+def _op(Ns, split=False, flag="SPLIT_COLUMNS", backend="fft"):
     from aspher_b200 import Operator
-    if not split:
-        return Operator(backend, Ns)
-    os.environ[env] = "1"
-    try:
-        return Operator(backend, Ns)
-    finally:
-        del os.environ[env]
+    return Operator(backend, Ns, flags=getattr(Operator, flag) if split else 0)
 
 
 def _mv(op, x, dtype):
@@ -121,7 +113,7 @@ def test_fp64_solve_runs_at_8192():
 
 @pytest.mark.parametrize("Ns", [256, 1024])
 def test_split_kh_build_matches_one_cta_build(Ns):
-    opk, op = _op(Ns, split=True, env="ASPHER_SPLIT_KH"), _op(Ns)
+    opk, op = _op(Ns, split=True, flag="SPLIT_KH"), _op(Ns)
     assert opk.info().max_im_ratio < 1e-10
     x = np.random.default_rng(13).standard_normal(Ns * Ns)
     y = _mv(op, x, torch.float64)
