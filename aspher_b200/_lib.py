@@ -88,6 +88,21 @@ class AdjointInfo(C.Structure):
                 ("time", C.c_double)]
 
 
+class Problem(C.Structure):
+    _fields_ = [("backend", C.c_int), ("grid_size", C.c_int), ("domain_size", C.c_double),
+                ("E_star", C.c_double), ("g0_dev", C.c_void_p), ("p_bar", C.c_double),
+                ("pressure_dev", C.c_void_p)]
+
+
+class ManyOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("tol", C.c_double), ("float_tol", C.c_double),
+                ("polish_tol", C.c_double), ("max_iter", C.c_int), ("precond", C.c_int),
+                ("precond_radius", C.c_int), ("concurrent", C.c_int)]
+
+
+MANY_PRECISION = {"double": 0, "float": 1, "float_then_double": 2}
+
+
 # exported symbol -> (restype, argtypes)
 SIGNATURES = {
     "aspher_abi_version": (C.c_int, []),
@@ -128,6 +143,9 @@ SIGNATURES = {
                                            C.POINTER(C.c_void_p), C.POINTER(C.c_double),
                                            C.c_double, C.c_int, C.POINTER(C.c_void_p),
                                            C.POINTER(Result), C.POINTER(Result), C.c_void_p]),
+    "aspher_many_opts_default": (None, [C.POINTER(ManyOpts)]),
+    "aspher_solve_many": (C.c_int, [C.c_int, C.POINTER(Problem), C.POINTER(ManyOpts),
+                                    C.POINTER(Result), C.POINTER(Result), C.c_void_p]),
     "aspher_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_double,
                                  C.c_int, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double),
                                  C.POINTER(AdjointInfo), C.c_void_p]),

@@ -1,23 +1,25 @@
 """Many independent solves of uneven grid sizes and backends.
 
-No reference counterpart (the reference solves one problem per call).  The
-problems are grouped by (backend, grid size); each group is one batched
-solve on one operator (``aspher_solve_batch_mixed``: every kernel of the
-loop launched once for the whole group, one CUDA-graph loop, per-instance
-convergence masks), and the groups run concurrently, one host thread and
-one CUDA stream each, so the small grids fill the SMs the large ones leave
+No reference counterpart (the reference solves one problem per call).
+``solve_many`` is one call of the library's ``aspher_solve_many``, which
+groups the problems by operator (backend, grid size); each group is one
+batched solve on one operator (every kernel of the loop launched once for
+the whole group, one CUDA-graph loop, per-instance convergence masks), and
+the groups run concurrently, one host thread and one CUDA stream each
+inside the library, so the small grids fill the SMs the large ones leave
 idle.  Across GPUs the problems are dealt out by a greedy
 longest-processing-time partition of their estimated cost (no collective:
 each rank solves its own problems).
 """
 
-import concurrent.futures as cf
+import ctypes as C
 import math
 
 import numpy as np
 import torch
 
-from .api import Operator, solve_device_batch, solve_device_batch_mixed
+from . import _lib as L
+from .api import ContactResult, Operator, _stream
 from .surfaces import self_affine_gap
 
 
@@ -82,73 +84,54 @@ class Operators:
 
 def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max_iter=5000,
                precision="float_then_double", concurrent=True, operators=None,
-               device=None, float_tol=None):
+               device=None, float_tol=None, domain_size=1.0, E_star=1.0):
     """Solve ``problems`` (dicts with backend, grid_size, p_nominal) with the
-    matching ``gaps`` (device tensors or arrays of Ns^2 FP64 values).
-    Returns the ContactResults in problem order (pressures on the device).
-    Work recorded on the caller's current stream afterwards runs after every
-    group (so CUDA events on that stream bracket the whole batch)."""
+    matching ``gaps`` (device tensors or arrays of Ns^2 FP64 values) in one
+    library call (``aspher_solve_many``): the library groups them per
+    operator, solves each group as one batched solve and runs the groups
+    concurrently on its own streams and host threads.  Returns the
+    ContactResults in problem order (pressures on the device).  Work recorded
+    on the caller's current stream afterwards runs after every group (so CUDA
+    events on that stream bracket the whole batch).  ``operators`` is kept
+    for signature compatibility: the library caches its operators itself."""
+    del operators
     if len(problems) != len(gaps):
         raise ValueError("solve_many: one gap per problem")
-    if precision not in ("double", "float", "float_then_double"):
+    if precision not in L.MANY_PRECISION:
         raise ValueError("precision must be 'double', 'float' or 'float_then_double'")
+    if precond not in L.PRECOND:
+        raise ValueError("precond must be 'none', 'fourier' or 'fourier-fft'")
+    n = len(problems)
+    if n == 0:
+        return []
     dev = torch.device(device) if device is not None else torch.device(
         "cuda", torch.cuda.current_device())
-    ops = operators or Operators()
-    groups = {}
+    arr = (L.Problem * n)()
+    ins, outs = [], []
     for i, pr in enumerate(problems):
-        groups.setdefault((pr["backend"], int(pr["grid_size"])), []).append(i)
-    # Everything that allocates or copies is done here, before any worker
-    # starts: the operators, the groups' streams, gaps and outputs.  The
-    # workers then only run the library's batched solves (which serialise
-    # their own graph captures and set-up against each other).
-    caller = torch.cuda.current_stream(dev)
-    streams, inputs, outputs = {}, {}, {}
-    for key, idx in groups.items():
-        ops.get(*key)
-        streams[key] = torch.cuda.Stream(device=dev)
-        inputs[key] = [torch.as_tensor(gaps[i], dtype=torch.float64).to(dev).reshape(-1)
-                       for i in idx]
-        N = key[1] * key[1]
-        outputs[key] = [torch.empty(N, dtype=torch.float64, device=dev) for _ in idx]
-    torch.cuda.synchronize(dev)
-    results = [None] * len(problems)
-    done = []
-
-    def run_group(key):
-        b, Ns = key
-        idx = groups[key]
-        op = ops.get(b, Ns)
-        stream = streams[key]
-        stream.wait_stream(caller)
-        with torch.cuda.device(dev), torch.cuda.stream(stream):
-            g = inputs[key]
-            pn = [problems[i]["p_nominal"] for i in idx]
-            if precision == "double":
-                rs = solve_device_batch(op, g, pn, tol=tol, max_iter=max_iter, precond=precond,
-                                        dtype=torch.float64, keep_best=False,
-                                        pressures_out=outputs[key])
-            else:
-                rs, _ = solve_device_batch_mixed(op, g, pn, tol=tol, float_tol=float_tol,
-                                                 max_iter=max_iter,
-                                                 precond=precond, keep_best=False,
-                                                 polish=precision == "float_then_double",
-                                                 polish_tol=polish_tol,
-                                                 pressures_out=outputs[key])
-            ev = torch.cuda.Event()
-            ev.record(stream)
-            done.append(ev)
-        for i, r in zip(idx, rs):
-            results[i] = r
-
-    keys = sorted(groups, key=lambda k: -len(groups[k]) * solve_cost(k[0], k[1]))
-    if concurrent and len(keys) > 1:
-        with cf.ThreadPoolExecutor(len(keys)) as ex:
-            for f in [ex.submit(run_group, k) for k in keys]:
-                f.result()
-    else:
-        for k in keys:
-            run_group(k)
-    for ev in done:
-        caller.wait_event(ev)
-    return results
+        if pr["backend"] not in L.BACKEND:
+            raise ValueError("unknown backend: %s" % pr["backend"])
+        Ns = int(pr["grid_size"])
+        g = torch.as_tensor(gaps[i], dtype=torch.float64).to(dev).reshape(-1).contiguous()
+        if g.numel() != Ns * Ns:
+            raise ValueError("solve_many: problem %d: gap has %d entries, expected %d"
+                             % (i, g.numel(), Ns * Ns))
+        out = torch.empty(Ns * Ns, dtype=torch.float64, device=dev)
+        ins.append(g)
+        outs.append(out)
+        arr[i] = L.Problem(L.BACKEND[pr["backend"]], Ns, float(pr.get("domain_size", domain_size)),
+                           float(pr.get("E_star", E_star)), g.data_ptr(),
+                           float(pr["p_nominal"]), out.data_ptr())
+    o = L.ManyOpts()
+    L.lib().aspher_many_opts_default(C.byref(o))
+    o.precision = L.MANY_PRECISION[precision]
+    o.tol = float(tol)
+    o.float_tol = float(float_tol or 0.0)
+    o.polish_tol = float(polish_tol or 0.0)
+    o.max_iter = int(max_iter)
+    o.precond = L.PRECOND[precond]
+    o.concurrent = int(bool(concurrent))
+    res, resf = (L.Result * n)(), (L.Result * n)()
+    with torch.cuda.device(dev):
+        L.check(L.lib().aspher_solve_many(n, arr, C.byref(o), res, resf, _stream()))
+    return [ContactResult(res[i], int(problems[i]["grid_size"]), outs[i]) for i in range(n)]

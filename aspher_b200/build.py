@@ -11,6 +11,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -35,9 +36,13 @@ def _compile(src, verbose=False):
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(src), hdr):
         return obj, ""
     cmd = [NVCC] + ARCH + FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
+    t0 = time.time()
     p = subprocess.run(cmd, capture_output=True, text=True)
     if p.returncode != 0:
         raise RuntimeError("nvcc failed for %s:\n%s" % (src, p.stderr))
+    # date the object at the start of its compile: a source or header edited
+    # while it compiled is newer than it, so the next build recompiles
+    os.utime(obj, (t0, t0))
     return obj, p.stderr
 
 
@@ -53,7 +58,8 @@ def build(verbose=False, jobs=None):
             if log:
                 sys.stderr.write(log)
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart"]
+        cmd = [NVCC] + ARCH + ["-shared", "-o", OUT] + objs + ["-lcudart",
+                                                              "-Xlinker", "--no-undefined"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError("link failed:\n" + p.stderr)

@@ -234,7 +234,8 @@ __host__ __device__ constexpr int col_smem_total() {
 // ---- row forward ---------------------------------------------------------------
 // Load:  cplx<T> operator()(int row, int n) -> z[n] = (x[2n], x[2n+1]);
 //        static constexpr bool kRaw: true when x / pitch / bs expose plain
-//        contiguous rows (then the kernel stages them with cp.async)
+//        contiguous rows (then the kernel stages them with cp.async and
+//        passes each staged pair through ld.fix())
 // Store: void operator()(int row, int k, cplx<T> X), k in [0, LR]
 //        static constexpr bool kTiled: true for the tiled half-spectrum store
 //        (then the kernel writes whole tile chunks through base / nrows / ct /
@@ -365,7 +366,7 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
 #pragma unroll
             for (int m = 0; m < RPT; ++m) {
                 if (PAD && m >= RPT / 2) v[m] = mk<T>(0, 0);
-                else v[m] = valid ? srow[t + m * TT] : mk<T>(0, 0);
+                else v[m] = valid ? ld.fix(srow[t + m * TT]) : mk<T>(0, 0);
             }
             __syncthreads();
             if (grp + (int)gridDim.x < ngroups) issue(grp + gridDim.x);

@@ -8,16 +8,34 @@ namespace asb {
 
 // Every functor offsets by blockIdx.y * bs (elements): instance blockIdx.y
 // of a batched launch (bs = 0 or gridDim.y = 1 for a single field).
+// The PK loop's pressure with the pending load rescale of instance
+// blockIdx.y (PkState::scale / scale_add): Real(x f) + a.
+template <typename T>
+__device__ __forceinline__ T pending_scale(const PkState* sc, T x) {
+    const PkState* sb = sc + blockIdx.y;
+    return x * (T)__ldg(&sb->scale) + (T)__ldg(&sb->scale_add);
+}
+
 template <typename T>
 struct LoadRealRows {  // z[n] = (x[row*pitch + 2n], x[row*pitch + 2n + 1])
     const T* x;
     int pitch;
     long bs;
+    // optional: x is the PK loop's pressure, scaled by the pending load
+    // rescale of sc[blockIdx.y] as it is loaded
+    const PkState* sc = nullptr;
     static constexpr bool kTiled = false;
     static constexpr bool kRaw = true;  // plain rows: the row kernel may stage them
+    __device__ __forceinline__ cplx<T> fix(cplx<T> v) const {
+        if (sc) {
+            v.x = pending_scale(sc, v.x);
+            v.y = pending_scale(sc, v.y);
+        }
+        return v;
+    }
     __device__ __forceinline__ cplx<T> operator()(int row, int n) const {
-        return *reinterpret_cast<const cplx<T>*>(x + blockIdx.y * bs + (size_t)row * pitch +
-                                                  2 * n);
+        return fix(*reinterpret_cast<const cplx<T>*>(x + blockIdx.y * bs + (size_t)row * pitch +
+                                                      2 * n));
     }
 };
 
@@ -44,9 +62,16 @@ struct LoadDiffRows {
     const double* x0;
     int pitch;
     long bs;
+    // optional: x is the PK loop's pressure with a pending load rescale
+    // (see LoadRealRows)
+    const PkState* sc = nullptr;
     __device__ __forceinline__ cplx<float> operator()(int row, int n) const {
         const size_t i = blockIdx.y * bs + (size_t)row * pitch + 2 * n;
         double2 v = *reinterpret_cast<const double2*>(x + i);
+        if (sc) {
+            v.x = pending_scale(sc, v.x);
+            v.y = pending_scale(sc, v.y);
+        }
         if (x0) {
             const double2 w = *reinterpret_cast<const double2*>(x0 + i);
             v.x -= w.x;

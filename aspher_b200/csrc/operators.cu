@@ -497,9 +497,9 @@ struct FreeImpl {
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
-                       const int* gate, int B) {
+                       const int* gate, int B, const PkState* sc) {
         const long bx = (long)NS * NS;
-        apply(op, LoadRealRows<T>{x, NS, bx}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
+        apply(op, LoadRealRows<T>{x, NS, bx, sc}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
     }
 };
 
@@ -532,10 +532,10 @@ struct PeriodicImpl {
     }
 
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
-                       const int* gate, int B) {
+                       const int* gate, int B, const PkState* sc) {
         const int dbl = sizeof(T) == 8;
         const long bx = (long)NS * NS;
-        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS, bx},
+        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS, bx, sc},
               PeriodicMult<T>{op.scale, NS}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
     }
 };
@@ -925,7 +925,7 @@ bool Operator::supports(bool dbl) const {
 }
 
 void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate, int B,
-                      void* spec_b) {
+                      void* spec_b, const PkState* sc) {
     if (!supports(dbl))
         throw Error(-1, "FP64 applies are not supported above grid_size 8192 (an FP64 row or "
                         "column of 16384 points does not fit one CTA's shared memory); use FP32");
@@ -933,35 +933,36 @@ void Operator::matvec(bool dbl, const void* x, void* y, cudaStream_t s, const in
     if (kind == OP_FFT) {
         if (dbl) {
             ASB_SIZE_SWITCH(Ns, FreeImpl<double, NS>::matvec(*this, (const double*)x, (double*)y,
-                                                             (double2*)spec, s, gate, B));
+                                                             (double2*)spec, s, gate, B, sc));
         } else {
             ASB_SIZE_SWITCH(Ns, FreeImpl<float, NS>::matvec(*this, (const float*)x, (float*)y,
-                                                            (float2*)spec, s, gate, B));
+                                                            (float2*)spec, s, gate, B, sc));
         }
     } else {
         if (dbl) {
             ASB_SIZE_SWITCH(Ns, PeriodicImpl<double, NS>::matvec(*this, (const double*)x,
                                                                  (double*)y, (double2*)spec, s,
-                                                                 gate, B));
+                                                                 gate, B, sc));
         } else {
             ASB_SIZE_SWITCH(Ns, PeriodicImpl<float, NS>::matvec(*this, (const float*)x,
                                                                 (float*)y, (float2*)spec, s,
-                                                                gate, B));
+                                                                gate, B, sc));
         }
     }
 }
 
 void Operator::matvec_defect(const double* x, const double* x0, double* y, const double* y0,
-                             cudaStream_t s, const int* gate, int B, void* spec_b) {
+                             cudaStream_t s, const int* gate, int B, void* spec_b,
+                             const PkState* sc) {
     void* spec = spec_b ? spec_b : spectrum(false, s);
     const long bx = (long)Ns * Ns;
     if (kind == OP_FFT) {
-        ASB_SIZE_SWITCH(Ns, FreeImpl<float, NS>::apply(*this, LoadDiffRows{x, x0, NS, bx},
+        ASB_SIZE_SWITCH(Ns, FreeImpl<float, NS>::apply(*this, LoadDiffRows{x, x0, NS, bx, sc},
                                                        StoreAddRows{y, y0, NS, bx},
                                                        (float2*)spec, s, gate, B));
     } else {
         ASB_SIZE_SWITCH(Ns, PeriodicImpl<float, NS>::apply(
-                                rowv[0], colv[0], LoadDiffRows{x, x0, NS, bx},
+                                rowv[0], colv[0], LoadDiffRows{x, x0, NS, bx, sc},
                                 PeriodicMult<float>{scale, NS}, StoreAddRows{y, y0, NS, bx},
                                 (float2*)spec, s, gate, B));
     }

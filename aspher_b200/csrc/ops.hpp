@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include "pk_state.hpp"
+
 #include <cstddef>
 #include <cstdint>
 #include <memory>
@@ -122,8 +124,10 @@ struct Operator {
     // Batched (B > 1): x, y hold B fields back to back, spec_b a spectrum
     // scratch of B * spectrum_bytes(dbl), and gate[b * kGateStride] gates
     // instance b.
+    // sc (optional): x is a PK loop's pressure with a pending load rescale in
+    // sc[b] (PkState::scale / scale_add), applied as x is loaded.
     void matvec(bool dbl, const void* x, void* y, cudaStream_t s, const int* gate = nullptr,
-                int B = 1, void* spec_b = nullptr);
+                int B = 1, void* spec_b = nullptr, const PkState* sc = nullptr);
     // Defect-corrected FP64 apply: y = y0 + S_32(x - x0) with x, x0, y, y0
     // FP64 fields (x0, y0 optional) and the transform in FP32.  With
     // y0 = S x0 exact, the result carries the FP32 rounding of S only on the
@@ -131,7 +135,7 @@ struct Operator {
     // Batched as matvec (spec_b: B * spectrum_bytes(false) at least).
     void matvec_defect(const double* x, const double* x0, double* y, const double* y0,
                        cudaStream_t s, const int* gate = nullptr, int B = 1,
-                       void* spec_b = nullptr);
+                       void* spec_b = nullptr, const PkState* sc = nullptr);
     void* spectrum(bool dbl, cudaStream_t s);
     int col_tile(bool dbl, int cv) const;
     void set_variants(bool dbl, int rv, int cv);

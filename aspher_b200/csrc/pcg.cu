@@ -6,7 +6,7 @@
 // double}; every reduction is accumulated in FP64 as in the reference.
 //
 // One CG iteration is the kernel sequence
-//   [apply p->u] eval [evalpk] stencil+dots tupd [apply t->r] rden pupd rescale
+//   [apply p->u] eval [evalpk] stencil+dots tupd [apply t->r] rden pupd
 // where each pass is one HBM sweep and each reduction's scalar logic runs in
 // the last block of its pass (see pk_state.hpp).  The loop is a CUDA graph
 // with a while node; once a pass sets `halt`, the rest of the iteration is a
@@ -118,6 +118,16 @@ __device__ inline void rden_tail(PkState* st, const double (&acc)[4]) {
     }
 }
 
+// The pending load rescale of an instance (PkState::scale / scale_add),
+// read once at kernel entry: the iterate is Real(x f) + a of the stored x
+// (bit-identical to the reference's p(i) *= f, where a = 0).
+template <typename T>
+struct PScale {
+    T f, a;
+    __device__ explicit PScale(const PkState* st) : f((T)st->scale), a((T)st->scale_add) {}
+    __device__ __forceinline__ T operator()(T x) const { return x * f + a; }
+};
+
 // One pass for evaluate() (contact_solver.cpp:263-303): v -> g buffer, the
 // contact mask, and the sums whose last-block logic is the certificate, the
 // convergence test and the best/stall bookkeeping (contact_solver.cpp:379-412).
@@ -146,6 +156,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_eval(const PkPar
     const PkParams& P = *Pp;
     if (!final_mode && st->halt) return;
     const T gs = (T)P.gshift;
+    const PScale<T> ps(st);
     double acc[5] = {0.0, 0.0, (double)INFINITY, 0.0, 0.0};  // sum_C v, n_C, min v, pv, psum
     GRID_LOOP4(P.N) {
         T uu[4], gg0[4], pp[4], vv[4];
@@ -153,6 +164,8 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_eval(const PkPar
         ldp4(u, i4, uu);
         ldp4(g0, i4, gg0);
         ldp4(p, i4, pp);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) pp[j] = ps(pp[j]);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const T v = uu[j] + (gg0[j] - gs);
@@ -247,13 +260,14 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_evalpk(const PkP
     const PkParams& P = *Pp;
     if (!final_mode && !st->pk_due) return;
     const T aT = (T)st->alpha;
+    const PScale<T> ps(st);
     double acc[1] = {0.0};
     GRID_LOOP4(P.N) {
         T pp[4], gv[4];
         ldp4(p, i4, pp);
         ldp4(g, i4, gv);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[0] += (double)pp[j] * fabs((double)gc(gv[j], aT));
+        for (int j = 0; j < 4; ++j) acc[0] += (double)ps(pp[j]) * fabs((double)gc(gv[j], aT));
     }
     const int kinds[1] = {0};
     if (grid_reduce_last<1>(acc, kinds, part, &st->counter[12]) && threadIdx.x == 0) {
@@ -728,6 +742,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_tupd(const PkPar
     if (st->halt) return;
     const T zm = (T)st->zmean, beta = (T)st->beta, aT = (T)st->alpha;
     const int cb = st->copy_best;
+    const PScale<T> ps(st);
     GRID_LOOP4(P.N) {
         T zz[4], gv[4], tt[4];
         uint8_t mm[4];
@@ -745,6 +760,8 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_tupd(const PkPar
         if (cb) {
             T pp[4];
             ldp4(p, i4, pp);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) pp[j] = ps(pp[j]);
             st4(best, i4, pp);
         }
     }
@@ -803,6 +820,9 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_pupd(const PkPar
     const PkParams& P = *Pp;
     if (st->halt) return;
     const T tau = (T)st->tau, tov = (T)st->tau_ov, aT = (T)st->alpha;
+    // every block reads the pending rescale here, before it arrives at the
+    // last-block counter; only the last block's tail rewrites it
+    const PScale<T> ps(st);
     double acc[2] = {0, 0};  // changed (max), total
     GRID_LOOP4(P.N) {
         T pp[4], tt[4], gv[4];
@@ -811,7 +831,7 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_pupd(const PkPar
         ldp4(g, i4, gv);
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            T pi = pp[j];
+            T pi = ps(pp[j]);
             const T gi = gc(gv[j], aT);
             const bool was = pi > T(0);
             if (was) {
@@ -829,40 +849,51 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_pupd(const PkPar
     if (grid_reduce_last<2>(acc, kinds, part, &st->counter[6]) && threadIdx.x == 0) {
         st->delta = acc[0] > 0.0 ? 0.0 : 1.0;
         st->total = acc[1];
+        // the load rescale (contact_solver.cpp:489-500), pending until the
+        // next consumer of p forms it
         if (acc[1] > 0.0) {
             st->scale = (double)(T)(P.P_total / acc[1]);
+            st->scale_add = 0.0;
             st->fill = 0;
-        } else {
+        } else {  // every p is 0: p = p_bar
+            st->scale = 1.0;
+            st->scale_add = (double)(T)P.p_bar;
             st->fill = 1;
         }
+        st->it++;
+        if (st->it >= P.max_iter) set_halt(st, H_FINAL);  // status stays max_iterations
     }
 }
 
+// The pending load rescale applied to the stored pressure of every instance
+// of the launch (before the host reads p), leaving scale 1 and fill 0.
+// Reads the state of all blocks before the last block resets it.
 template <typename T>
-__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_rescale(const PkParams* __restrict__ Pp, PkState* st, T* p,
-                                                         double* part) {
-    // instance blockIdx.y of a batched solve (0 when unbatched)
+__global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_materialize(
+    const PkParams* __restrict__ Pp, PkState* st, T* p, double* part) {
     Pp += blockIdx.y;
     st += blockIdx.y;
     part += (size_t)blockIdx.y * kPartStride;
     const long bo_ = (long)blockIdx.y * Pp->N;
     p += bo_;
     const PkParams& P = *Pp;
-    if (st->halt) return;
-    const int fill = st->fill;
-    const T f = (T)st->scale, pb = (T)P.p_bar;
-    GRID_LOOP4(P.N) {
-        T pp[4];
-        ldp4(p, i4, pp);
+    const PScale<T> ps(st);
+    const bool identity = ps.f == T(1) && ps.a == T(0);
+    if (!identity) {
+        GRID_LOOP4(P.N) {
+            T pp[4];
+            ldp4(p, i4, pp);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) pp[j] = fill ? pb : pp[j] * f;
-        st4(p, i4, pp);
+            for (int j = 0; j < 4; ++j) pp[j] = ps(pp[j]);
+            st4(p, i4, pp);
+        }
     }
     double acc[1] = {0};
     const int kinds[1] = {0};
     if (grid_reduce_last<1>(acc, kinds, part, &st->counter[7]) && threadIdx.x == 0) {
-        st->it++;
-        if (st->it >= P.max_iter) set_halt(st, H_FINAL);  // status stays max_iterations
+        st->scale = 1.0;
+        st->scale_add = 0.0;
+        st->fill = 0;
     }
 }
 
@@ -1229,22 +1260,25 @@ struct SolverCtx : SolverCtxBase {
     T* at(T* v, int b) const { return v + (size_t)b * N; }
 
     // B instances: gates per instance, spectrum of the batch when B > 1
-    void apply(const T* x, T* y, const int* gate, cudaStream_t s, int B) {
-        op.matvec(sizeof(T) == 8, x, y, s, gate, B, B > 1 ? spec : nullptr);
+    void apply(const T* x, T* y, const int* gate, cudaStream_t s, int B,
+               const PkState* sc = nullptr) {
+        op.matvec(sizeof(T) == 8, x, y, s, gate, B, B > 1 ? spec : nullptr, sc);
     }
     // one CG iteration of B instances (the common path), every pass gated
     // per instance on the device:
     //   [apply p->u] eval (evalpk) | stencil+dots  or  [precond] dots |
-    //   tupd [apply t->r] rden | pupd rescale
+    //   tupd [apply t->r] rden | pupd (load rescale pending, formed by the
+    //   next consumers of p)
     // the loop's two applies: u = S p (gated by skip_mv1) and r = S t
     void apply_u(cudaStream_t s, int B) {
         if constexpr (sizeof(T) == 8) {
             if (defect) {
-                op.matvec_defect(p, p0, u, u0, s, &st->skip_mv1, B, B > 1 ? spec : nullptr);
+                op.matvec_defect(p, p0, u, u0, s, &st->skip_mv1, B, B > 1 ? spec : nullptr, st);
                 return;
             }
         }
-        apply(p, u, &st->skip_mv1, s, B);
+        // p carries its pending load rescale (formed as it is loaded)
+        apply(p, u, &st->skip_mv1, s, B, st);
     }
     void apply_r(cudaStream_t s, int B) {
         if constexpr (sizeof(T) == 8) {
@@ -1281,8 +1315,7 @@ struct SolverCtx : SolverCtxBase {
         k_rden<T><<<gr, kRedThreads, 0, s>>>(Pd, st, r, g, t, mask, part);
         n += 2;
         k_pupd<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, t, g, part);
-        k_rescale<T><<<gr, kRedThreads, 0, s>>>(Pd, st, p, part);
-        count_launches(n + 2);
+        count_launches(n + 1);
         ASB_CUDA(cudaGetLastError());
     }
     // g <- centred gap for instance b (or all B when b < 0)
@@ -1605,6 +1638,7 @@ struct Solver {
         for (int b = 0; b < B; ++b) {
             PkState& H = h[b];
             std::memset(&H, 0, sizeof(H));
+            H.scale = 1.0;  // no load rescale pending
             H.G_old = 1.0;
             H.delta = 0.0;
             H.best_merit = std::numeric_limits<double>::infinity();
@@ -1649,6 +1683,10 @@ struct Solver {
                 write_states();
             }
             c.launch_graph(s, lo, n);
+            // the host takes over: form the pending load rescale of p
+            k_materialize<T><<<dim3(c.grid, n), kRedThreads, 0, s>>>(
+                c.Pd + lo, c.st + lo, c.at(c.p, lo), c.part + (size_t)lo * kPartStride);
+            count_launches(1);
             read_states();
             bool changed = false;
             for (int b = 0; b < B; ++b) {

@@ -59,6 +59,9 @@ void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const do
                        double* const* pressures, aspher_result* res, aspher_result* res_float,
                        cudaStream_t s);
 
+void solve_many(int n, const aspher_problem* problems, const aspher_many_opts& o,
+                aspher_result* res, aspher_result* res_float, cudaStream_t s);
+
 template <typename T>
 void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
                   int precond, int radius, double* grad_g0, double* grad_pbar,

@@ -61,14 +61,22 @@ struct PkState {
     int stall, forced_id;
     int copy_best, have_best;
     int status;
-    int fill;  // total <= 0 -> p = p_bar
+    int fill;  // total <= 0: the pressure is p_bar everywhere (pending, see scale)
     int pk_due;  // k_eval ran; k_evalpk records this iteration's pk
     double best_merit, seen_merit;
     // CG recurrences
     double G_old, delta, beta, gg, bv;  // bv: PR+ / FR ratio before the delta gate
     double zmean;  // preconditioner output contact mean
     double rsum, num, rmean, den, tau, tau_ov;
-    double total, scale;
+    double total;
+    // the load rescale p <- p P / sum p (contact_solver.cpp:491-497) is
+    // applied lazily: the iterate is Real(x * scale) + scale_add of the
+    // stored x, every consumer in the loop forms it (bit-identical to the
+    // reference's p(i) *= f: scale_add is 0 then), and the host materialises
+    // it whenever it takes over (scale 1, scale_add 0 afterwards).  The
+    // reference's p = p_bar fill (every p zero after the update) is scale 1,
+    // scale_add p_bar.
+    double scale, scale_add;
     // identification / helpers: generic reduction results
     double red[8];
     // last-block counters, one per kernel kind (reset by the last block)

@@ -24,7 +24,7 @@ data path.
 ``--impl reference`` times the reference's own CPU implementation of the
 same workload: its unmodified hot-path C++ built here with OpenMP
 (oracle/_ref, see oracle/ref.py) on every host core.  Each step samples the
-six problems with two bounded solves each (stopped after 3 and 9 PCG
+six problems with two bounded solves each (stopped after 4 and 16 PCG
 iterations); a whole solve is the fitted fixed part plus the per-iteration
 slope times the reference's own iteration count
 (tests/golden/ref_ns2048.json), and one complete solve of the cheapest
@@ -703,6 +703,41 @@ def adjoint_check(dev, Ns=1024, pbar=0.005, n_dirs=16, sig=1e-4):
         out[name]["median_rel_err_fd_gap"] = float(np.median(errs[name]))
         out[name]["max_err_rel_grad_norm"] = max(errn[name])
         out[name]["rel_err_fd_pnominal"] = abs(grads[name][1] - fdp) / abs(fdp)
+    # config 4's own directions: 64 unit-RMS white-noise gap directions
+    # (seeds 100..163), each differenced at three steps (1e-6, 1e-7, 1e-8 x
+    # rms): a step study instead of a filter.  At a smooth point the central
+    # difference converges to the adjoint as h shrinks (error O(h^2)); a
+    # white-noise step moves contact-boundary cells, where L(gap) has a kink,
+    # and the difference there carries O(1) error that shrinks with the
+    # number of moved cells.
+    steps = (1e-6, 1e-7, 1e-8)
+    gf = grads["f64"][0]
+    rnd = {"steps_x_rms": list(steps), "directions": n_dirs, "rel_err": [], "moved": []}
+    rng_w = np.random.default_rng(100)
+    for k in range(n_dirs):
+        d = torch.from_numpy(rng_w.standard_normal(N)).to(dev)
+        d /= torch.sqrt(torch.mean(d ** 2))
+        ad = float(torch.dot(gf, d))
+        errs_k, moved_k = [], []
+        for st_ in steps:
+            hh = st_ * rms
+            Lp, rp = L_of(g0 + hh * d, warm=p0)
+            Lm, rm = L_of(g0 - hh * d, warm=p0)
+            fd_ = (Lp - Lm) / (2 * hh)
+            errs_k.append(abs(ad - fd_) / max(abs(fd_), 1e-300))
+            moved_k.append(int(((rp.pressure_device > 0) != c0).sum()) +
+                           int(((rm.pressure_device > 0) != c0).sum()))
+        rnd["rel_err"].append(errs_k)
+        rnd["moved"].append(moved_k)
+    ea = np.asarray(rnd["rel_err"])
+    ma = np.asarray(rnd["moved"])
+    rnd["median_rel_err_per_step"] = [float(np.median(ea[:, j])) for j in range(len(steps))]
+    rnd["n_within_1e-4_per_step"] = [int((ea[:, j] <= 1e-4).sum()) for j in range(len(steps))]
+    rnd["n_no_moved_cells_per_step"] = [int((ma[:, j] == 0).sum()) for j in range(len(steps))]
+    rnd["max_rel_err_no_moved_cells_per_step"] = [
+        float(ea[ma[:, j] == 0, j].max()) if (ma[:, j] == 0).any() else None
+        for j in range(len(steps))]
+    out["random_directions"] = rnd
     out["f64_adjoint_vs_fd_pairs"] = pairs
     out["fd_directions"] = n_dirs
     out["fd_same_contact_set"] = len(keep)
@@ -753,7 +788,7 @@ class CpuSampler:
     fixed + n slope; n is the reference's own iteration count of the
     problem."""
 
-    def __init__(self, n1=3, n2=9):
+    def __init__(self, n1=4, n2=16):
         from aspher_b200.surfaces import self_affine_gap
         self.n1, self.n2 = n1, n2
         make, self.kind, self.cores = _cpu_solver_factory()
@@ -805,6 +840,9 @@ def cpu_baseline(**_unused):
     10 s on 16 host threads)."""
     try:
         cs = CpuSampler()
+        for b in BACKENDS:  # warm-up: first-touch pages, FFT plan caches
+            cs.sample(b, LOADS[0])
+        cs.fits.clear()
         for b in BACKENDS:
             for p in LOADS:
                 cs.sample(b, p)

@@ -256,6 +256,60 @@ int aspher_solve_batch_mixed(aspher_op* op, const aspher_solve_opts* opts, int b
                              int polish, double* const* pressure_devs, aspher_result* res,
                              aspher_result* res_float, void* stream);
 
+/* ---- many problems of uneven size and backend ------------------------------ */
+/* One problem of aspher_solve_many: the survey's aspher_problem of the
+ * batch entry aspher_solve_batch(n, const aspher_problem*, aspher_result*,
+ * stream), whose one-operator form keeps that name above.  Buffers are the
+ * caller's: g0_dev (Ns*Ns FP64 gap) and pressure_dev (Ns*Ns FP64 output) on
+ * the current device, 16-byte aligned. */
+typedef struct {
+    int backend;           /* ASPHER_BACKEND_FFT / ASPHER_BACKEND_PERIODIC */
+    int grid_size;         /* power of two in [16, 16384] */
+    double domain_size;    /* <= 0: 1 */
+    double E_star;         /* <= 0: 1 */
+    const double* g0_dev;
+    double p_bar;
+    double* pressure_dev;
+} aspher_problem;
+
+enum aspher_many_precision {
+    ASPHER_MANY_DOUBLE = 0,           /* FP64 solves (the reference's) */
+    ASPHER_MANY_FLOAT = 1,            /* FP32 operator / CG, FP64 reductions */
+    ASPHER_MANY_FLOAT_THEN_DOUBLE = 2 /* FP32 to float_tol, FP64 polish to polish_tol */
+};
+
+/* Options shared by every problem of a call. */
+typedef struct {
+    int precision;        /* enum aspher_many_precision */
+    double tol;           /* requested certificate */
+    double float_tol;     /* FP32 stage target (<= 0: tol) */
+    double polish_tol;    /* FP64 polish certificate, in (0, tol] (<= 0: tol) */
+    int max_iter;         /* per stage (<= 0: 5000) */
+    int precond;          /* enum aspher_precond */
+    int precond_radius;   /* stencil radius (<= 0: 2) */
+    int concurrent;       /* groups run concurrently on their own streams */
+} aspher_many_opts;
+
+/* Fills the defaults: float_then_double, tol 1e-6, float_tol = polish_tol
+ * = tol, max_iter 5000, stencil preconditioner of radius 2, concurrent. */
+void aspher_many_opts_default(aspher_many_opts* o);
+
+/* n independent solves of any (backend, grid_size, domain_size, E_star) in
+ * one call.  No reference counterpart (the reference solves one problem per
+ * call).  The library groups the problems by operator (operators from the
+ * per-process cache of aspher_solve_nested), solves each group as one
+ * batched solve (aspher_solve_batch / aspher_solve_batch_mixed: one CUDA-
+ * graph loop, per-problem convergence masks), and runs the groups
+ * concurrently, longest first, each on its own stream of a per-device pool
+ * driven by its own host thread.  res[i] (and res_float[i], nullable: the
+ * FP32 stage alone) is problem i's result, the result aspher_solve_batch
+ * would give it (light: pressure only).  The groups wait for the caller's
+ * earlier work on `stream` and later work on `stream` waits for them.
+ * Invalid problems return ASPHER_EINVAL (the message names the problem)
+ * before any device work.  Synchronous. */
+int aspher_solve_many(int n, const aspher_problem* problems, const aspher_many_opts* opts,
+                      aspher_result* res, aspher_result* res_float, void* stream);
+
 /* ---- adjoint of a converged solve ------------------------------------------ */
 /* No reference counterpart (the reference has no derivative of the solve).
  * With C = {p > 0} the contact set of a converged solve of (op, g0, p_bar)

@@ -4,8 +4,8 @@ INFRASTRUCTURE ONLY.
 ``oracle/Makefile`` compiles the unmodified reference sources
 (``src/contact_solver.cpp``, ``src/fft_operator.cpp``,
 ``src/periodic_fft_operator.cpp``, ``src/boussinesq_kernel.cpp``,
-``src/stencil_precond.cpp``, ``src/fourier_precond.cpp``, with the vendored
-pocketfft and OpenMP) against the project's Eigen-API shim
+``src/stencil_precond.cpp``, ``src/fourier_precond.cpp``,
+``src/cerruti_kernel.cpp``, with the vendored pocketfft and OpenMP) against the project's Eigen-API shim
 (``oracle/eigen_shim``) and the C-ABI harness ``oracle/ref_harness.cpp`` into
 ``oracle/_ref/libaspher_ref.so``.  ``ContactSolver`` below mirrors the
 reference's pybind11 class (``python/bindings.cpp:115-214``) for the fft and
@@ -72,6 +72,12 @@ def lib():
         L.aref_project_simplex.restype = ctypes.c_double
         L.aref_project_simplex.argtypes = [_D, ctypes.c_int64, ctypes.c_double]
         L.aref_set_threads.argtypes = [ctypes.c_int]
+        L.aref_cerruti_tables.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_double, _D, _D, _D]
+        for f in (L.aref_cerruti_uxx, L.aref_cerruti_uxy):
+            f.restype = ctypes.c_double
+        L.aref_cerruti_uxx.argtypes = [ctypes.c_double] * 5
+        L.aref_cerruti_uxy.argtypes = [ctypes.c_double] * 4
         _lib = L
     return _lib
 
@@ -94,6 +100,25 @@ def project_load_simplex(y, P_total):
     y = np.ascontiguousarray(y, np.float64).copy()
     th = lib().aref_project_simplex(_dp(y), y.size, float(P_total))
     return y, th
+
+
+def cerruti_tables(Ns, L=1.0, E_star=1.0, nu=0.3):
+    """CerrutiKernel's signed offset tables (xx, yy, xy), each indexed
+    [dy + Ns - 1, dx + Ns - 1] for offsets in (-Ns, Ns)."""
+    W = 2 * Ns - 1
+    xx, yy, xy = (np.empty(W * W) for _ in range(3))
+    if lib().aref_cerruti_tables(int(Ns), float(L), float(E_star), float(nu), _dp(xx), _dp(yy),
+                                 _dp(xy)) != 0:
+        raise ValueError(lib().aref_last_error().decode())
+    return xx.reshape(W, W), yy.reshape(W, W), xy.reshape(W, W)
+
+
+def cerruti_uxx(x, y, a, b, nu):
+    return lib().aref_cerruti_uxx(float(x), float(y), float(a), float(b), float(nu))
+
+
+def cerruti_uxy(x, y, a, b):
+    return lib().aref_cerruti_uxy(float(x), float(y), float(a), float(b))
 
 
 _SCALARS = ("status", "iterations", "converged", "contact_fraction", "mean_pressure",

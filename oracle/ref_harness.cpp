@@ -4,7 +4,8 @@
 // sources, read in place from the reference tree (src/contact_solver.cpp,
 // src/fft_operator.cpp, src/periodic_fft_operator.cpp,
 // src/boussinesq_kernel.cpp, src/stencil_precond.cpp,
-// src/fourier_precond.cpp with the vendored pocketfft), against the
+// src/fourier_precond.cpp with the vendored pocketfft,
+// src/cerruti_kernel.cpp), against the
 // project's Eigen-API shim (oracle/eigen_shim), into oracle/_ref/
 // libaspher_ref.so.  Only tests/, __graft_entry__.smoke() and bench.py's
 // reference / CPU-baseline legs load it (oracle/ref.py), as the checker and
@@ -29,6 +30,7 @@
 #endif
 
 #include "boussinesq_kernel.hpp"
+#include "cerruti_kernel.hpp"
 #include "contact_solver.hpp"
 #include "fft_operator.hpp"
 #include "fourier_precond.hpp"
@@ -281,6 +283,36 @@ int aref_solve(void* h, int dtype, const double* g0, double p_bar, const double*
         g_err = e.what();
         return -1;
     }
+}
+
+// CerrutiKernel(Ns, L, E*, nu) (src/cerruti_kernel.cpp:114-128): the signed
+// offset tables xx_offset / xy_offset / yy_offset for offsets dx, dy in
+// (-Ns, Ns), written row-major as out[(dy + Ns - 1) * (2 Ns - 1) + dx + Ns - 1]
+int aref_cerruti_tables(int Ns, double L, double E_star, double nu, double* xx, double* yy,
+                        double* xy) {
+    try {
+        hmc::CerrutiKernel C(Ns, L, E_star, nu);
+        const int W = 2 * Ns - 1;
+        for (int dy = -(Ns - 1); dy < Ns; ++dy)
+            for (int dx = -(Ns - 1); dx < Ns; ++dx) {
+                const int64_t at = int64_t(dy + Ns - 1) * W + dx + Ns - 1;
+                xx[at] = C.xx_offset(dx, dy);
+                yy[at] = C.yy_offset(dx, dy);
+                xy[at] = C.xy_offset(dx, dy);
+            }
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+// The element-integrated Cerruti brackets (src/cerruti_kernel.cpp:64-112)
+double aref_cerruti_uxx(double x, double y, double a, double b, double nu) {
+    return hmc::cerruti_uxx(x, y, a, b, nu);
+}
+double aref_cerruti_uxy(double x, double y, double a, double b) {
+    return hmc::cerruti_uxy(x, y, a, b);
 }
 
 const char* aref_status_string(int s) { return hmc::to_string(static_cast<hmc::SolveStatus>(s)); }

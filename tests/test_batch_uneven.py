@@ -92,3 +92,55 @@ def test_solve_many_matches_single_solves():
         a, b = r.pressure.ravel(), r1.pressure.ravel()
         assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b)
         assert abs(r.contact_area - r1.contact_area) <= 1e-4
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["double", "float", "float_then_double"])
+def test_solve_many_c_abi_mixed_grid_sizes(precision):
+    """aspher_solve_many through the C ABI on problems of four grid sizes and
+    both backends (and two domain sizes): every problem certified, each
+    result equal to that problem's own solve of the same precision, the
+    serial and concurrent forms agree, and groups and problems come back in
+    input order."""
+    torch = pytest.importorskip("torch")
+    import aspher_b200 as asb
+    from aspher_b200.batch import problem_gap, solve_many
+    probs = uneven_problems(n=12, seed=11, sizes=(32, 64, 128, 256),
+                            weights=(0.25, 0.25, 0.25, 0.25))
+    probs[3]["domain_size"] = 2.0
+    gaps = [problem_gap(p) for p in probs]
+    tol = 1e-6 if precision != "double" else 1e-8
+    kw = dict(tol=tol, precision=precision)
+    rs = solve_many(probs, gaps, **kw)
+    rs_serial = solve_many(probs, gaps, concurrent=False, **kw)
+    torch.cuda.synchronize()
+    for i, (p, g, r, rz) in enumerate(zip(probs, gaps, rs, rs_serial)):
+        assert r.status == "converged", (i, p, r.status)
+        assert r.pressure.shape == (p["grid_size"], p["grid_size"])
+        op = asb.Operator(p["backend"], p["grid_size"], p.get("domain_size", 1.0))
+        gd = torch.as_tensor(g, device="cuda")
+        if precision == "double":
+            r1 = asb.solve_device(op, gd, p["p_nominal"], tol=tol, precond="fourier",
+                                  dtype=torch.float64, light=True, keep_best=False)
+        else:
+            r1, _ = asb.solve_device_mixed(op, gd, p["p_nominal"], tol=tol, precond="fourier",
+                                           polish=precision == "float_then_double",
+                                           light=True, keep_best=False)
+        a, b = r.pressure.ravel(), r1.pressure.ravel()
+        assert np.linalg.norm(a - b) <= 1e-9 * np.linalg.norm(b), (i, p)
+        assert np.array_equal(r.pressure, rz.pressure), i
+        assert r.iterations == r1.iterations == rz.iterations, i
+
+
+@pytest.mark.gpu
+def test_solve_many_rejects_bad_problems():
+    pytest.importorskip("torch")
+    from aspher_b200.batch import solve_many
+    probs = [dict(backend="fft", grid_size=64, p_nominal=0.01),
+             dict(backend="periodic", grid_size=64, p_nominal=0.01),
+             dict(backend="fft", grid_size=64, p_nominal=-1.0)]
+    gaps = [np.zeros(64 * 64)] * 3
+    with pytest.raises(ValueError, match="problem 2"):
+        solve_many(probs, gaps)
+    with pytest.raises(ValueError, match="polish_tol"):
+        solve_many(probs[:2], gaps[:2], tol=1e-6, polish_tol=1e-5)
