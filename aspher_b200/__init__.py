@@ -8,6 +8,7 @@ Public API (drop-in for the reference's fft / periodic backends):
 Lower level: Operator (device matvec), solve_device (device tensors in / out),
 solve_device_batch / solve_device_batch_mixed (many problems, one loop graph).
 Derivatives: adjoint(op, pressure, dL/dp), contact_pressure (torch.autograd).
+Tangential: TangentialOperator (the Cerruti block on the device).
 """
 
 from ._lib import AspherError, LIB_PATH  # noqa: F401
@@ -16,8 +17,9 @@ from .api import (ContactResult, ContactSolver, Operator, solve_device,  # noqa:
 from .adjoint import adjoint, contact_pressure  # noqa: F401
 from .nested import solve_nested  # noqa: F401
 from .surfaces import self_affine_gap  # noqa: F401
+from .tangential import TangentialOperator  # noqa: F401
 
 __all__ = ["ContactSolver", "ContactResult", "Operator", "solve_device", "solve_device_mixed",
            "solve_device_batch", "solve_device_batch_mixed",
            "solve_nested", "adjoint", "contact_pressure",
-           "stencil_taps", "self_affine_gap", "AspherError"]
+           "stencil_taps", "self_affine_gap", "AspherError", "TangentialOperator"]

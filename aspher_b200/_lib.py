@@ -38,7 +38,8 @@ class SolveOpts(C.Structure):
                 ("keep_best", C.c_int), ("load_tol", C.c_double), ("stall_limit", C.c_int),
                 ("allow_tolerance_relaxation", C.c_int), ("precond", C.c_int),
                 ("precond_radius", C.c_int), ("p_ref", C.c_double), ("g_ref", C.c_double),
-                ("datum_mode", C.c_int), ("datum", C.c_double), ("dtype", C.c_int)]
+                ("datum_mode", C.c_int), ("datum", C.c_double), ("dtype", C.c_int),
+                ("n_grid", C.c_int), ("loop_mode", C.c_int)]
 
 
 class Result(C.Structure):
@@ -103,6 +104,16 @@ class ManyOpts(C.Structure):
 MANY_PRECISION = {"double": 0, "float": 1, "float_then_double": 2}
 
 
+class TanResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("status_reason", C.c_char * 48), ("iterations", C.c_int),
+                ("converged", C.c_int), ("error", C.c_double), ("delta_t", C.c_double * 2),
+                ("q_mean", C.c_double * 2), ("n_stick", C.c_int), ("n_slip", C.c_int),
+                ("n_open", C.c_int), ("cone_violation", C.c_double),
+                ("stick_residual", C.c_double), ("slip_residual", C.c_double),
+                ("proj_residual", C.c_double), ("force_error", C.c_double), ("rho", C.c_double),
+                ("s_ref", C.c_double), ("w_ref", C.c_double), ("kkt_tol", C.c_double)]
+
+
 # exported symbol -> (restype, argtypes)
 SIGNATURES = {
     "aspher_abi_version": (C.c_int, []),
@@ -143,6 +154,16 @@ SIGNATURES = {
                                            C.POINTER(C.c_void_p), C.POINTER(C.c_double),
                                            C.c_double, C.c_int, C.POINTER(C.c_void_p),
                                            C.POINTER(Result), C.POINTER(Result), C.c_void_p]),
+    "aspher_tan_create": (C.c_int, [C.c_int, C.c_double, C.c_double, C.c_double,
+                                    C.POINTER(C.c_void_p)]),
+    "aspher_tan_destroy": (C.c_int, [C.c_void_p]),
+    "aspher_tan_matvec": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "aspher_tan_max_im_ratio": (C.c_int, [C.c_void_p, C.POINTER(C.c_double)]),
+    "aspher_solve_tangential": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                          C.c_double, C.c_double, C.c_int, C.c_int, C.c_double,
+                                          C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.POINTER(TanResult), C.c_void_p]),
+    "aspher_tan_tables": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "aspher_many_opts_default": (None, [C.POINTER(ManyOpts)]),
     "aspher_solve_many": (C.c_int, [C.c_int, C.POINTER(Problem), C.POINTER(ManyOpts),
                                     C.POINTER(Result), C.POINTER(Result), C.c_void_p]),

@@ -251,11 +251,14 @@ def solve_device(op, g0, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precon
                  p_init=None, dtype=torch.float64, light=False, record_history=False,
                  keep_best=None, requested_tol=0.0, allow_tolerance_relaxation=False,
                  g_ref=0.0, p_ref=0.0, datum_mode="automatic", datum=0.0, precond_radius=2,
-                 load_tol=0.0, stall_limit=200, pressure_out=None):
+                 load_tol=0.0, stall_limit=200, pressure_out=None, loop_mode="graph"):
     """solve_contact_impl<Real> on device tensors (Real = dtype).
 
     g0 / p_init: device tensors of ``dtype`` (Ns*Ns); the FP64 pressure is
     written to ``pressure_out`` (allocated when None) and stays on the device.
+    loop_mode: "graph" (the iterations in a CUDA-graph while loop) or
+    "eager" (the same kernels launched one by one, for per-kernel
+    profilers; same results, slower).
     """
     N = op.N
     if g0.numel() != N:
@@ -287,6 +290,7 @@ def solve_device(op, g0, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precon
     o.datum_mode = L.DATUM[datum_mode]
     o.datum = float(datum)
     o.dtype = L.F64 if dtype == torch.float64 else L.F32
+    o.loop_mode = _loop_mode(loop_mode)
     p_out = pressure_out if pressure_out is not None else torch.empty(N, dtype=torch.float64,
                                                                     device=dev)
     u_out = g_out = None
@@ -306,6 +310,12 @@ def solve_device(op, g0, p_nominal, tol=1e-8, max_iter=5000, use_pr=True, precon
         C.byref(res), _stream()))
     h = hist[:res.history_len].copy() if hist is not None else None
     return ContactResult(res, op.Ns, p_out, u_out, g_out, h)
+
+
+def _loop_mode(mode):
+    if mode not in ("graph", "eager"):
+        raise ValueError("loop_mode must be 'graph' or 'eager'")
+    return 0 if mode == "graph" else 1
 
 
 def _opts(tol, max_iter, use_pr, precond, keep_best, dtype, precond_radius=2, light=True):
@@ -483,7 +493,8 @@ class ContactSolver:
 def solve_device_mixed(op, g0, p_nominal, tol=1e-6, float_tol=None, polish=True,
                        max_iter=5000, use_pr=True, precond="fourier", p_init=None,
                        light=False, keep_best=None, g_ref=0.0, datum_mode="automatic",
-                       datum=0.0, precond_radius=2, pressure_out=None, polish_tol=None):
+                       datum=0.0, precond_radius=2, pressure_out=None, polish_tol=None,
+                       loop_mode="graph"):
     """FP32 PK solve with FP64 reductions to ``float_tol`` (default: tol),
     then (polish) an FP64 PK solve warm-started from it that certifies
     ``polish_tol`` (default: tol; must be <= tol): the reference's
@@ -519,6 +530,7 @@ def solve_device_mixed(op, g0, p_nominal, tol=1e-6, float_tol=None, polish=True,
     o.g_ref = float(g_ref)
     o.datum_mode = L.DATUM[datum_mode]
     o.datum = float(datum)
+    o.loop_mode = _loop_mode(loop_mode)
     p_out = pressure_out if pressure_out is not None else torch.empty(N, dtype=torch.float64,
                                                                     device=dev)
     u_out = g_out = None

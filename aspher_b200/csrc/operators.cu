@@ -15,7 +15,9 @@
 // scale/|m| (scale = L/(pi E* Ns^2), m = (kx, signed ky), zero mode 0) is
 // evaluated in FP64 inside the column kernel and cast to the working type.
 #include "fft_kernels.cuh"
+#include "fft_launch.cuh"
 #include "functors.cuh"
+#include "kernel_tables.cuh"
 #include "ops.hpp"
 #include "pcg.hpp"
 #include "reduce.cuh"
@@ -93,39 +95,6 @@ void smem_optin(const void* func, int bytes) {
 // ----------------------------------------------------------------------------
 // Love table (reference: src/boussinesq_kernel.cpp:44-106)
 // ----------------------------------------------------------------------------
-__device__ double asinh_diff_dev(double u, double v, double du) {
-    if (fabs(u) > 1e150 || fabs(v) > 1e150) return asinh(u) - asinh(v);
-    const double su = sqrt(1.0 + u * u), sv = sqrt(1.0 + v * v);
-    const double den = u * sv + v * su;
-    const double w = (u * v > 0.0 && den != 0.0) ? du * (u + v) / den : u * sv - v * su;
-    return asinh(w);
-}
-
-__device__ __forceinline__ double love_term(double t, double s1, double s2, double ds) {
-    if (t == 0.0) return 0.0;
-    const double c = fabs(t);
-    return t * asinh_diff_dev(s1 / c, s2 / c, ds / c);
-}
-
-__device__ double love_uz_dev(double x, double y, double a, double b) {
-    x = fabs(x);
-    y = fabs(y);
-    const double m = a > b ? a : b;
-    const double r2 = x * x + y * y;
-    const double sw = 1500.0 * m;
-    if (r2 > sw * sw) {
-        const double r = sqrt(r2);
-        const double A = 4.0 * a * b;
-        const double quad = (a * a * (3.0 * x * x - r2) + b * b * (3.0 * y * y - r2)) /
-                            (6.0 * r2 * r2);
-        return A * (1.0 + quad) / r;
-    }
-    const double xp = x + a, xm = x - a, yp = y + b, ym = y - b;
-    const double da = 2.0 * a, db = 2.0 * b;
-    return love_term(xp, yp, ym, db) + love_term(yp, xp, xm, da) +
-           love_term(xm, ym, yp, -db) + love_term(ym, xm, xp, -da);
-}
-
 __global__ void love_table_kernel(double* __restrict__ tab, int Ns, double h, double scale) {
     const long n = (long)Ns * Ns;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
@@ -297,10 +266,8 @@ void record_tuned(int kind, int dbl, int Ns, int rv, int cv) {
 }
 
 // ----------------------------------------------------------------------------
-// launchers (variant V compile-time; small sizes collapse to variant 0)
+// launch attributes and persistent grids (the launchers are in fft_launch.cuh)
 // ----------------------------------------------------------------------------
-__host__ __device__ constexpr int vclamp(int L, int V) { return L >= 128 ? V : 0; }
-
 namespace {
 std::mutex g_attr_mu;
 std::map<std::pair<const void*, int>, int> g_attr_done;
@@ -347,41 +314,6 @@ int persistent_blocks(const void* func, int threads, int smem, int units) {
         g_occ[key] = resident;
     }
     return units < resident ? units : resident;
-}
-
-// B > 1: gridDim.y = B instances (functors / gates / spectrum per instance)
-template <typename T, int LR, bool PAD, int V, class Load, class Store>
-void launch_row_fwd(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
-    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-    constexpr int sm = row_fwd_smem<T, LR, PAD, V, Load>();
-    auto k = row_fwd_kernel<T, LR, PAD, V, Load, Store>;
-    fft_attrs((const void*)k, sm);
-    const int units = (nrows + rb - 1) / rb;
-    const int gx = row_fwd_staged<T, LR, PAD, V, Load::kRaw>()
-                       ? persistent_blocks((const void*)k, thr, sm, units) : units;
-    k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
-}
-template <typename T, int LR, bool PAD, int V, class Load, class Store>
-void launch_row_inv(Load ld, Store st, int nrows, cudaStream_t s, const int* gate, int B = 1) {
-    constexpr int rb = row_rb_v<T>(LR, V), thr = row_threads<T>(LR, V);
-    constexpr int sm = row_inv_smem<T, LR, PAD, V, Load>();
-    auto k = row_inv_kernel<T, LR, PAD, V, Load, Store>;
-    fft_attrs((const void*)k, sm);
-    const int units = (nrows + rb - 1) / rb;
-    const int gx = row_inv_staged<T, LR, PAD, V, Load::kTiled>()
-                       ? persistent_blocks((const void*)k, thr, sm, units) : units;
-    k<<<dim3(gx, B), thr, sm, s>>>(ld, st, nrows, tw<T>(LR), tw<T>(2 * LR), gate);
-}
-template <typename T, int LC, int NCM1, bool PAD, int V, class Mult>
-void launch_col(cplx<T>* spec, int nrows, Mult m, cudaStream_t s, const int* gate, int B = 1) {
-    constexpr int ct = col_ct_v<T>(LC, NCM1, V), thr = col_threads<T>(LC, NCM1, V);
-    constexpr int sm = col_smem_total<T, LC, NCM1, PAD, V>();
-    auto k = col_kernel<T, LC, NCM1, PAD, V, Mult>;
-    fft_attrs((const void*)k, sm);
-    const int gx = col_staged<T, LC, NCM1, PAD, V>()
-                       ? persistent_blocks((const void*)k, thr, sm, NCM1 / ct + 1)
-                       : NCM1 / ct + 1;
-    k<<<dim3(gx, B), thr, sm, s>>>(spec, nrows, m, tw<T>(LC), gate);
 }
 
 // the two launches of the split column transform (variant 0 only): parity 0

@@ -1392,6 +1392,11 @@ struct SolverCtx : SolverCtxBase {
         ASB_CUDA(cudaStreamSynchronize(s));
         build_graph(s, lo, n);
     }
+    // one iteration of instances [lo, lo + n) launched kernel by kernel
+    void launch_eager(cudaStream_t s, int lo, int n) {
+        InstanceView view(*this, lo);
+        enqueue_iteration(s, n);
+    }
     void launch_graph(cudaStream_t s, int lo, int n) {
         ASB_CUDA(cudaGraphLaunch(graphs.at(std::make_tuple((int)defect, lo, n)).exec, s));
         count_launches(1);
@@ -1658,8 +1663,24 @@ struct Solver {
                 for (int b = 0; b < B; ++b) ih[b].mv_host += 1;
             }
         }
-        c.ensure_graph(s, 0, B);
+        const bool eager = o.loop_mode == 1;
+        if (o.loop_mode != 0 && !eager) throw Error(ASPHER_EINVAL, "solve_contact: bad loop_mode");
+        if (!eager) c.ensure_graph(s, 0, B);
         write_states();
+        // loop_mode 1: the loop body's kernels launched one by one, the end
+        // instances' halt flags read back after each iteration (the graph's
+        // while condition, evaluated on the host)
+        auto run_eager = [&](int lo, int n) {
+            int hv[2];
+            do {
+                c.launch_eager(s, lo, n);
+                ASB_CUDA(cudaMemcpyAsync(&hv[0], &c.st[lo].halt, sizeof(int),
+                                         cudaMemcpyDeviceToHost, s));
+                ASB_CUDA(cudaMemcpyAsync(&hv[1], &c.st[lo + n - 1].halt, sizeof(int),
+                                         cudaMemcpyDeviceToHost, s));
+                ASB_CUDA(cudaStreamSynchronize(s));
+            } while (hv[0] == H_RUN && hv[1] == H_RUN);
+        };
 
         // ---- the loop: device-driven, the host services rare branches
         auto any_running = [&]() {
@@ -1678,11 +1699,15 @@ struct Solver {
                     hi = b;
                 }
             const int n = hi - lo + 1;
-            if (!c.has_graph(lo, n)) {
-                c.ensure_graph(s, lo, n);  // clobbers st[lo, lo + n)
-                write_states();
+            if (eager) {
+                run_eager(lo, n);
+            } else {
+                if (!c.has_graph(lo, n)) {
+                    c.ensure_graph(s, lo, n);  // clobbers st[lo, lo + n)
+                    write_states();
+                }
+                c.launch_graph(s, lo, n);
             }
-            c.launch_graph(s, lo, n);
             // the host takes over: form the pending load rescale of p
             k_materialize<T><<<dim3(c.grid, n), kRedThreads, 0, s>>>(
                 c.Pd + lo, c.st + lo, c.at(c.p, lo), c.part + (size_t)lo * kPartStride);

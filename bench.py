@@ -362,6 +362,34 @@ def run_ours(args):
     alg_bytes = 12 * 4 * N  # 12 b N, b = 4 (free-space apply model)
     achieved = alg_bytes / t_apply / 1e9
 
+    # the tangential (Cerruti) operator at Ns=2048: both fields' applies in
+    # one pass structure; model bytes 2 x 12 b N (two fields, as the normal
+    # free-space apply) + 3 b N for its three real spectra
+    tangential = {}
+    top = asb.TangentialOperator(Ns)
+    for name, tdt, b in (("f32", torch.float32, 4), ("f64", torch.float64, 8)):
+        qs = [torch.randn(2 * N, dtype=tdt, device=dev) for _ in range(2)]
+        us = torch.empty(2 * N, dtype=tdt, device=dev)
+        for i in range(3):
+            top.matvec_(qs[i % 2], us)
+        tt = []
+        for i in range(10):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            c = torch.cuda.Event(enable_timing=True)
+            a.record()
+            top.matvec_(qs[i % 2], us)
+            c.record()
+            torch.cuda.synchronize()
+            tt.append(a.elapsed_time(c) / 1e3)
+        tm = statistics.mean(tt)
+        tbytes = (2 * 12 + 3) * b * N
+        tangential[name] = {"ms": tm * 1e3, "model_bytes": tbytes,
+                            "achieved_gbs": tbytes / tm / 1e9,
+                            "frac": tbytes / tm / 1e9 / peak}
+        del qs, us
+    del top
+
     # whole-solve roofline: modelled bytes of every PCG iteration over the
     # timed solve time.  FP32 stage: 2 B_op (12 b N free space, 6 b N
     # periodic, b = 4) + the stencil and vector passes (9 + 107) N.  FP64
@@ -499,6 +527,9 @@ def run_ours(args):
                                "model": "FP32 iterations 2 B_op(b=4) + 116 N; FP64 polish "
                                         "iterations FP32 transforms with FP64 row I/O + "
                                         "232 N vector passes; one FP64 apply per polish"},
+            "tangential_apply": {"workload": "TangentialFFTOperator (Cerruti block, nu 0.3) "
+                                             "at Ns=2048, q = [q_x; q_y], L2 flushed",
+                                 **tangential},
             "gpu_launches": launches,
             "clocks": clocks,
             "wall_s_timed": wall,

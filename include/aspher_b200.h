@@ -25,7 +25,7 @@
 extern "C" {
 #endif
 
-#define ASPHER_B200_ABI_VERSION 2
+#define ASPHER_B200_ABI_VERSION 3
 
 /* ---- error codes ------------------------------------------------------- */
 #define ASPHER_OK 0
@@ -164,6 +164,14 @@ typedef struct {
     int datum_mode;         /* enum aspher_datum_mode */
     double datum;
     int dtype;              /* working precision Real: ASPHER_F32 / ASPHER_F64 */
+    int n_grid;             /* SolveOptions::n_grid: the physical cell count for
+                               P = p_bar n_grid and the reported fractions
+                               (0 -> Ns*Ns); set by the library where the solve
+                               runs on a larger embedding grid */
+    int loop_mode;          /* 0: the iterations in a CUDA-graph while loop (default);
+                               1: the same kernels launched one by one (for
+                               per-kernel profilers, which cannot see inside
+                               graphs with conditional nodes) */
 } aspher_solve_opts;
 
 /* Fills the reference defaults (SolveOptions{} and solve_contact(...)'s
@@ -351,6 +359,72 @@ int aspher_adjoint(aspher_op* op, int dtype, const double* p_dev, const double* 
  * x_dev and y_dev must not alias.  Async on `stream`. */
 int aspher_periodic_matvec_noalloc(int grid_size, double domain_size, double E_star, int dtype,
                                    const void* x_dev, void* y_dev, void* stream);
+
+/* ---- tangential (Cerruti) operator ------------------------------------------ */
+typedef struct aspher_tan_op aspher_tan_op;
+
+/* Replaces CerrutiKernel(Ns, L, E*, nu) + TangentialFFTOperator(kernel).build()
+ * (include/cerruti_kernel.hpp:35-61, include/tangential_operator.hpp:32-57;
+ * src/cerruti_kernel.cpp:114-128, src/tangential_operator.cpp:18-77): the
+ * Cerruti tables and their three real spectra built on the device in FP64,
+ * with the reference's realness check (ASPHER_EBUILD when it fails).
+ * grid_size: a power of two in [16, 2048]; nu in [0, 1).  Synchronous. */
+int aspher_tan_create(int grid_size, double domain_size, double E_star, double nu,
+                      aspher_tan_op** out);
+int aspher_tan_destroy(aspher_tan_op* op);
+
+/* u = C q (TangentialFFTOperator::matvec_into,
+ * include/tangential_operator.hpp:41-42): q = [q_x; q_y] and u = [u_x; u_y],
+ * 2 Ns*Ns values of `dtype` each (F64, or F32 with the spectra in FP32),
+ * stacked as the reference's dense block [[XX, XY], [XY, YY]] expects.  q
+ * and u may alias.  Async on `stream`. */
+int aspher_tan_matvec(aspher_tan_op* op, int dtype, const void* q_dev, void* u_dev,
+                      void* stream);
+
+/* Build-time max |discarded part| / max |kept part| over the three spectra
+ * (the reference's realness check, tangential_operator.cpp:52-59). */
+int aspher_tan_max_im_ratio(const aspher_tan_op* op, double* out);
+
+/* CerrutiKernel::xx_offset / yy_offset / xy_offset (cerruti_kernel.hpp:44-58)
+ * for dx, dy in (-Ns, Ns), copied to host arrays of (2 Ns - 1)^2 doubles,
+ * row-major [dy + Ns - 1][dx + Ns - 1]. */
+int aspher_tan_tables(const aspher_tan_op* op, double* xx_host, double* yy_host,
+                      double* xy_host);
+
+/* TangentialResult (include/friction_solve.hpp:14-44) */
+typedef struct {
+    int status;              /* enum aspher_status */
+    char status_reason[48];  /* "", "stall", "local_kkt", "outer force iteration",
+                                "local_kkt_near_tolerance" */
+    int iterations;
+    int converged;
+    double error;            /* the iteration's KKT stationarity metric */
+    double delta_t[2];       /* rigid shift (the force-control multiplier) */
+    double q_mean[2];        /* grid-mean traction */
+    int n_stick, n_slip, n_open;
+    double cone_violation;   /* max(0, |q_i| - s_i) / s_ref */
+    double stick_residual;   /* max |w_i| over stick / w_ref */
+    double slip_residual;    /* max(|w_perp|, (-w.qhat)+) over slip / w_ref */
+    double proj_residual;    /* ||q - proj[q - rho g]||_inf / s_ref */
+    double force_error;      /* |q_mean - q_bar| / s_ref (force control) */
+    double rho, s_ref, w_ref, kkt_tol;
+} aspher_tan_result;
+
+/* solve_tangential (include/friction_solve.hpp:62-76, src/friction_solve.cpp:
+ * 375-688) on the operator of `op`, unpreconditioned, FP64:
+ *   displacement control (force_control = 0): min 1/2 q'Cq - sum q_i.delta,
+ *     |q_i| <= s_i, with delta = (target_x, target_y);
+ *   force control: the same with mean(q) = (target_x, target_y), by the
+ *     reference's outer Newton / Broyden iteration on the rigid shift.
+ * s_dev: Ns*Ns thresholds (>= 0; open points s = 0); q_init_dev (nullable,
+ * 2 Ns*Ns) a warm start; u_hist_dev (nullable, 2 Ns*Ns) the history term
+ * added to u; q_dev: 2 Ns*Ns output.  kkt_tol <= 0: 1e-2 (the reference's
+ * default local-KKT acceptance).  Synchronous. */
+int aspher_solve_tangential(aspher_tan_op* op, const double* s_dev, int force_control,
+                            double target_x, double target_y, double tol, int max_iter,
+                            int use_pr, double kkt_tol, const double* q_init_dev,
+                            const double* u_hist_dev, double* q_dev, aspher_tan_result* res,
+                            void* stream);
 
 /* ---- nested-grid driver ---------------------------------------------------- */
 /* NestedParams, reference include/nested_solve.hpp:11-119 (the fields that

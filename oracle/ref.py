@@ -5,7 +5,8 @@ INFRASTRUCTURE ONLY.
 (``src/contact_solver.cpp``, ``src/fft_operator.cpp``,
 ``src/periodic_fft_operator.cpp``, ``src/boussinesq_kernel.cpp``,
 ``src/stencil_precond.cpp``, ``src/fourier_precond.cpp``,
-``src/cerruti_kernel.cpp``, with the vendored pocketfft and OpenMP) against the project's Eigen-API shim
+``src/cerruti_kernel.cpp``, ``src/friction_solve.cpp``, with the vendored
+pocketfft and OpenMP) against the project's Eigen-API shim
 (``oracle/eigen_shim``) and the C-ABI harness ``oracle/ref_harness.cpp`` into
 ``oracle/_ref/libaspher_ref.so``.  ``ContactSolver`` below mirrors the
 reference's pybind11 class (``python/bindings.cpp:115-214``) for the fft and
@@ -74,6 +75,15 @@ def lib():
         L.aref_set_threads.argtypes = [ctypes.c_int]
         L.aref_cerruti_tables.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_double, _D, _D, _D]
+        L.aref_tan_create.restype = ctypes.c_void_p
+        L.aref_tan_create.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double]
+        L.aref_tan_destroy.argtypes = [ctypes.c_void_p]
+        L.aref_tan_matvec.argtypes = [ctypes.c_void_p, _D, _D]
+        L.aref_solve_tangential.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
+                                            ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_double, _D, _D,
+                                            ctypes.c_char_p]
         for f in (L.aref_cerruti_uxx, L.aref_cerruti_uxy):
             f.restype = ctypes.c_double
         L.aref_cerruti_uxx.argtypes = [ctypes.c_double] * 5
@@ -119,6 +129,57 @@ def cerruti_uxx(x, y, a, b, nu):
 
 def cerruti_uxy(x, y, a, b):
     return lib().aref_cerruti_uxy(float(x), float(y), float(a), float(b))
+
+
+_TAN_FIELDS = ("status", "iterations", "converged", "error", "delta_x", "delta_y", "qmean_x",
+               "qmean_y", "n_stick", "n_slip", "n_open", "cone_violation", "stick_residual",
+               "slip_residual", "proj_residual", "force_error", "rho", "s_ref", "w_ref",
+               "kkt_tol")
+
+
+class Tangential:
+    """The tangential (Cerruti) FFT operator of src/tangential_operator.cpp,
+    restated in the harness on the reference's FFT engine and CerrutiKernel,
+    with the reference's solve_tangential (src/friction_solve.cpp) on it."""
+
+    def __init__(self, grid_size, domain_size=1.0, E_star=1.0, nu=0.3):
+        self.Ns = int(grid_size)
+        self._h = lib().aref_tan_create(self.Ns, float(domain_size), float(E_star), float(nu))
+        if not self._h:
+            raise ValueError(lib().aref_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().aref_tan_destroy(self._h)
+            self._h = None
+
+    def matvec(self, q):
+        q = np.ascontiguousarray(np.asarray(q, np.float64).reshape(-1))
+        u = np.empty_like(q)
+        lib().aref_tan_matvec(self._h, _dp(q), _dp(u))
+        return u
+
+    def solve(self, s, force_control, target, tol=1e-8, max_iter=5000, use_pr=True,
+              kkt_tol=0.0):
+        """solve_tangential(C, s, force_control, target, tol, max_iter, use_pr)
+        unpreconditioned; returns (q (2N,), dict of the result fields)."""
+        s = np.ascontiguousarray(np.asarray(s, np.float64).reshape(-1))
+        q = np.empty(2 * s.size, np.float64)
+        out = np.zeros(len(_TAN_FIELDS), np.float64)
+        reason = ctypes.create_string_buffer(64)
+        rc = lib().aref_solve_tangential(self._h, _dp(s), int(bool(force_control)),
+                                         float(target[0]), float(target[1]), float(tol),
+                                         int(max_iter), int(bool(use_pr)), float(kkt_tol),
+                                         _dp(q), _dp(out), reason)
+        if rc != 0:
+            raise ValueError(lib().aref_last_error().decode())
+        d = dict(zip(_TAN_FIELDS, out.tolist()))
+        d["status"] = STATUS[int(d["status"])]
+        d["status_reason"] = reason.value.decode()
+        for k in ("iterations", "n_stick", "n_slip", "n_open"):
+            d[k] = int(d[k])
+        d["converged"] = bool(d["converged"])
+        return q, d
 
 
 _SCALARS = ("status", "iterations", "converged", "contact_fraction", "mean_pressure",

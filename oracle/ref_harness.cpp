@@ -32,6 +32,8 @@
 #include "boussinesq_kernel.hpp"
 #include "cerruti_kernel.hpp"
 #include "contact_solver.hpp"
+#include "fft_engine.hpp"
+#include "friction_solve.hpp"
 #include "fft_operator.hpp"
 #include "fourier_precond.hpp"
 #include "periodic_fft_operator.hpp"
@@ -139,6 +141,79 @@ int solve_t(RefOp* op, const double* g0, double p_bar, const hmc::SolveOptions& 
     std::snprintf(status_out, 64, "%s", r.status_reason.c_str());
     return 0;
 }
+
+// The tangential FFT operator, restated from src/tangential_operator.cpp:
+// 18-140 on the reference's own FFT engine (fft_engine.hpp) and Cerruti
+// tables: that file itself cannot be compiled here (it includes the H2
+// operator, which needs far more of Eigen than the stand-in has).  Checked
+// against the dense Cerruti block in tests/test_tangential_oracle.py.
+struct RefTangential {
+    int Ns, M, nh;
+    hmc::CerrutiKernel kernel;
+    std::vector<double> Kxx, Kyy, Kxy;  // (nh x M), 1/M^2 folded in
+    mutable Eigen::MatrixXd G1, G2;
+    mutable Eigen::MatrixXcd C1, C2;
+    mutable hmc::fft::SquareR2C<double> f1, f2;
+
+    RefTangential(int Ns_, double L, double E, double nu)
+        : Ns(Ns_), M(2 * Ns_), nh(Ns_ + 1), kernel(Ns_, L, E, nu) {
+        Eigen::MatrixXd K(M, M);
+        Eigen::MatrixXcd Kc(nh, M);
+        hmc::fft::SquareR2C<double> plan;
+        plan.bind(M, K.data(), Kc.data());
+        const double norm = 1.0 / (double(M) * double(M));
+        auto harvest = [&](int which, std::vector<double>& out) {
+            for (int iy = 0; iy < M; ++iy)
+                for (int ix = 0; ix < M; ++ix) {
+                    const int dy = iy < Ns ? iy : iy - M, dx = ix < Ns ? ix : ix - M;
+                    double v = 0.0;
+                    if (iy != Ns && ix != Ns)
+                        v = which == 0 ? kernel.xx_offset(dx, dy)
+                                       : which == 1 ? kernel.yy_offset(dx, dy)
+                                                    : kernel.xy_offset(dx, dy);
+                    K(ix, iy) = v;
+                }
+            plan.fwd();
+            out.resize(size_t(nh) * M);
+            for (int ky = 0; ky < M; ++ky)
+                for (int kx = 0; kx < nh; ++kx) out[size_t(ky) * nh + kx] = norm * Kc(kx, ky).real();
+        };
+        harvest(0, Kxx);
+        harvest(1, Kyy);
+        harvest(2, Kxy);
+        G1.resize(M, M);
+        G2.resize(M, M);
+        C1.resize(nh, M);
+        C2.resize(nh, M);
+        f1.bind(M, G1.data(), C1.data(), Ns);
+        f2.bind(M, G2.data(), C2.data(), Ns);
+    }
+    void apply(const Eigen::VectorXd& q, Eigen::VectorXd& u) const {
+        const int N = Ns * Ns;
+        if (u.size() != 2 * N) u.resize(2 * N);
+        for (int iy = 0; iy < Ns; ++iy)
+            for (int ix = 0; ix < M; ++ix) {
+                G1(ix, iy) = ix < Ns ? q(iy * Ns + ix) : 0.0;
+                G2(ix, iy) = ix < Ns ? q(N + iy * Ns + ix) : 0.0;
+            }
+        f1.fwd();
+        f2.fwd();
+        for (int ky = 0; ky < M; ++ky)
+            for (int kx = 0; kx < nh; ++kx) {
+                const size_t at = size_t(ky) * nh + kx;
+                const std::complex<double> a = C1(kx, ky), b = C2(kx, ky);
+                C1(kx, ky) = Kxx[at] * a + Kxy[at] * b;
+                C2(kx, ky) = Kxy[at] * a + Kyy[at] * b;
+            }
+        f1.inv();
+        f2.inv();
+        for (int iy = 0; iy < Ns; ++iy)
+            for (int ix = 0; ix < Ns; ++ix) {
+                u(iy * Ns + ix) = G1(ix, iy);
+                u(N + iy * Ns + ix) = G2(ix, iy);
+            }
+    }
+};
 
 }  // namespace
 
@@ -313,6 +388,59 @@ double aref_cerruti_uxx(double x, double y, double a, double b, double nu) {
 }
 double aref_cerruti_uxy(double x, double y, double a, double b) {
     return hmc::cerruti_uxy(x, y, a, b);
+}
+
+void* aref_tan_create(int Ns, double L, double E_star, double nu) {
+    try {
+        return new RefTangential(Ns, L, E_star, nu);
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return nullptr;
+    }
+}
+void aref_tan_destroy(void* h) { delete static_cast<RefTangential*>(h); }
+int aref_tan_matvec(void* h, const double* q, double* u) {
+    const RefTangential* t = static_cast<RefTangential*>(h);
+    const int64_t n2 = 2 * int64_t(t->Ns) * t->Ns;
+    hmc::VecT<double> qv(n2), uv;
+    std::memcpy(qv.data(), q, sizeof(double) * n2);
+    t->apply(qv, uv);
+    std::memcpy(u, uv.data(), sizeof(double) * n2);
+    return 0;
+}
+
+// solve_tangential (src/friction_solve.cpp:375-688) on the tangential FFT
+// operator, unpreconditioned: displacement control (force_control = 0,
+// target = the rigid shift) or force control (target = the mean traction).
+// out[] = status, iterations, converged, error, delta_t x/y, q_mean x/y,
+// n_stick, n_slip, n_open, cone_violation, stick_residual, slip_residual,
+// proj_residual, force_error, rho, s_ref, w_ref, kkt_tol
+int aref_solve_tangential(void* h, const double* s, int force_control, double tx, double ty,
+                          double tol, int max_iter, int use_pr, double kkt_tol, double* q_out,
+                          double* out, char* status_reason) {
+    try {
+        const RefTangential* t = static_cast<RefTangential*>(h);
+        const int N = t->Ns * t->Ns;
+        Eigen::VectorXd sv(N);
+        std::memcpy(sv.data(), s, sizeof(double) * N);
+        hmc::TanMatVecInto C = [t](const Eigen::VectorXd& q, Eigen::VectorXd& u) { t->apply(q, u); };
+        hmc::TangentialResult r =
+            hmc::solve_tangential(C, sv, force_control != 0, Eigen::Vector2d(tx, ty), tol,
+                                  max_iter, use_pr != 0, {}, nullptr, nullptr, 0.0, nullptr,
+                                  nullptr, kkt_tol);
+        std::memcpy(q_out, r.q.data(), sizeof(double) * 2 * N);
+        const double v[] = {double(int(r.status)), double(r.iterations), r.converged ? 1.0 : 0.0,
+                            r.error, r.delta_t(0), r.delta_t(1), r.q_mean(0), r.q_mean(1),
+                            double(r.n_stick), double(r.n_slip), double(r.n_open),
+                            r.cone_violation, r.stick_residual, r.slip_residual, r.proj_residual,
+                            r.force_error, r.rho, r.s_ref, r.w_ref, r.kkt_tol};
+        std::memcpy(out, v, sizeof(v));
+        std::snprintf(status_reason, 64, "%s", r.status_reason.c_str());
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return -1;
+    }
 }
 
 const char* aref_status_string(int s) { return hmc::to_string(static_cast<hmc::SolveStatus>(s)); }

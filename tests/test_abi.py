@@ -29,7 +29,7 @@ def test_library_loads_and_exports_every_declared_symbol():
     for n in names:
         assert hasattr(lib, n), n
         assert n in _lib.SIGNATURES, "ctypes signature missing for " + n
-    assert lib.aspher_abi_version() == 2
+    assert lib.aspher_abi_version() == 3
 
 
 def test_status_strings_match_reference_taxonomy():

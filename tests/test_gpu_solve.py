@@ -203,3 +203,28 @@ def test_mixed_result_states_its_accuracy_vs_fp64(precision):
     assert r.pressure_rel_l2_vs_fp64 <= 1e-4 and r.contact_area_error_vs_fp64 <= 1e-4
     plain = s.solve(g0, pbar, tol, precond="fourier", precision=precision)
     assert plain.pressure_rel_l2_vs_fp64 is None and plain.contact_area_error_vs_fp64 is None
+
+
+@pytest.mark.parametrize("dtype", ["f64", "f32"])
+def test_eager_loop_matches_graph_loop(dtype):
+    """loop_mode="eager" launches the loop body's kernels one by one with the
+    while condition read on the host: the same kernels in the same order, so
+    the same iterates bit for bit (FP64 and FP32, stencil preconditioner,
+    the mixed float_then_double path included)."""
+    from aspher_b200 import Operator, solve_device, solve_device_mixed
+    Ns, pbar = 128, 0.005
+    op = Operator("fft", Ns)
+    g0 = torch.as_tensor(_rough(Ns), device="cuda")
+    dt = torch.float64 if dtype == "f64" else torch.float32
+    a = solve_device(op, g0, pbar, tol=1e-8, precond="fourier", dtype=dt)
+    b = solve_device(op, g0, pbar, tol=1e-8, precond="fourier", dtype=dt, loop_mode="eager")
+    assert a.status == b.status == "converged"
+    assert a.iterations == b.iterations and a.matvec_count == b.matvec_count
+    assert torch.equal(a.pressure_device, b.pressure_device)
+    if dtype == "f64":
+        ma, _ = solve_device_mixed(op, g0, pbar, tol=1e-8, precond="fourier")
+        mb, _ = solve_device_mixed(op, g0, pbar, tol=1e-8, precond="fourier", loop_mode="eager")
+        assert ma.iterations == mb.iterations
+        assert torch.equal(ma.pressure_device, mb.pressure_device)
+    with pytest.raises(ValueError):
+        solve_device(op, g0, pbar, loop_mode="stream")
