@@ -39,7 +39,7 @@ class SolveOpts(C.Structure):
                 ("allow_tolerance_relaxation", C.c_int), ("precond", C.c_int),
                 ("precond_radius", C.c_int), ("p_ref", C.c_double), ("g_ref", C.c_double),
                 ("datum_mode", C.c_int), ("datum", C.c_double), ("dtype", C.c_int),
-                ("n_grid", C.c_int), ("loop_mode", C.c_int)]
+                ("loop_mode", C.c_int)]
 
 
 class Result(C.Structure):

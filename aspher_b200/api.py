@@ -318,7 +318,8 @@ def _loop_mode(mode):
     return 0 if mode == "graph" else 1
 
 
-def _opts(tol, max_iter, use_pr, precond, keep_best, dtype, precond_radius=2, light=True):
+def _opts(tol, max_iter, use_pr, precond, keep_best, dtype, precond_radius=2, light=True,
+          loop_mode="graph"):
     o = L.SolveOpts()
     L.lib().aspher_solve_opts_default(C.byref(o))
     o.tol = float(tol)
@@ -331,12 +332,13 @@ def _opts(tol, max_iter, use_pr, precond, keep_best, dtype, precond_radius=2, li
     o.precond = L.PRECOND[precond]
     o.precond_radius = int(precond_radius)
     o.dtype = L.F64 if dtype == torch.float64 else L.F32
+    o.loop_mode = _loop_mode(loop_mode)
     return o
 
 
 def solve_device_batch(op, g0s, p_nominals, tol=1e-8, max_iter=5000, use_pr=True,
                        precond="none", p_inits=None, dtype=torch.float64, keep_best=True,
-                       pressures_out=None):
+                       pressures_out=None, loop_mode="graph"):
     """Batched solve_contact_impl<Real>: the problems g0s[b] (device fields
     of ``dtype``) with loads p_nominals[b] on one operator, solved together
     in one loop graph.  Returns one ContactResult per problem (pressure on
@@ -354,7 +356,7 @@ def solve_device_batch(op, g0s, p_nominals, tol=1e-8, max_iter=5000, use_pr=True
         pis = [None if p is None else p.to(dtype).contiguous().reshape(-1) for p in p_inits]
     outs = pressures_out or [torch.empty(N, dtype=torch.float64, device=g0s[0].device)
                              for _ in range(B)]
-    o = _opts(tol, max_iter, use_pr, precond, keep_best, dtype)
+    o = _opts(tol, max_iter, use_pr, precond, keep_best, dtype, loop_mode=loop_mode)
     arr = C.c_void_p * B
     res = (L.Result * B)()
     L.check(L.lib().aspher_solve_batch(
@@ -367,7 +369,7 @@ def solve_device_batch(op, g0s, p_nominals, tol=1e-8, max_iter=5000, use_pr=True
 
 def solve_device_batch_mixed(op, g0s, p_nominals, tol=1e-6, float_tol=None, polish=True,
                              max_iter=5000, use_pr=True, precond="fourier", keep_best=True,
-                             pressures_out=None, polish_tol=None):
+                             pressures_out=None, polish_tol=None, loop_mode="graph"):
     """Batched FP32 stage (FP64 reductions) + FP64 polish: the batched form
     of solve_device_mixed (same float_tol / polish_tol meaning).  g0s: FP64
     device fields.  Returns (final results, FP32-stage results)."""
@@ -384,7 +386,7 @@ def solve_device_batch_mixed(op, g0s, p_nominals, tol=1e-6, float_tol=None, poli
     outs = pressures_out or [torch.empty(N, dtype=torch.float64, device=g0s[0].device)
                              for _ in range(B)]
     o = _opts(tol if polish_tol is None or not polish else polish_tol, max_iter, use_pr,
-              precond, keep_best, torch.float64)
+              precond, keep_best, torch.float64, loop_mode=loop_mode)
     o.requested_tol = float(tol)
     arr = C.c_void_p * B
     res, resf = (L.Result * B)(), (L.Result * B)()

@@ -85,7 +85,7 @@ int aspher_op_matvec(aspher_op* op, int dtype, const void* x, void* y, void* str
     const size_t align = dtype == ASPHER_F64 ? 16 : 8;
     if (((uintptr_t)x % align) || ((uintptr_t)y % align))
         throw asb::Error(ASPHER_EINVAL, "aspher_op_matvec: buffers must be 16-byte aligned");
-    op->impl->matvec(dtype == ASPHER_F64, x, y, static_cast<cudaStream_t>(stream));
+    op->impl->apply_caller(dtype == ASPHER_F64, x, y, static_cast<cudaStream_t>(stream));
     return ASPHER_OK;
     ASB_API_END
 }
@@ -95,10 +95,12 @@ int aspher_op_get_info(const aspher_op* op, aspher_op_info* info) {
     if (!op || !op->impl || !info) throw asb::Error(ASPHER_EINVAL, "aspher_op_get_info: NULL");
     const asb::Operator& o = *op->impl;
     std::memset(info, 0, sizeof(*info));
-    info->backend = o.kind;
-    info->grid_size = o.Ns;
+    info->backend = o.backend;
+    info->grid_size = o.Nl;
+    // the transform side of the compute pipeline (embedded grids: that of
+    // the power-of-two grid the caller's block sits in)
     info->padded_side = o.kind == asb::OP_FFT ? 2 * o.Ns : o.Ns;
-    info->n = (int64_t)o.Ns * o.Ns;
+    info->n = (int64_t)o.Nl * o.Nl;
     if (o.kind == asb::OP_FFT)
         info->bytes_spectrum = (int64_t)(o.Ns + 16) * (o.Ns + 1) * 12 + (int64_t)(o.Ns + 1) * (o.Ns + 1) * 8;
     info->bytes_scratch = (int64_t)(o.spec_d_bytes + o.spec_f_bytes);
@@ -145,11 +147,15 @@ int aspher_op_autotune(aspher_op* op, int dtype, int reps, int* row_variant, int
 int aspher_op_love_table(const aspher_op* op, double* host_out) {
     ASB_API_BEGIN
     if (!op || !op->impl || !host_out) throw asb::Error(ASPHER_EINVAL, "aspher_op_love_table: NULL");
-    if (op->impl->kind != asb::OP_FFT || !op->impl->table)
+    const asb::Operator& o = *op->impl;
+    if (o.backend != asb::OP_FFT || !o.table)
         throw asb::Error(ASPHER_EINVAL, "aspher_op_love_table: only the fft backend has a table");
-    const size_t n = (size_t)op->impl->Ns * op->impl->Ns;
+    // the Nl x Nl offsets of the caller's grid (the device table has the
+    // compute grid's pitch)
     std::lock_guard<std::recursive_mutex> setup(asb::setup_mutex());
-    ASB_CUDA(cudaMemcpy(host_out, op->impl->table, n * sizeof(double), cudaMemcpyDeviceToHost));
+    ASB_CUDA(cudaMemcpy2D(host_out, (size_t)o.Nl * sizeof(double), o.table,
+                          (size_t)o.Ns * sizeof(double), (size_t)o.Nl * sizeof(double), o.Nl,
+                          cudaMemcpyDeviceToHost));
     return ASPHER_OK;
     ASB_API_END
 }

@@ -17,6 +17,7 @@
 #include "fft_kernels.cuh"
 #include "fft_launch.cuh"
 #include "functors.cuh"
+#include "embed.cuh"
 #include "kernel_tables.cuh"
 #include "ops.hpp"
 #include "pcg.hpp"
@@ -631,6 +632,99 @@ struct KhBuild {
     }
 };
 
+// ----------------------------------------------------------------------------
+// Real-space kernel of the periodic operator on an Nl torus (embedded
+// periodic operators).  The reference applies c2r(sigma r2c(x)) with
+// sigma(kx, ky) = scale / |m| (0 at the zero mode; periodic_fft_operator.cpp:
+// 31-45); with sigma even in each wavenumber that is the circulant
+//   y(i) = sum_j T((i - j) mod Nl) x(j),
+//   T(dy, dx) = sum_{ky, kx < Nl} sigma cos(2 pi kx dx / Nl) cos(2 pi ky dy / Nl),
+// which the free-space pipeline computes as the padded linear convolution of
+// the block with T over offsets |d| < Nl (T even: T(-d) = T(Nl - d) = T(d)).
+// T is formed as two cosine sums over the half range of each wavenumber
+// (weights 2 but at 0 and the even-Nl Nyquist index), each accumulated with
+// Kahan compensation in FP64, so every entry carries a few roundings of the
+// largest term (T(0, 0) ~ scale Nl) rather than sqrt(Nl) of them.
+// ----------------------------------------------------------------------------
+__global__ void k_cos_table(int Nl, double* __restrict__ c) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < Nl; r += gridDim.x * blockDim.x)
+        c[r] = cospi(2.0 * (double)r / (double)Nl);
+}
+
+__device__ __forceinline__ double half_weight(int k, int Nl) {
+    return (k == 0 || 2 * k == Nl) ? 1.0 : 2.0;
+}
+
+__device__ __forceinline__ void kahan_add(double& sum, double& comp, double term) {
+    const double y = term - comp;
+    const double t = sum + y;
+    comp = (t - sum) - y;
+    sum = t;
+}
+
+// A[ky][dx] = sum_{kx < nh} w(kx) sigma(kx, ky) cos(2 pi kx dx / Nl), ky < nh
+// (block: one ky, threads over dx; shared: the cosine table and sigma's row)
+__global__ void k_periodic_rows(int Nl, double scale, const double* __restrict__ ctab,
+                                double* __restrict__ A) {
+    extern __shared__ double sh[];
+    const int nh = Nl / 2 + 1;
+    double* cs = sh;        // Nl cosines
+    double* sg = sh + Nl;   // nh weighted symbol values of this ky
+    const int ky = blockIdx.y;
+    for (int r = threadIdx.x; r < Nl; r += blockDim.x) cs[r] = ctab[r];
+    for (int kx = threadIdx.x; kx < nh; kx += blockDim.x) {
+        const double m2 = (double)kx * kx + (double)ky * ky;
+        sg[kx] = m2 > 0.0 ? half_weight(kx, Nl) * (scale / sqrt(m2)) : 0.0;
+    }
+    __syncthreads();
+    const int dx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (dx >= Nl) return;
+    double sum = 0.0, comp = 0.0;
+    int idx = 0;  // (dx kx) mod Nl
+    for (int kx = 0; kx < nh; ++kx) {
+        kahan_add(sum, comp, sg[kx] * cs[idx]);
+        idx += dx;
+        if (idx >= Nl) idx -= Nl;
+    }
+    A[(size_t)ky * Nl + dx] = sum;
+}
+
+// T[dy][dx] = sum_{ky < nh} w(ky) cos(2 pi ky dy / Nl) A[ky][dx], written
+// into the Ns x Ns table (pitch Ns) whose entries at |d| >= Nl stay zero
+__global__ void k_periodic_cols(int Nl, int Ns, const double* __restrict__ ctab,
+                                const double* __restrict__ A, double* __restrict__ tab) {
+    const int nh = Nl / 2 + 1;
+    const int dy = blockIdx.y;
+    const int dx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (dx >= Nl) return;
+    double sum = 0.0, comp = 0.0;
+    int idx = 0;  // (dy ky) mod Nl
+    for (int ky = 0; ky < nh; ++ky) {
+        kahan_add(sum, comp, half_weight(ky, Nl) * __ldg(&ctab[idx]) * A[(size_t)ky * Nl + dx]);
+        idx += dy;
+        if (idx >= Nl) idx -= Nl;
+    }
+    tab[(size_t)dy * Ns + dx] = sum;
+}
+
+void periodic_kernel_table(int Nl, int Ns, double scale, double* tab) {
+    const int nh = Nl / 2 + 1;
+    double *ctab = nullptr, *A = nullptr;
+    ASB_CUDA(cudaMalloc(&ctab, (size_t)Nl * sizeof(double)));
+    ASB_CUDA(cudaMalloc(&A, (size_t)nh * Nl * sizeof(double)));
+    ASB_CUDA(cudaMemset(tab, 0, (size_t)Ns * Ns * sizeof(double)));
+    k_cos_table<<<(Nl + 255) / 256, 256>>>(Nl, ctab);
+    const int smem = (Nl + nh) * (int)sizeof(double);
+    smem_optin((const void*)k_periodic_rows, smem);
+    k_periodic_rows<<<dim3((Nl + 127) / 128, nh), 128, smem>>>(Nl, scale, ctab, A);
+    k_periodic_cols<<<dim3((Nl + 127) / 128, Nl), 128>>>(Nl, Ns, ctab, A, tab);
+    count_launches(3);
+    ASB_CUDA(cudaGetLastError());
+    ASB_CUDA(cudaDeviceSynchronize());
+    cudaFree(ctab);
+    cudaFree(A);
+}
+
 // tiled copy of the canonical Kh for column tile width ct (both precisions)
 __global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
                             double* __restrict__ kd, int ct_f, float* __restrict__ kf) {
@@ -665,29 +759,41 @@ __global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
     }
 
 Operator::Operator(int kind_, int Ns_, double L_, double E_, int flags)
-    : kind(kind_), Ns(Ns_), L(L_), E_star(E_) {
+    : kind(kind_), Ns(Ns_), L(L_), E_star(E_), Nl(Ns_), backend(kind_) {
     if (kind != OP_FFT && kind != OP_PERIODIC) throw Error(-1, "unknown operator kind");
-    if (!is_pow2(Ns) || Ns < 16 || Ns > kMaxNs)
-        throw Error(-1, "grid_size must be a power of two in [16, 16384]");
+    if (Nl < 2 || Nl > kMaxNs) throw Error(-1, "grid_size must be in [2, 16384]");
     if (!(L > 0.0) || !std::isfinite(L)) throw Error(-1, "domain_size must be positive");
     if (!(E_star > 0.0) || !std::isfinite(E_star)) throw Error(-1, "E_star must be positive");
+    if (flags & ~(OPF_SPLIT_COLUMNS | OPF_SPLIT_KH)) throw Error(-1, "unknown operator flags");
+    if (!is_pow2(Nl) || Nl < 16) {
+        // embedded: the free-space pipeline of the next power of two
+        if (flags) throw Error(-1, "operator flags need a power-of-two grid_size in [16, 16384]");
+        int nc = 16;
+        while (nc < Nl) nc *= 2;
+        Ns = nc;
+        kind = OP_FFT;
+    }
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ASB_CUDA(cudaGetDevice(&device));
     (void)tw_table(false, 2);
-    if (flags & ~(OPF_SPLIT_COLUMNS | OPF_SPLIT_KH)) throw Error(-1, "unknown operator flags");
     // cross-check forms: the free-space column pass in its split (two
     // half-length) form and the FP64 Kh build from even / odd row samples at
     // every size >= kSplitMin, the forms FP64 at Ns = 8192 and 16384 need
     split_cols = kind == OP_FFT && Ns >= kSplitMin && (flags & OPF_SPLIT_COLUMNS);
     split_kh = kind == OP_FFT && Ns >= kSplitMin && (flags & OPF_SPLIT_KH);
-    if (kind == OP_PERIODIC) {
-        scale = L / (M_PI * E_star * (double)Ns * Ns);
-    } else {
-        // Love table on the device (boussinesq_kernel.cpp:97-106)
+    if (backend == OP_PERIODIC) scale = L / (M_PI * E_star * (double)Nl * Nl);
+    if (kind == OP_FFT) {
         ASB_CUDA(cudaMalloc(&table, (size_t)Ns * Ns * sizeof(double)));
-        const double h = L / Ns;
-        love_table_kernel<<<592, 256>>>(table, Ns, h, 1.0 / (M_PI * E_star));
-        ASB_CUDA(cudaGetLastError());
+        if (backend == OP_FFT) {
+            // Love table on the device (boussinesq_kernel.cpp:97-106) at the
+            // caller's cell size L / Nl (embedded: offsets up to the compute
+            // grid, of which the padded convolution of the block reads |d| < Nl)
+            const double h = L / Nl;
+            love_table_kernel<<<592, 256>>>(table, Ns, h, 1.0 / (M_PI * E_star));
+            ASB_CUDA(cudaGetLastError());
+        } else {
+            periodic_kernel_table(Nl, Ns, scale, table);
+        }
         ASB_SIZE_SWITCH(Ns, KhBuild<NS>::run(*this));
         const size_t nt = (size_t)(Ns + 16) * (Ns + 1);  // widest tiling
         if (supports(true)) {  // no FP64 copy where FP64 applies do not exist
@@ -710,6 +816,8 @@ Operator::~Operator() {
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     ctx_f.reset();
     ctx_d.reset();
+    cudaFree(emb_x);
+    cudaFree(emb_y);
     cudaFree(kh_d);
     cudaFree(kh_f);
     cudaFree(kh_canon);
@@ -898,6 +1006,34 @@ void Operator::matvec_defect(const double* x, const double* x0, double* y, const
                                 PeriodicMult<float>{scale, NS}, StoreAddRows{y, y0, NS, bx},
                                 (float2*)spec, s, gate, B));
     }
+}
+
+void Operator::apply_caller(bool dbl, const void* x, void* y, cudaStream_t s) {
+    if (!embedded()) {
+        matvec(dbl, x, y, s);
+        return;
+    }
+    const long n = (long)Ns * Ns, nl = (long)Nl * Nl;
+    if (!emb_x) {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+        ASB_CUDA(cudaMalloc(&emb_x, n * sizeof(double)));
+        ASB_CUDA(cudaMalloc(&emb_y, n * sizeof(double)));
+    }
+    if (dbl) {
+        k_embed<double, double><<<embed_grid(n), 256, 0, s>>>(Nl, Ns, 1, (const double*)x,
+                                                              (double*)emb_x, 0.0);
+        matvec(true, emb_x, emb_y, s);
+        k_extract<double, double><<<embed_grid(nl), 256, 0, s>>>(Nl, Ns, 1,
+                                                                 (const double*)emb_y, (double*)y);
+    } else {
+        k_embed<float, float><<<embed_grid(n), 256, 0, s>>>(Nl, Ns, 1, (const float*)x,
+                                                            (float*)emb_x, 0.0f);
+        matvec(false, emb_x, emb_y, s);
+        k_extract<float, float><<<embed_grid(nl), 256, 0, s>>>(Nl, Ns, 1, (const float*)emb_y,
+                                                               (float*)y);
+    }
+    count_launches(2);
+    ASB_CUDA(cudaGetLastError());
 }
 
 template <typename T>

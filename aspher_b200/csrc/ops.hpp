@@ -82,9 +82,30 @@ std::recursive_mutex& setup_mutex();
 void smem_optin(const void* func, int bytes);
 
 struct Operator {
+    // the compute grid: a power of two in [16, 16384] and the pipeline
+    // (free-space padded or periodic) that every kernel of this library sees
     int kind = OP_FFT;
     int Ns = 0;
     double L = 1.0, E_star = 1.0;
+    // the caller's grid side and backend.  Equal to Ns / kind unless the
+    // caller's side is not a power of two in [16, 16384]: the operator then
+    // runs EMBEDDED, its Nl x Nl cells the top-left block of an Ns x Ns
+    // free-space pipeline (Ns the next power of two, at least 16) whose
+    // kernel table holds the caller's operator at every offset |d| < Nl:
+    // the Love table at the caller's cell size (backend fft: the padded
+    // convolution of the block is the free-space operator of the Nl grid),
+    // or the real-space kernel of the periodic symbol on the Nl torus
+    // (backend periodic: a circulant on the Nl torus is a linear
+    // convolution with that kernel over offsets |d| < Nl)
+    int Nl = 0;
+    int backend = OP_FFT;
+    bool embedded() const { return Nl != Ns || backend != kind; }
+    // embedded: Ns*Ns scratch fields of the caller-facing apply (lazy)
+    void* emb_x = nullptr;
+    void* emb_y = nullptr;
+    // caller-facing apply: x, y hold Nl*Nl values (embedded: copied into the
+    // compute grid's block and back; otherwise matvec)
+    void apply_caller(bool dbl, const void* x, void* y, cudaStream_t s);
     int device = 0;
     // free space: real half spectrum Kh (1/M^2 folded in), rows ky in [0, Ns]
     // only (Kh is even in ky): canonical [ky][kx] FP64, plus FP64 / FP32

@@ -16,6 +16,7 @@
 #include "ops.hpp"
 #include "pk_state.hpp"
 #include "pcg.hpp"
+#include "embed.cuh"
 #include "reduce.cuh"
 
 #include <algorithm>
@@ -346,10 +347,15 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
     if (gated && st->halt) return;
     constexpr int TW = kStX + 2 * R, TH = kStY + 2 * R;
     __shared__ double tile[TH * TW];
-    const int Ns = P.Ns, msk = Ns - 1;  // Ns is a power of two
+    // Nw: the periodic grid of the wrap (the caller's side; Ns, the row
+    // pitch, unless the operator is embedded)
+    const int Ns = P.Ns, Nw = P.Nl;
+    // halo coordinates run from -R to the last tile's end (up to 63 + R past
+    // Nw); 2R + 1 <= Nw
+    auto wrap = [Nw](int v) { return v < 0 ? v + Nw : v % Nw; };
     const double gmean = st->nc ? st->gcs / st->nc : 0.0;
     const T aT = LAZY ? (T)st->alpha : T(0);
-    const int ntx = (Ns + kStX - 1) / kStX, nty = (Ns + kStY - 1) / kStY;
+    const int ntx = (Nw + kStX - 1) / kStX, nty = (Nw + kStY - 1) / kStY;
     const int tx = threadIdx.x % kStX, tq = threadIdx.x / kStX;
     // sum z (unrounded), sum zT g, sum g, sum zT (g - gp), sum (g - gp), sum g^2
     double acc[DOTS ? 6 : 1];
@@ -368,20 +374,20 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
             const int idx = threadIdx.x + u * 256;
             if (idx < TW * TH) {
                 const int ly = idx / TW, lx = idx - ly * TW;
-                const int gy = (ty0 + ly - R) & msk, gx = (tx0 + lx - R) & msk;
+                const int gy = wrap(ty0 + ly - R), gx = wrap(tx0 + lx - R);
                 const size_t j = (size_t)gy * Ns + gx;
                 hm[u] = mask[j];
                 hv[u] = g[j];
             }
         }
         const int x = tx0 + tx;
-        const bool xin = x < Ns;
+        const bool xin = x < Nw;
         uint8_t om[kStRows];
         T og[kStRows], op[kStRows];
 #pragma unroll
         for (int k = 0; k < kStRows; ++k) {
             const int y = ty0 + tq * kStRows + k;
-            const bool in = xin && y < Ns;
+            const bool in = xin && y < Nw;
             const size_t i = (size_t)(in ? y : 0) * Ns + (in ? x : 0);
             om[k] = in ? mask[i] : 0;
             og[k] = g[i];
@@ -397,7 +403,7 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
 #pragma unroll
         for (int k = 0; k < kStRows; ++k) {
             const int ly = tq * kStRows + k, y = ty0 + ly;
-            if (!xin || y >= Ns) continue;
+            if (!xin || y >= Nw) continue;
             const size_t i = (size_t)y * Ns + x;
             if (!om[k]) {
                 z[i] = T(0);
@@ -635,12 +641,13 @@ StencilW stencil_weights(const StencilTaps& taps) {
 }
 
 // launch of the stencil pass for the runtime radius R in [1, kMaxR]: the
-// register-window kernel for Ns >= 128, the tile kernel below that
+// register-window kernel for Ns >= 128, the tile kernel below that and for
+// embedded grids (Nl < Ns: the wrap is at the caller's side Nl)
 template <typename T, bool LAZY, bool DOTS>
-void launch_stencil(int R, int Ns, dim3 grid, cudaStream_t s, const PkParams* Pp, PkState* st,
-                    const StencilW& W, const T* g, const T* gprev, const uint8_t* mask, T* z,
-                    double* part, int gated) {
-    if (Ns >= kSwSeg) {
+void launch_stencil(int R, int Ns, int Nl, dim3 grid, cudaStream_t s, const PkParams* Pp,
+                    PkState* st, const StencilW& W, const T* g, const T* gprev,
+                    const uint8_t* mask, T* z, double* part, int gated) {
+    if (Ns >= kSwSeg && Nl == Ns) {
         // strips of 32, 16 or 8 rows: the longest that still gives every SM
         // 12 or more warps (a shorter strip re-reads more halo rows; at
         // Ns=2048 16-row strips measured 1 % faster per solve than 8 or 32)
@@ -855,6 +862,11 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_pupd(const PkPar
             st->scale = (double)(T)(P.P_total / acc[1]);
             st->scale_add = 0.0;
             st->fill = 0;
+        } else if (P.Nl != P.Ns) {  // every p is 0, embedded: the host fills the block
+            st->scale = 1.0;
+            st->scale_add = 0.0;
+            st->fill = 2;
+            set_halt(st, H_FILL);
         } else {  // every p is 0: p = p_bar
             st->scale = 1.0;
             st->scale_add = (double)(T)P.p_bar;
@@ -933,6 +945,10 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_reduce(const PkP
             const double x = (double)A[j];
             switch (mode) {
                 case 0:
+                    if (P.Nl != P.Ns) {  // embedded: the caller's block only
+                        const long e = 4 * i4 + j;
+                        if (e / P.Ns >= P.Nl || e % P.Ns >= P.Nl) break;
+                    }
                     acc[0] = fmin(acc[0], x);
                     acc[1] = fmax(acc[1], x);
                     if (!isfinite(x)) acc[2] += 1.0;
@@ -1249,8 +1265,11 @@ struct SolverCtx : SolverCtxBase {
     }
     void configure(int pc, int R) {
         if (pc == precond && (pc != 1 || R == radius)) return;
+        if (pc == 2 && op.embedded())
+            throw Error(ASPHER_EINVAL, "precond 'fourier-fft' needs a power-of-two grid_size in "
+                                       "[16, 16384] (use 'fourier', the stencil, on this grid)");
         if (pc == 1) {
-            taps = make_stencil_taps(op.Ns, R);
+            taps = make_stencil_taps(op.Nl, R);
             W = stencil_weights(taps);
         }
         precond = pc;
@@ -1300,7 +1319,7 @@ struct SolverCtx : SolverCtxBase {
             ++n;
         }
         if (precond == 1) {
-            launch_stencil<T, true, true>(radius, op.Ns, dim3(stencil_grid(op.Ns), B), s, Pd, st, W, g,
+            launch_stencil<T, true, true>(radius, op.Ns, op.Nl, dim3(stencil_grid(op.Nl), B), s, Pd, st, W, g,
                                           gprev, mask, z, part, 1);
             ++n;
         } else {
@@ -1435,6 +1454,15 @@ struct Solver {
         if (cudaEventRecord(c.ev_out, s) == cudaSuccess) cudaStreamWaitEvent(caller, c.ev_out, 0);
     }
 
+    // p = v on the caller's cells (0 outside the block of an embedded grid)
+    void fill_p(T* p, T v) {
+        if (c.op.embedded())
+            k_fill_block<T><<<embed_grid(c.N), 256, 0, s>>>(c.op.Nl, c.op.Ns, p, v);
+        else
+            k_fill<T><<<c.grid, kRedThreads, 0, s>>>(c.N, p, v);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+    }
     void read_states() {
         ASB_CUDA(cudaMemcpyAsync(h.data(), c.st, B * sizeof(PkState), cudaMemcpyDeviceToHost, s));
         ASB_CUDA(cudaStreamSynchronize(s));
@@ -1547,6 +1575,12 @@ struct Solver {
         const auto t_start = std::chrono::steady_clock::now();
         const int Ns = c.op.Ns;
         const long N = (long)Ns * Ns;
+        // the caller's cell count: the load P = p_bar n_grid and the reported
+        // fractions (contact_solver.cpp:623-625,1003-1004); N but for
+        // embedded operators, whose fields hold the caller's block in
+        // compute-grid layout (gap kEmbedPadGap, pressure 0 outside it)
+        const bool emb = c.op.embedded();
+        const double n_grid = (double)c.op.Nl * (double)c.op.Nl;
         constexpr bool is_double = sizeof(T) == 8;
         if (B < 1 || B > c.cap) throw Error(ASPHER_EINVAL, "solve: batch size out of range");
         for (int b = 0; b < B; ++b)
@@ -1565,6 +1599,7 @@ struct Solver {
             P[b] = PkParams{};
             P[b].N = N;
             P[b].Ns = Ns;
+            P[b].Nl = c.op.Nl;
             if (g0s[b] != c.at(c.g0c, b))
                 ASB_CUDA(cudaMemcpyAsync(c.at(c.g0c, b), g0s[b], (size_t)N * sizeof(T),
                                          cudaMemcpyDeviceToDevice, s));
@@ -1586,7 +1621,7 @@ struct Solver {
             if (h[b].red[2] > 0.0)
                 throw Error(ASPHER_EINVAL, "solve_contact: g0 contains non-finite values");
             I.p_bar = p_bars[b];
-            I.P_total = (double)(T)p_bars[b] * (double)N;
+            I.P_total = (double)(T)p_bars[b] * n_grid;
             double g_ref = gref_b ? gref_b[b] : o.g_ref;
             if (!(g_ref > 0.0)) g_ref = gmax_v - gmin_v;
             if (!(g_ref > 0.0)) g_ref = 1.0;
@@ -1630,9 +1665,9 @@ struct Solver {
                 if (ssum > 0.0)
                     k_scale<T><<<c.grid, kRedThreads, 0, s>>>(N, p, (T)(ih[b].P_total / ssum));
                 else
-                    k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, p, pb);
+                    fill_p(p, pb);
             } else {
-                k_fill<T><<<c.grid, kRedThreads, 0, s>>>(N, p, pb);
+                fill_p(p, pb);
             }
             count_launches(1);
         }
@@ -1717,6 +1752,20 @@ struct Solver {
             for (int b = 0; b < B; ++b) {
                 PkState& H = h[b];
                 InstHost& I = ih[b];
+                if (H.fill == 2) {
+                    // an embedded solve's p = p_bar (contact_solver.cpp:498-500)
+                    // on the caller's block; the iteration counter already
+                    // moved on
+                    fill_p(c.at(c.p, b), (T)I.p_bar);
+                    H.fill = 0;
+                    H.u_fresh = 0;
+                    if (H.halt == H_FILL) {
+                        H.halt = H_RUN;
+                        H.skip_mv1 = 0;
+                    }
+                    changed = true;
+                    continue;
+                }
                 if (H.halt != H_STALL && H.halt != H_IDENT) continue;
                 changed = true;
                 if (H.copy_best) {
@@ -1840,8 +1889,8 @@ struct Solver {
             std::strncpy(R.status_reason, reason.c_str(), sizeof(R.status_reason) - 1);
             R.iterations = H.it;
             R.converged = status == ST_CONVERGED;
-            R.contact_fraction = (double)H.nc / (double)N;
-            R.mean_pressure = H.psum / (double)N;
+            R.contact_fraction = (double)H.nc / n_grid;
+            R.mean_pressure = H.psum / n_grid;
             R.approach = H.alpha_ref + I.datum;
             R.objective = ob[b].red[0] + I.datum * I.P_total;
             R.error = H.pk;
@@ -1942,16 +1991,62 @@ StencilTaps make_stencil_taps(int Ns, int R) {
     return t;
 }
 
+// Embedded operators: the caller's Nl x Nl fields copied into compute-grid
+// temporaries (gaps padded with kEmbedPadGap, pressures with 0) on the
+// caller's stream before a solve, and the outputs' blocks copied back after
+// it; stream-ordered allocations, freed on exit.  For other operators every
+// call passes its pointer through.
+struct EmbedIO {
+    Operator& op;
+    cudaStream_t s;
+    std::vector<void*> bufs;
+    EmbedIO(Operator& o, cudaStream_t st) : op(o), s(st) {}
+    ~EmbedIO() {
+        for (void* p : bufs) cudaFreeAsync(p, s);
+    }
+    long n() const { return (long)op.Ns * op.Ns; }
+    template <typename T>
+    T* alloc() {
+        void* p = nullptr;
+        ASB_CUDA(cudaMallocAsync(&p, (size_t)n() * sizeof(T), s));
+        bufs.push_back(p);
+        return static_cast<T*>(p);
+    }
+    template <typename T>
+    const T* in(const T* src, T pad) {
+        if (!src || !op.embedded()) return src;
+        T* d = alloc<T>();
+        k_embed<T, T><<<embed_grid(n()), 256, 0, s>>>(op.Nl, op.Ns, 1, src, d, pad);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+        return d;
+    }
+    double* out(double* dst) { return dst && op.embedded() ? alloc<double>() : dst; }
+    void back(const double* tmp, double* dst) {
+        if (!dst || !op.embedded()) return;
+        k_extract<double, double><<<embed_grid((long)op.Nl * op.Nl), 256, 0, s>>>(op.Nl, op.Ns, 1,
+                                                                                 tmp, dst);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+    }
+};
+
 template <typename T>
 void solve_impl(Operator& op, const aspher_solve_opts& o, const void* g0, double p_bar,
                 const void* p_init, double* pressure, double* disp, double* gap, double* hist,
                 int hist_cap, aspher_result& res, cudaStream_t s, bool polish_stage) {
-    Solver<T> S(get_ctx<T>(op), s);
-    const T* g = (const T*)g0;
-    const T* pi = (const T*)p_init;
-    const bool defect = sizeof(T) == 8 && polish_stage && p_init;
-    S.run(o, &g, &p_bar, &pi, &pressure, disp, gap, hist, hist_cap, &res, nullptr, nullptr,
-          defect);
+    EmbedIO io(op, s);
+    const T* g = io.in((const T*)g0, (T)kEmbedPadGap);
+    const T* pi = io.in((const T*)p_init, T(0));
+    double *pr = io.out(pressure), *ds = io.out(disp), *gp = io.out(gap);
+    {
+        Solver<T> S(get_ctx<T>(op), s);
+        const bool defect = sizeof(T) == 8 && polish_stage && p_init;
+        S.run(o, &g, &p_bar, &pi, &pr, ds, gp, hist, hist_cap, &res, nullptr, nullptr, defect);
+    }
+    io.back(pr, pressure);
+    io.back(ds, disp);
+    io.back(gp, gap);
 }
 template void solve_impl<float>(Operator&, const aspher_solve_opts&, const void*, double,
                                 const void*, double*, double*, double*, double*, int,
@@ -1975,6 +2070,7 @@ void mixed_prepare(Operator& op, const aspher_solve_opts& o, int B, const double
     for (int b = 0; b < B; ++b) {
         probe.P[b].N = N;
         probe.P[b].Ns = op.Ns;
+        probe.P[b].Nl = op.Nl;
     }
     probe.write_params();
     for (int b = 0; b < B; ++b) {
@@ -2020,10 +2116,11 @@ void add_stage(aspher_result& r, const aspher_result& rf) {
 // float_tol with FP64 reductions, and -- when polish -- an FP64 PK solve
 // warm-started from that pressure certifies opts.tol (the caller may ask
 // for a polish tolerance below the requested one).
-void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
-                 const double* p_init, double float_tol, int polish, double* pressure,
-                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
-                 cudaStream_t s) {
+namespace {
+void solve_mixed_core(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
+                      const double* p_init, double float_tol, int polish, double* pressure,
+                      double* disp, double* gap, aspher_result& res, aspher_result* res_float,
+                      cudaStream_t s) {
     std::vector<double> datum, gref;
     mixed_prepare(op, o, 1, &g0, datum, gref, s);
     SolverCtx<double>& cd = get_ctx<double>(op);
@@ -2061,6 +2158,21 @@ void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, dou
     }
     add_stage(res, rf);
 }
+}  // namespace
+
+void solve_mixed(Operator& op, const aspher_solve_opts& o, const double* g0, double p_bar,
+                 const double* p_init, double float_tol, int polish, double* pressure,
+                 double* disp, double* gap, aspher_result& res, aspher_result* res_float,
+                 cudaStream_t s) {
+    EmbedIO io(op, s);
+    const double* g = io.in(g0, kEmbedPadGap);
+    const double* pi = io.in(p_init, 0.0);
+    double *pr = io.out(pressure), *ds = io.out(disp), *gp = io.out(gap);
+    solve_mixed_core(op, o, g, p_bar, pi, float_tol, polish, pr, ds, gp, res, res_float, s);
+    io.back(pr, pressure);
+    io.back(ds, disp);
+    io.back(gp, gap);
+}
 
 // Batched solve of B instances sharing the operator and the options, in one
 // loop graph (per-instance gates = convergence masks).
@@ -2069,12 +2181,22 @@ void solve_batch_impl(Operator& op, const aspher_solve_opts& o, int B, const voi
                       const double* p_bars, const void* const* p_inits, double* const* pressures,
                       aspher_result* res, cudaStream_t s) {
     if (B < 1) throw Error(ASPHER_EINVAL, "solve_batch: batch must be >= 1");
-    Solver<T> S(get_ctx<T>(op, B), s, B);
-    aspher_solve_opts ob = o;
-    if (B > 1) ob.light = 1;
-    S.run(ob, reinterpret_cast<const T* const*>(g0s), p_bars,
-          reinterpret_cast<const T* const*>(p_inits), pressures, nullptr, nullptr, nullptr, 0,
-          res);
+    EmbedIO io(op, s);
+    std::vector<const T*> g(B), pi(B);
+    std::vector<double*> pr(B);
+    for (int b = 0; b < B; ++b) {
+        g[b] = io.in(static_cast<const T*>(g0s[b]), (T)kEmbedPadGap);
+        pi[b] = p_inits ? io.in(static_cast<const T*>(p_inits[b]), T(0)) : nullptr;
+        pr[b] = io.out(pressures[b]);
+    }
+    {
+        Solver<T> S(get_ctx<T>(op, B), s, B);
+        aspher_solve_opts ob = o;
+        if (B > 1) ob.light = 1;
+        S.run(ob, g.data(), p_bars, p_inits ? pi.data() : nullptr, pr.data(), nullptr, nullptr,
+              nullptr, 0, res);
+    }
+    for (int b = 0; b < B; ++b) io.back(pr[b], pressures[b]);
 }
 template void solve_batch_impl<float>(Operator&, const aspher_solve_opts&, int, const void* const*,
                                       const double*, const void* const*, double* const*,
@@ -2083,12 +2205,36 @@ template void solve_batch_impl<double>(Operator&, const aspher_solve_opts&, int,
                                        const void* const*, const double*, const void* const*,
                                        double* const*, aspher_result*, cudaStream_t);
 
+namespace {
+void solve_batch_mixed_core(Operator& op, const aspher_solve_opts& o, int B,
+                            const double* const* g0s, const double* p_bars, double float_tol,
+                            int polish, double* const* pressures, aspher_result* res,
+                            aspher_result* res_float, cudaStream_t s);
+}  // namespace
+
 // Batched FP32 stage + FP64 polish (solve_mixed for B instances).
 void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const double* const* g0s,
                        const double* p_bars, double float_tol, int polish,
                        double* const* pressures, aspher_result* res, aspher_result* res_float,
                        cudaStream_t s) {
     if (B < 1) throw Error(ASPHER_EINVAL, "solve_batch: batch must be >= 1");
+    EmbedIO io(op, s);
+    std::vector<const double*> gv(B);
+    std::vector<double*> prv(B);
+    for (int b = 0; b < B; ++b) {
+        gv[b] = io.in(g0s[b], kEmbedPadGap);
+        prv[b] = io.out(pressures[b]);
+    }
+    solve_batch_mixed_core(op, o, B, gv.data(), p_bars, float_tol, polish, prv.data(), res,
+                           res_float, s);
+    for (int b = 0; b < B; ++b) io.back(prv[b], pressures[b]);
+}
+
+namespace {
+void solve_batch_mixed_core(Operator& op, const aspher_solve_opts& o, int B,
+                            const double* const* g0s, const double* p_bars, double float_tol,
+                            int polish, double* const* pressures, aspher_result* res,
+                            aspher_result* res_float, cudaStream_t s) {
     std::vector<double> datum, gref;
     mixed_prepare(op, o, B, g0s, datum, gref, s);
     SolverCtx<double>& cd = get_ctx<double>(op, B);
@@ -2121,11 +2267,14 @@ void solve_batch_mixed(Operator& op, const aspher_solve_opts& o, int B, const do
     }
     for (int b = 0; b < B; ++b) add_stage(res[b], rf[b]);
 }
+}  // namespace
 
 // Standalone preconditioner apply: z = M^-1 g on contact, contact-mean removed.
 template <typename T>
 void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
                         const uint8_t* mask, T* z, cudaStream_t s) {
+    if (op.embedded())
+        throw Error(ASPHER_EINVAL, "precond_apply needs a power-of-two grid_size in [16, 16384]");
     const long N = (long)op.Ns * op.Ns;
     PkState* st = nullptr;
     double* part = nullptr;
@@ -2135,6 +2284,7 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     PkParams P{};
     P.N = N;
     P.Ns = op.Ns;
+    P.Nl = op.Ns;
     P.precond = precond;
     PkParams* Pd = nullptr;
     ASB_CUDA(cudaMallocAsync((void**)&Pd, sizeof(PkParams), s));
@@ -2143,7 +2293,7 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
     if (precond == 1) {
         StencilTaps taps = make_stencil_taps(op.Ns, radius);
-        launch_stencil<T, false, false>(radius, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st,
+        launch_stencil<T, false, false>(radius, op.Ns, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st,
                                         stencil_weights(taps), g, nullptr, mask, z, part, 0);
     } else {
         fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
@@ -2379,6 +2529,8 @@ template <typename T>
 void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
                   int precond, int radius, double* grad_g0, double* grad_pbar,
                   aspher_adjoint_info* info, cudaStream_t s) {
+    if (op.embedded())
+        throw Error(ASPHER_EINVAL, "adjoint needs a power-of-two grid_size in [16, 16384]");
     if (!(tol > 0.0)) throw Error(ASPHER_EINVAL, "adjoint: tol must be positive");
     if (max_iter < 1) throw Error(ASPHER_EINVAL, "adjoint: max_iter must be >= 1");
     if (precond != ASPHER_PRECOND_NONE && precond != ASPHER_PRECOND_STENCIL)
@@ -2403,6 +2555,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     PkParams P{};
     P.N = N;
     P.Ns = op.Ns;
+    P.Nl = op.Ns;
     P.tol = tol;
     P.max_iter = max_iter;
     P.precond = precond;
@@ -2422,7 +2575,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
         for (int k = 0; k < 16; ++k) {  // kernels return at entry once halted
             const T* zz = r;
             if (precond == ASPHER_PRECOND_STENCIL) {
-                launch_stencil<T, false, false>(radius, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
+                launch_stencil<T, false, false>(radius, op.Ns, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
                                                 nullptr, mask, z, part, 1);
                 zz = z;
             }

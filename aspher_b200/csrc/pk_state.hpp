@@ -14,7 +14,9 @@
 
 namespace asb {
 
-enum Halt : int { H_RUN = 0, H_FINAL = 1, H_STALL = 2, H_IDENT = 3 };
+// H_FILL: every p became 0 in an embedded solve; the host sets p = p_bar on
+// the caller's block (the fill of the cells outside it would be wrong)
+enum Halt : int { H_RUN = 0, H_FINAL = 1, H_STALL = 2, H_IDENT = 3, H_FILL = 4 };
 
 enum Status : int {
     ST_CONVERGED = 0,
@@ -30,6 +32,9 @@ enum Status : int {
 struct PkParams {
     long N;
     int Ns;
+    // the caller's grid side: Ns, or (embedded operators) the side of the
+    // top-left block of the Ns x Ns field that holds the caller's cells
+    int Nl;
     int max_iter;
     int stall_limit;
     int keep_best;
@@ -61,7 +66,8 @@ struct PkState {
     int stall, forced_id;
     int copy_best, have_best;
     int status;
-    int fill;  // total <= 0: the pressure is p_bar everywhere (pending, see scale)
+    int fill;  // total <= 0: the pressure is p_bar everywhere (pending, see scale);
+               // 2: an embedded solve's fill, done by the host (H_FILL)
     int pk_due;  // k_eval ran; k_evalpk records this iteration's pk
     double best_merit, seen_merit;
     // CG recurrences

@@ -73,8 +73,15 @@ typedef struct aspher_op aspher_op;
  * backend FFT and PeriodicFFTOperator(Ns, L, E*)
  * (include/periodic_fft_operator.hpp:26) for backend PERIODIC.  The Love
  * table and its FP64 spectrum are built on the device; synchronous.
- * grid_size must be a power of two in [16, 16384]; at 16384 only FP32
- * applies and solves exist (FP64 ones return ASPHER_EINVAL). */
+ * grid_size in [2, 16384]; at 16384 only FP32 applies and solves exist
+ * (FP64 ones return ASPHER_EINVAL).  A grid_size that is not a power of two
+ * >= 16 runs embedded: its cells are the top-left block of the next
+ * power-of-two grid's free-space pipeline, whose kernel table is the Love
+ * table at cell size domain_size / grid_size (FFT) or the real-space kernel
+ * of the periodic symbol on the grid_size torus (PERIODIC); every entry
+ * point still takes grid_size^2 fields.  Creation flags, the FFT
+ * preconditioner, the adjoint, the standalone preconditioner apply and
+ * the nested driver need a power of two >= 16 (ASPHER_EINVAL otherwise). */
 int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
                      aspher_op** out);
 /* The same with creation flags (the survey's aspher_op_create(kind, Ns, L,
@@ -164,10 +171,6 @@ typedef struct {
     int datum_mode;         /* enum aspher_datum_mode */
     double datum;
     int dtype;              /* working precision Real: ASPHER_F32 / ASPHER_F64 */
-    int n_grid;             /* SolveOptions::n_grid: the physical cell count for
-                               P = p_bar n_grid and the reported fractions
-                               (0 -> Ns*Ns); set by the library where the solve
-                               runs on a larger embedding grid */
     int loop_mode;          /* 0: the iterations in a CUDA-graph while loop (default);
                                1: the same kernels launched one by one (for
                                per-kernel profilers, which cannot see inside
@@ -272,7 +275,7 @@ int aspher_solve_batch_mixed(aspher_op* op, const aspher_solve_opts* opts, int b
  * the current device, 16-byte aligned. */
 typedef struct {
     int backend;           /* ASPHER_BACKEND_FFT / ASPHER_BACKEND_PERIODIC */
-    int grid_size;         /* power of two in [16, 16384] */
+    int grid_size;         /* in [2, 16384] (see aspher_op_create) */
     double domain_size;    /* <= 0: 1 */
     double E_star;         /* <= 0: 1 */
     const double* g0_dev;

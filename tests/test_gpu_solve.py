@@ -216,8 +216,9 @@ def test_eager_loop_matches_graph_loop(dtype):
     op = Operator("fft", Ns)
     g0 = torch.as_tensor(_rough(Ns), device="cuda")
     dt = torch.float64 if dtype == "f64" else torch.float32
-    a = solve_device(op, g0, pbar, tol=1e-8, precond="fourier", dtype=dt)
-    b = solve_device(op, g0, pbar, tol=1e-8, precond="fourier", dtype=dt, loop_mode="eager")
+    tol = 1e-8 if dtype == "f64" else 1e-6
+    a = solve_device(op, g0, pbar, tol=tol, precond="fourier", dtype=dt)
+    b = solve_device(op, g0, pbar, tol=tol, precond="fourier", dtype=dt, loop_mode="eager")
     assert a.status == b.status == "converged"
     assert a.iterations == b.iterations and a.matvec_count == b.matvec_count
     assert torch.equal(a.pressure_device, b.pressure_device)

@@ -190,3 +190,16 @@ def test_oracle_iterations_at_ns2048_equal_reference():
         assert ours[k]["iterations"] == theirs[k]["tol6"]["iterations"], k
         assert ours[k]["status"] == theirs[k]["tol6"]["status"] == "converged", k
         assert abs(ours[k]["contact_area"] - theirs[k]["tol6"]["contact_area"]) <= 1e-6, k
+
+
+@needs_ref
+@pytest.mark.parametrize("backend", ["fft", "periodic"])
+@pytest.mark.parametrize("Ns", [5, 12, 37, 100])
+def test_matvec_matches_reference_any_size(backend, Ns):
+    """Grids that are not powers of two (the reference's pocketfft engine
+    takes any n, src/fft_engine.hpp:147-290): the numpy oracle equals the
+    reference's own operators there too."""
+    a = ref.ContactSolver(Ns, backend=backend, domain_size=1.1, E_star=1.3)
+    b = OracleSolver(Ns, backend=backend, domain_size=1.1, E_star=1.3)
+    x = np.random.default_rng(Ns + 1).standard_normal(Ns * Ns)
+    assert _rel(a.matvec(x), b.matvec(x)) <= 1e-14
