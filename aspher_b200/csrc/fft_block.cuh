@@ -84,6 +84,28 @@ __device__ __forceinline__ void dft(cplx<T>* a) {
     }
 }
 
+// The DFT of R points whose upper half a[R/2 .. R-1] is zero (the first
+// stage of a zero-padded transform): with w = exp(DIR 2 pi i / R),
+//   X[2k] = DFT_{R/2}(a)[k],   X[2k+1] = DFT_{R/2}(a[n] w^n)[k],  n < R/2,
+// two half-length DFTs instead of the full one on zeros (x + 0 is not folded
+// by the compiler: -0 + 0 = +0).
+template <int R, int DIR, typename T>
+__device__ __forceinline__ void dft_upper_zero(cplx<T>* a) {
+    cplx<T> b[R / 2], c[R / 2];
+#pragma unroll
+    for (int n = 0; n < R / 2; ++n) {
+        b[n] = a[n];
+        c[n] = rot_const<R, DIR, T>(a[n], n);
+    }
+    dft<R / 2, DIR, T>(b);
+    dft<R / 2, DIR, T>(c);
+#pragma unroll
+    for (int k = 0; k < R / 2; ++k) {
+        a[2 * k] = b[k];
+        a[2 * k + 1] = c[k];
+    }
+}
+
 __host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v >> 1); }
 
 // Radix of stage `s` for a length-L transform with at most RMAX per stage.
@@ -122,7 +144,7 @@ __device__ __forceinline__ V tw_apply(V a, V w) {
 // Shared-memory elements needed by one transform of length L (padded).
 __host__ __device__ constexpr int sm_len(int L) { return L + L / 16 + 1; }
 
-template <typename T, int L, int RPT, int DIR, int S, int STAGE, int SPAN>
+template <typename T, int L, int RPT, int DIR, int S, int STAGE, int SPAN, bool HZ>
 __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
                                            const cplx<T>* __restrict__ tw) {
     constexpr int RMAX = RPT < 16 ? RPT : 16;
@@ -175,7 +197,13 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
                     }
                 }
             }
-            dft<R, DIR, T>(a);
+            // the zero upper half of the input (HZ) is the upper half of
+            // every first-stage butterfly: a[r] = v[q + r Q] with v[m] = 0
+            // for m >= RPT / 2 exactly when r >= R / 2
+            if constexpr (HZ && STAGE == 0 && R >= 2)
+                dft_upper_zero<R, DIR, T>(a);
+            else
+                dft<R, DIR, T>(a);
             if constexpr (LAST) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) v[q + r * Q] = a[r];
@@ -190,7 +218,7 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
 #pragma unroll
             for (int m = 0; m < RPT; ++m) v[m] = sm[smaddr_run<TT, 1 << 30>(t, m, S, off)];
             __syncthreads();
-            fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R>(v, t, sm, off, tw);
+            fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R, HZ>(v, t, sm, off, tw);
         }
     }
 }
@@ -201,12 +229,13 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
 // table of every power-of-two length M <= L at offset M (so tw - L is the
 // array base and the stages read the shorter tables).  Every thread of the CTA must
 // call this (it contains __syncthreads), including threads whose transform
-// is a dummy.
-template <typename T, int L, int RPT, int DIR, int S>
+// is a dummy.  HZ: the upper half of the input is zero (v[m] = 0 for
+// m >= RPT / 2, a zero-padded transform); its first stage skips the zeros.
+template <typename T, int L, int RPT, int DIR, int S, bool HZ = false>
 __device__ __forceinline__ void block_fft(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
                                           const cplx<T>* __restrict__ tw) {
     static_assert(L % RPT == 0, "L must be a multiple of RPT");
-    fft_stages<T, L, RPT, DIR, S, 0, 1>(v, t, sm, off, tw);
+    fft_stages<T, L, RPT, DIR, S, 0, 1, HZ>(v, t, sm, off, tw);
 }
 
 }  // namespace asb

@@ -287,7 +287,7 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
     auto body = [&](int grp, cplx<T> (&v)[RPT]) {
         const int row = grp * RB + r;
         const bool valid = row < nrows;
-        block_fft<T, LR, RPT, -1, 1>(v, t, sm, off, tw_lr);
+        block_fft<T, LR, RPT, -1, 1, PAD>(v, t, sm, off, tw_lr);
 #pragma unroll
         for (int m = 0; m < RPT; ++m) sm[smaddr_run<TT, 1 << 30>(t, m, 1, off)] = v[m];
         __syncthreads();
@@ -559,7 +559,7 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     // transform, multiply, inverse and store of tile `tile` from registers v
     auto body = [&](int tile, cplx<T> (&v)[RPT]) {
         cplx<T>* base = inst + (size_t)tile * nrows * CT;
-        block_fft<T, LC, RPT, -1, CT>(v, t, sm, c, tw_lc);
+        block_fft<T, LC, RPT, -1, CT, PAD>(v, t, sm, c, tw_lc);
         const int kx = tile * CT + c;
 #pragma unroll
         for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, t + m * TT);

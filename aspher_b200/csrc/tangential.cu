@@ -193,7 +193,7 @@ col_pair_kernel(cplx<T>* __restrict__ spec, long bsp, int nrows, TanMix<T> mix,
 #pragma unroll
     for (int m = 0; m < RPT; ++m)
         v[m] = m >= RPT / 2 ? mk<T>(0, 0) : base[(size_t)(t + m * TT) * CT + cc];
-    block_fft<T, LC, RPT, -1, S>(v, t, sm, c, tw_lc);
+    block_fft<T, LC, RPT, -1, S, true>(v, t, sm, c, tw_lc);
     // every thread publishes its column's spectrum, then reads the other
     // field's column at the same kx (the forward transform's last stage ran
     // in registers, after its last barrier: the workspace is free)

@@ -82,8 +82,8 @@ def lib():
         L.aref_tan_matvec.argtypes = [ctypes.c_void_p, _D, _D]
         L.aref_solve_tangential.argtypes = [ctypes.c_void_p, _D, ctypes.c_int, ctypes.c_double,
                                             ctypes.c_double, ctypes.c_double, ctypes.c_int,
-                                            ctypes.c_int, ctypes.c_double, _D, _D,
-                                            ctypes.c_char_p]
+                                            ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                                            _D, _D, ctypes.c_char_p]
         for f in (L.aref_cerruti_uxx, L.aref_cerruti_uxy):
             f.restype = ctypes.c_double
         L.aref_cerruti_uxx.argtypes = [ctypes.c_double] * 5
@@ -160,17 +160,23 @@ class Tangential:
         return u
 
     def solve(self, s, force_control, target, tol=1e-8, max_iter=5000, use_pr=True,
-              kkt_tol=0.0):
-        """solve_tangential(C, s, force_control, target, tol, max_iter, use_pr)
-        unpreconditioned; returns (q (2N,), dict of the result fields)."""
+              kkt_tol=0.0, q_init=None):
+        """solve_tangential(C, s, force_control, target, tol, max_iter, use_pr,
+        {}, q_init) unpreconditioned; returns (q (2N,), dict of the result
+        fields)."""
         s = np.ascontiguousarray(np.asarray(s, np.float64).reshape(-1))
         q = np.empty(2 * s.size, np.float64)
+        qi = None if q_init is None else np.ascontiguousarray(
+            np.asarray(q_init, np.float64).reshape(-1))
+        if qi is not None and qi.size != 2 * s.size:
+            raise ValueError("q_init has %d entries, expected %d" % (qi.size, 2 * s.size))
         out = np.zeros(len(_TAN_FIELDS), np.float64)
         reason = ctypes.create_string_buffer(64)
         rc = lib().aref_solve_tangential(self._h, _dp(s), int(bool(force_control)),
                                          float(target[0]), float(target[1]), float(tol),
                                          int(max_iter), int(bool(use_pr)), float(kkt_tol),
-                                         _dp(q), _dp(out), reason)
+                                         None if qi is None else qi.ctypes.data, _dp(q), _dp(out),
+                                         reason)
         if rc != 0:
             raise ValueError(lib().aref_last_error().decode())
         d = dict(zip(_TAN_FIELDS, out.tolist()))

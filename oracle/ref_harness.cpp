@@ -416,18 +416,23 @@ int aref_tan_matvec(void* h, const double* q, double* u) {
 // n_stick, n_slip, n_open, cone_violation, stick_residual, slip_residual,
 // proj_residual, force_error, rho, s_ref, w_ref, kkt_tol
 int aref_solve_tangential(void* h, const double* s, int force_control, double tx, double ty,
-                          double tol, int max_iter, int use_pr, double kkt_tol, double* q_out,
-                          double* out, char* status_reason) {
+                          double tol, int max_iter, int use_pr, double kkt_tol,
+                          const double* q_init, double* q_out, double* out,
+                          char* status_reason) {
     try {
         const RefTangential* t = static_cast<RefTangential*>(h);
         const int N = t->Ns * t->Ns;
-        Eigen::VectorXd sv(N);
+        Eigen::VectorXd sv(N), qi;
         std::memcpy(sv.data(), s, sizeof(double) * N);
+        if (q_init) {
+            qi.resize(2 * N);
+            std::memcpy(qi.data(), q_init, sizeof(double) * 2 * N);
+        }
         hmc::TanMatVecInto C = [t](const Eigen::VectorXd& q, Eigen::VectorXd& u) { t->apply(q, u); };
         hmc::TangentialResult r =
             hmc::solve_tangential(C, sv, force_control != 0, Eigen::Vector2d(tx, ty), tol,
-                                  max_iter, use_pr != 0, {}, nullptr, nullptr, 0.0, nullptr,
-                                  nullptr, kkt_tol);
+                                  max_iter, use_pr != 0, {}, q_init ? &qi : nullptr, nullptr,
+                                  0.0, nullptr, nullptr, kkt_tol);
         std::memcpy(q_out, r.q.data(), sizeof(double) * 2 * N);
         const double v[] = {double(int(r.status)), double(r.iterations), r.converged ? 1.0 : 0.0,
                             r.error, r.delta_t(0), r.delta_t(1), r.q_mean(0), r.q_mean(1),

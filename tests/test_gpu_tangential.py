@@ -132,7 +132,12 @@ def test_tangential_solve_matches_reference(Ns, mode):
     differ by 2.3e-3 (Ns = 32) and its tol 1e-8 and 1e-12 ones by 1.6e-3
     (Ns = 64), and its acceptance (friction_solve.cpp:399-413) is local KKT
     within 1e-2.  The force-control gate is the reference's acceptance
-    level: tractions within 1e-2 and both KKT certificates passing."""
+    level: tractions within 1e-2, the rigid shift (the multiplier of
+    mean(q) = q_bar, to which the outer iteration's load residual F maps
+    through the 2x2 stiffness) within 1e-3 -- the acceptance
+    F <= 1e-3 |q_bar| -- and both KKT certificates passing.  The inner
+    iteration itself is pinned tightly in
+    test_tangential_warm_solve_equals_reference."""
     from aspher_b200 import TangentialOperator
     s = _hertz_threshold(Ns)
     if mode == "displacement":
@@ -155,9 +160,33 @@ def test_tangential_solve_matches_reference(Ns, mode):
     if fc:
         assert abs(d["q_mean"][0] - target[0]) <= 1e-12 * abs(target[0])
         assert abs(d["q_mean"][1] - target[1]) <= 1e-12 * abs(target[0])
-        assert abs(d["delta_t"][0] - dr["delta_x"]) <= 1e-4 * abs(dr["delta_x"])
+        assert abs(d["delta_t"][0] - dr["delta_x"]) <= 1e-3 * abs(dr["delta_x"])
+        assert abs(d["delta_t"][1] - dr["delta_y"]) <= 1e-3 * abs(dr["delta_x"])
     else:
         assert d["delta_t"] == target
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("Ns", [32, 64])
+def test_tangential_warm_solve_equals_reference(Ns):
+    """The step force control repeats: a displacement-control solve warm-
+    started from the previous traction (friction_solve.cpp:586-590).  From the
+    same start the device iteration follows the reference's step by step:
+    the same iteration count and tractions equal to 1e-12 (the unpreconditioned
+    tangential PCG stalls at a local-KKT floor of 1e-4 .. 1e-3 at this load,
+    so cold solves from roundoff-different starts part ways at that level;
+    the warm chain does not)."""
+    from aspher_b200 import TangentialOperator
+    s = _hertz_threshold(Ns)
+    target = (0.3 * s.mean(), 0.1 * s.mean())
+    q0, d0 = ref.Tangential(Ns).solve(s, True, target, tol=1e-8, max_iter=5000)
+    delta = (d0["delta_x"] * 1.0001, d0["delta_y"])
+    qr, dr = ref.Tangential(Ns).solve(s, False, delta, tol=1e-8, max_iter=5000, q_init=q0)
+    q, d = TangentialOperator(Ns).solve(s, force_control=False, target=delta, tol=1e-8,
+                                        max_iter=5000, q_init=q0)
+    assert d["status"] == dr["status"]
+    assert d["iterations"] == dr["iterations"]
+    assert _rel(q, qr) <= 1e-12
 
 
 def test_tangential_solve_rejects():
