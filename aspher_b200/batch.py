@@ -112,7 +112,12 @@ def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max
         if pr["backend"] not in L.BACKEND:
             raise ValueError("unknown backend: %s" % pr["backend"])
         Ns = int(pr["grid_size"])
-        g = torch.as_tensor(gaps[i], dtype=torch.float64).to(dev).reshape(-1).contiguous()
+        g = torch.as_tensor(gaps[i], dtype=torch.float64)
+        # host gaps in pinned memory are copied asynchronously on the current
+        # stream (the library's groups wait for it; the tensors stay
+        # referenced until the synchronous call returns)
+        g = g.to(dev, non_blocking=g.device.type == "cpu" and g.is_pinned())
+        g = g.reshape(-1).contiguous()
         if g.numel() != Ns * Ns:
             raise ValueError("solve_many: problem %d: gap has %d entries, expected %d"
                              % (i, g.numel(), Ns * Ns))
@@ -134,4 +139,13 @@ def solve_many(problems, gaps, tol=1e-6, polish_tol=None, precond="fourier", max
     res, resf = (L.Result * n)(), (L.Result * n)()
     with torch.cuda.device(dev):
         L.check(L.lib().aspher_solve_many(n, arr, C.byref(o), res, resf, _stream()))
-    return [ContactResult(res[i], int(problems[i]["grid_size"]), outs[i]) for i in range(n)]
+    out = []
+    for i in range(n):
+        Ns = int(problems[i]["grid_size"])
+        r = ContactResult(res[i], Ns, outs[i])
+        # the FP32 stage of a float_then_double solve (its iterations are
+        # part of r.iterations)
+        r.float_stage = (ContactResult(resf[i], Ns, None) if precision == "float_then_double"
+                         else None)
+        out.append(r)
+    return out

@@ -8,11 +8,15 @@ L = E* = 1), tol 1e-6, 13-tap stencil preconditioner.  One step solves those
 reductions to tol, then an FP64 polish warm-started from it that certifies
 tol/2 on the FP64 operator (a tighter certificate than the plain FP64
 solve's, and on these problems a pressure at least as accurate as its; an
-accuracy gate outside the timed region checks the errors), the
-three loads of one backend solved as one batch.  ``value`` = certified
-solves/s with the gaps resident in HBM; ``e2e`` = the same solves one at a
-time through ``ContactSolver.solve`` with the gap copied from pinned host
-memory and the pressure read back every solve.  The same mixed solves one
+accuracy gate outside the timed region checks the errors), through the
+library's batch call (``solve_many`` / ``aspher_solve_many``): the three
+loads of one backend solved as one batch, the two backends' batches
+concurrently on the library's streams.  ``value`` = certified
+solves/s with the gaps resident in HBM; ``e2e`` = the same six solves
+through the library's batch call (``solve_many`` / ``aspher_solve_many``)
+with the gaps copied from pinned host memory and the pressures read back to
+pinned host memory every step (``e2e.single_contact_solver``: one
+``ContactSolver.solve`` per problem).  The same mixed solves one
 at a time, the plain FP64 GPU solve, a 96-problem uneven batch and the
 adjoint's finite-difference check are measured beside it, and so are the
 fft rows of the reference's backend x precision study (nested solves at
@@ -170,6 +174,7 @@ def run_ours(args):
     import torch.distributed as dist
     import aspher_b200 as asb
     from aspher_b200 import _lib
+    from aspher_b200.batch import solve_many
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -196,21 +201,20 @@ def run_ours(args):
             res.append((r, rf))
         return res
 
-    # batched: the loads of one backend solved together (one loop graph per
-    # backend, per-instance convergence masks)
+    # the loads of each backend
     by_backend = {b: [(p, g) for (bb, p, g) in probs if bb == b] for b in BACKENDS}
-    bouts = {b: [torch.empty(N, dtype=torch.float64, device=dev) for _ in by_backend[b]]
-             for b in BACKENDS}
+
+    # the six problems through the library's batch call with the gaps
+    # resident in HBM: grouped per operator (one batched mixed solve per
+    # backend), the groups concurrent on the library's streams
+    batch_probs = [dict(backend=b, grid_size=Ns, p_nominal=p)
+                   for b in BACKENDS for (p, _) in by_backend[b]]
+    batch_gaps = [gdev[id(g)] for b in BACKENDS for (_, g) in by_backend[b]]
 
     def step_batch():
-        res = []
-        for b in BACKENDS:
-            rs, rfs = asb.solve_device_batch_mixed(
-                ops[b], [gdev[id(g)] for (_, g) in by_backend[b]],
-                [p for (p, _) in by_backend[b]], tol=TOL, float_tol=FLOAT_TOL, polish_tol=POLISH_TOL,
-                precond="fourier", keep_best=False, pressures_out=bouts[b])
-            res.extend(zip(rs, rfs))
-        return res
+        rs = solve_many(batch_probs, batch_gaps, tol=TOL, polish_tol=POLISH_TOL,
+                        float_tol=FLOAT_TOL, precond="fourier", precision="float_then_double")
+        return [(r, r.float_stage) for r in rs]
 
     def step_fp64():
         res = []
@@ -220,6 +224,20 @@ def run_ours(args):
         return res
 
     solvers = {b: asb.ContactSolver(Ns, backend=b) for b in BACKENDS}
+
+    # end to end through the library's heterogeneous batch call: the six
+    # pinned host gaps in, the six pressures back to pinned host memory
+    many_probs = [dict(backend=b, grid_size=Ns, p_nominal=p) for (b, p, _) in probs]
+    many_gaps = [gpin[id(g)] for (_, _, g) in probs]
+    many_out = [torch.empty(N, dtype=torch.float64).pin_memory() for _ in probs]
+
+    def step_e2e_many():
+        rs = solve_many(many_probs, many_gaps, tol=TOL, polish_tol=POLISH_TOL,
+                        float_tol=FLOAT_TOL, precond="fourier", precision="float_then_double")
+        for r, o in zip(rs, many_out):
+            o.copy_(r.pressure_device, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return rs
 
     def step_e2e():
         for (b, p, g) in probs:
@@ -334,10 +352,15 @@ def run_ours(args):
     dt64, _, last64 = timed(step_fp64, max(1, args.steps // 2))
     value64 = len(probs) * max(1, args.steps // 2) * world / dt64
 
-    # end to end through the public API (pinned H2D of the gap, D2H of p)
+    # end to end through the public API (pinned H2D of the gaps, D2H of the
+    # pressures): the batch call (the headline e2e) and one ContactSolver.solve
+    # per problem
+    warm(step_e2e_many, args.warmup)
+    dtm, _, last_many = timed(step_e2e_many, args.steps)
+    value_e2e = n_solves / dtm
     warm(step_e2e, 1)
     dte, _, _ = timed(step_e2e, args.steps)
-    value_e2e = n_solves / dte
+    value_e2e_single = n_solves / dte
 
     # roofline: the operator apply (row_fwd + col + row_inv), FP32, Ns=2048,
     # free space, timed with CUDA events on the launching stream
@@ -418,47 +441,46 @@ def run_ours(args):
     # log-uniform in [1e-3, 2e-2], tol 1e-6), grouped per (backend, Ns) into
     # batched solves that run concurrently; ranks take LPT bins of the set
     uneven = None
-    if not os.environ.get("BENCH_SKIP_UNEVEN"):
-        from aspher_b200.batch import (Operators, lpt_partition, problem_gap, solve_cost,
-                                       solve_many, uneven_problems)
-        probs_u = uneven_problems()
-        costs = [solve_cost(p["backend"], p["grid_size"]) for p in probs_u]
-        mine = lpt_partition(costs, world)[rank]
-        pu = [probs_u[i] for i in mine]
-        gu = [torch.from_numpy(problem_gap(p)).to(dev) for p in pu]
-        opsu = Operators()
-        solve_many(pu, gu, tol=TOL, float_tol=FLOAT_TOL, polish_tol=POLISH_TOL, operators=opsu)  # warm-up
-        flush.zero_()
-        barrier()
-        u0 = torch.cuda.Event(enable_timing=True)
-        u1 = torch.cuda.Event(enable_timing=True)
-        u0.record()
-        ru = solve_many(pu, gu, tol=TOL, float_tol=FLOAT_TOL, polish_tol=POLISH_TOL, operators=opsu)
-        u1.record()
-        barrier()
-        dtu = u0.elapsed_time(u1) / 1e3
-        nconv = sum(r.status == "converged" for r in ru)
-        if world > 1:
-            t = torch.tensor([dtu], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dtu = float(t.item())
-            t = torch.tensor([nconv], device=dev, dtype=torch.float64)
-            dist.all_reduce(t)
-            nconv = int(t.item())
-        uneven = {"value": len(probs_u) / dtu, "unit": "solves/s", "problems": len(probs_u),
-                  "converged": nconv, "seconds": dtu,
-                  "workload": "96 solves, Ns ~ {256:.4,512:.3,1024:.2,2048:.1}, H ~ U[0.6,0.9], "
-                              "p_nominal log-uniform [1e-3,2e-2], fft/periodic alternating, "
-                              "tol 1e-6 (FP32 to the float floor 2e-5 + FP64 polish to "
-                              "tol/2), grouped batched "
-                              "solves run concurrently"}
-        del opsu
+    from aspher_b200.batch import (Operators, lpt_partition, problem_gap, solve_cost,
+                                   solve_many, uneven_problems)
+    probs_u = uneven_problems()
+    costs = [solve_cost(p["backend"], p["grid_size"]) for p in probs_u]
+    mine = lpt_partition(costs, world)[rank]
+    pu = [probs_u[i] for i in mine]
+    gu = [torch.from_numpy(problem_gap(p)).to(dev) for p in pu]
+    opsu = Operators()
+    solve_many(pu, gu, tol=TOL, float_tol=FLOAT_TOL, polish_tol=POLISH_TOL, operators=opsu)  # warm-up
+    flush.zero_()
+    barrier()
+    u0 = torch.cuda.Event(enable_timing=True)
+    u1 = torch.cuda.Event(enable_timing=True)
+    u0.record()
+    ru = solve_many(pu, gu, tol=TOL, float_tol=FLOAT_TOL, polish_tol=POLISH_TOL, operators=opsu)
+    u1.record()
+    barrier()
+    dtu = u0.elapsed_time(u1) / 1e3
+    nconv = sum(r.status == "converged" for r in ru)
+    if world > 1:
+        t = torch.tensor([dtu], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dtu = float(t.item())
+        t = torch.tensor([nconv], device=dev, dtype=torch.float64)
+        dist.all_reduce(t)
+        nconv = int(t.item())
+    uneven = {"value": len(probs_u) / dtu, "unit": "solves/s", "problems": len(probs_u),
+              "converged": nconv, "seconds": dtu,
+              "workload": "96 solves, Ns ~ {256:.4,512:.3,1024:.2,2048:.1}, H ~ U[0.6,0.9], "
+                          "p_nominal log-uniform [1e-3,2e-2], fft/periodic alternating, "
+                          "tol 1e-6 (FP32 to the float floor 2e-5 + FP64 polish to "
+                          "tol/2), grouped batched "
+                          "solves run concurrently"}
+    del opsu
 
     # large single solve: free-space Ns=8192 (k up to 256 cycles / domain),
     # nested from 256, FP32 with FP64 reductions, tol 1e-6 (the FP32 path
     # certifies 1e-6 here: float floor 1e-6)
     large = None
-    if rank == 0 and not os.environ.get("BENCH_SKIP_LARGE"):
+    if rank == 0:
         # the full-grid run first: it carries the one-off Ns=8192 operator
         # build and context allocation, so the restricted run (config 5) is
         # timed on a built operator
@@ -472,14 +494,14 @@ def run_ours(args):
     # the reference's own backend x precision study (fft rows), same settings
     # and surface law, next to its published CPU wall times
     study = None
-    if rank == 0 and not os.environ.get("BENCH_SKIP_STUDY"):
+    if rank == 0:
         study = precision_study(dev)
 
     # the adjoint (FP32 and FP64 CG), checked against central differences of
     # the FP64 solve
     adj = None
-    if rank == 0 and not os.environ.get("BENCH_SKIP_ADJOINT"):
-        adj = adjoint_check(dev, n_dirs=int(os.environ.get("BENCH_ADJ_DIRS", "64")))
+    if rank == 0:
+        adj = adjoint_check(dev, n_dirs=64)
 
     if rank == 0:
         line = {
@@ -516,7 +538,12 @@ def run_ours(args):
             "accuracy_gate": {"pass": ok, "problems": gate},
             "e2e": {"value": value_e2e, "unit": "solves/s",
                     "h2d_bytes_per_step": 8 * N * len(probs),
-                    "d2h_bytes_per_step": 8 * N * len(probs)},
+                    "d2h_bytes_per_step": 8 * N * len(probs),
+                    "api": "aspher_b200.batch.solve_many (aspher_solve_many) on pinned host "
+                           "gaps, pressures read back to pinned host memory",
+                    "statuses": [r.status for r in last_many],
+                    "single_contact_solver": {"value": value_e2e_single, "unit": "solves/s",
+                                              "api": "ContactSolver.solve per problem"}},
             "roofline": {"bound": "hbm", "kernel": "free-space apply FP32 Ns=2048 "
                          "(row_fwd+col+row_inv)", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
@@ -534,12 +561,11 @@ def run_ours(args):
             "clocks": clocks,
             "wall_s_timed": wall,
             "step_ms": {"batched": step_ms[0], "single_mixed": step_ms[1],
-                        "fp64_gpu": step_ms[2], "e2e": step_ms[3]},
+                        "fp64_gpu": step_ms[2], "e2e": step_ms[3],
+                        "e2e_single": step_ms[4]},
         }
         it64 = [r.iterations for r in last64]
-        line["cpu_baseline"] = (cpu_baseline()
-                                if not os.environ.get("BENCH_SKIP_CPU")
-                                else {"value": None, "sample": "skipped (BENCH_SKIP_CPU)"})
+        line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     for b in list(ops):
         del ops[b]
