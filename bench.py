@@ -489,7 +489,9 @@ def run_ours(args):
         large["full_grid_levels"] = {k: v for k, v in full.items()
                                      if k in ("seconds", "status", "finest_iterations",
                                               "contact_area", "fw_error")}
-        large["full_grid_levels"]["note"] = "includes the Ns=8192 operator build"
+        large["full_grid_levels"]["seconds_runs"] = full["seconds_runs"]
+        large["full_grid_levels"]["note"] = ("the faster of two calls; the first includes the "
+                                             "Ns=8192 operator build")
 
     # the reference's own backend x precision study (fft rows), same settings
     # and surface law, next to its published CPU wall times
@@ -574,11 +576,11 @@ def run_ours(args):
 
 
 def large_single(dev, Ns=8192, pbar=0.005, active=True):
-    """One nested FP32 solve of the free-space Ns=8192 problem with
-    active-set (restricted) levels (operator built and graphs captured by an
-    untimed run at Ns=1024 of the same driver; the timed call includes the
-    Ns=8192 operator build the first time); active=False: the same solve
-    with every level on the full grid."""
+    """Nested FP32 solves of the free-space Ns=8192 problem with active-set
+    (restricted) levels (graphs captured by an untimed run at Ns=1024 of the
+    same driver), two calls, the faster reported (the first call of the
+    process includes the Ns=8192 operator build); active=False: the same
+    solve with every level on the full grid."""
     import torch
     import aspher_b200 as asb
     from aspher_b200.surfaces import self_affine_gap
@@ -591,20 +593,25 @@ def large_single(dev, Ns=8192, pbar=0.005, active=True):
     asb.solve_nested(1024, gs, pbar, **kw)
     torch.cuda.synchronize()
     torch.cuda.empty_cache()  # the earlier legs' cached blocks back to the driver
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    r = asb.solve_nested(Ns, g, pbar, **kw)
-    e1.record()
-    torch.cuda.synchronize()
+    secs = []
+    for _ in range(2):  # the faster of two calls (see precision_study)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        r = asb.solve_nested(Ns, g, pbar, **kw)
+        e1.record()
+        torch.cuda.synchronize()
+        secs.append(e0.elapsed_time(e1) / 1e3)
     return {"workload": "free-space Ns=8192, H=0.8, k in [4,256] cycles/domain, rms 0.002, "
                         "p_nominal 0.005, nested from 256, FP32 (FP64 reductions), tol 1e-6, "
                         + ("active-set levels" if active else "full-grid levels"),
-            "seconds": e0.elapsed_time(e1) / 1e3, "status": r.status,
+            "seconds": min(secs), "seconds_runs": secs, "status": r.status,
             "active_rounds": r.active_rounds, "active_fallback": r.active_fallback,
             "finest_iterations": r.iterations, "fw_error": r.fw_error,
             "penetration_error": r.penetration_error, "contact_area": r.contact_area,
-            "stages": [[st["name"], st["iterations"], st["seconds"]] for st in r.stage_stats]}
+            "stages": [[st["name"], st["iterations"], st["seconds"]] for st in r.stage_stats],
+            "seconds_in_stages": sum(st["seconds"] for st in r.stage_stats),
+            "seconds_building_operators": r.time_build}
 
 
 # the reference's published fft rows of its backend x precision study
@@ -658,11 +665,19 @@ def precision_study(dev, sizes=(2048, 4096, 8192), float_sizes=(2048, 4096, 8192
     rows = []
     for precision in ("double", "float"):
         for Ns in (sizes if precision == "double" else float_sizes):
-            sec, r = run(Ns, precision)
+            # wall time of a host-driven call: the faster of two runs (a
+            # shared host adds its own stalls to some calls)
+            sec0, r0 = run(Ns, precision)
+            del r0
+            sec1, r = run(Ns, precision)
+            sec = min(sec0, sec1)
             ref = STUDY_REF.get((precision, Ns))
             refd = ({"seconds": ref[0], "iterations": ref[1], "contact_area": ref[2]}
                     if ref is not None else {"status": STUDY_REF_FAILED.get((precision, Ns))})
-            rows.append({"precision": precision, "Ns": Ns, "seconds": sec, "status": r.status,
+            rows.append({"precision": precision, "Ns": Ns, "seconds": sec,
+                         "seconds_runs": [sec0, sec1],
+                         "seconds_in_stages": sum(st["seconds"] for st in r.stage_stats),
+                         "status": r.status,
                          "iterations": r.iterations, "final_error": r.error,
                          "contact_area": r.contact_area, "reference_cpu": refd})
             del r
