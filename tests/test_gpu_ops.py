@@ -102,21 +102,23 @@ def test_periodic_matches_oracle(Ns):
     assert rel(_mv(op, x32, torch.float32), ref_op.matvec(x32.astype(np.float64))) < 2e-6
 
 
-def test_periodic_matrix_properties_and_alias():
-    """test_periodic.cpp:56-88: symmetric, PSD, circulant; x == y aliasing."""
-    n = 16
+@pytest.mark.parametrize("n", [7, 12, 16])
+def test_periodic_matrix_properties_and_alias(n):
+    """test_periodic.cpp:53-88 on its grids (7 and 12 run embedded, as the
+    circulant of the Nl torus inside a power-of-two free-space pipeline):
+    symmetric, PSD, circulant, null space = constants; x == y aliasing."""
     op = _op("periodic", n, 1.7, 0.8)
     N = n * n
     E = torch.eye(N, dtype=torch.float64, device="cuda")
     S = np.zeros((N, N))
     y = torch.empty(N, dtype=torch.float64, device="cuda")
     for j in range(N):
-        op.matvec_(E[j].contiguous(), y)
+        op.matvec_(E[j].clone(), y)  # a fresh (aligned) buffer: rows of E sit at 8 N j bytes
         S[:, j] = y.cpu().numpy()
     assert np.linalg.norm(S - S.T) / np.linalg.norm(S) < 1e-14
     ev = np.linalg.eigvalsh(S)
     assert ev[0] > -1e-13 * ev[-1] and ev[1] > 1e-6 * ev[-1]
-    sx, sy = 3, 5
+    sx, sy = 3 % n, 5 % n
     for iy in range(n):
         for ix in range(n):
             a = iy * n + ix
@@ -127,6 +129,23 @@ def test_periodic_matrix_properties_and_alias():
     op.matvec_(x, ref)
     op.matvec_(x, x)  # aliased
     assert torch.linalg.norm(x - ref) <= 1e-15 * torch.linalg.norm(ref)
+    xf = torch.as_tensor(np.random.default_rng(0).standard_normal(N), device="cuda")
+    xf = xf.float()
+    op.matvec_(xf, xf)  # aliased, float
+    assert torch.linalg.norm(xf.double() - ref) < 2e-6 * torch.linalg.norm(ref)
+
+
+def test_periodic_modes_exact_odd_grid():
+    """test_periodic.cpp:16-36 on an odd grid (embedded): a cosine mode is an
+    eigenvector with eigenvalue 2 / (E* |q|); constants map to 0."""
+    n, L, Es = 27, 3.0, 2.5
+    op = _op("periodic", n, L, Es)
+    ix = np.arange(n)
+    for mx, my in ((1, 0), (0, 3), (2, 5)):
+        q = 2 * np.pi * np.hypot(mx, my) / L
+        p = np.cos(2 * np.pi * (mx * ix[None, :] + my * ix[:, None]) / n).ravel()
+        assert rel(_mv(op, p, torch.float64), 2.0 / (Es * q) * p) < 2e-13
+    assert np.linalg.norm(_mv(op, np.ones(n * n), torch.float64)) < 1e-13
 
 
 @pytest.mark.parametrize("kind,radius", [("stencil", 1), ("stencil", 2), ("stencil", 3),
