@@ -152,6 +152,19 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# the tangential solve leg: grid, rigid shift and threshold field
+TAN_NS = 256
+TAN_SHIFT = (2e-3, -1e-3)
+
+
+def tangential_threshold(Ns, mu=0.3, a2=0.09):
+    """s = mu p on a Hertz-like pressure disk (open cells outside)."""
+    import numpy as np
+    x = (np.arange(Ns) + 0.5) / Ns - 0.5
+    r2 = x[None, :] ** 2 + x[:, None] ** 2
+    return mu * np.sqrt(np.maximum(0.0, a2 - r2)).ravel()
+
+
 def problem_gaps(Ns, rank):
     from aspher_b200.surfaces import self_affine_gap
     g = self_affine_gap(Ns, hurst=0.8, rms=0.002, k_lo=4.0, k_hi=64.0, seed=SEED + 1000 * rank)
@@ -412,6 +425,24 @@ def run_ours(args):
                             "frac": tbytes / tm / 1e9 / peak}
         del qs, us
     del top
+    # the tangential projected CG (displacement control, FP64) at Ns=256 on
+    # a Hertz-like threshold field: the faster of two solves; the CPU
+    # baseline times the reference's own solve_tangential on it
+    ttop = asb.TangentialOperator(TAN_NS)
+    s_tan = tangential_threshold(TAN_NS)
+    tsec = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        _, tres = ttop.solve(s_tan, force_control=False, target=TAN_SHIFT, tol=1e-8,
+                             max_iter=20000)
+        tsec.append(time.perf_counter() - t0)
+    tangential["solve"] = {"workload": "solve_tangential, displacement control (shift %g, %g), "
+                                       "Ns=%d, threshold 0.3 sqrt(0.09 - r^2), tol 1e-8, FP64"
+                                       % (TAN_SHIFT[0], TAN_SHIFT[1], TAN_NS),
+                           "seconds": min(tsec), "status": tres["status"],
+                           "iterations": tres["iterations"], "n_stick": tres["n_stick"],
+                           "n_slip": tres["n_slip"]}
+    del ttop
 
     # whole-solve roofline: modelled bytes of every PCG iteration over the
     # timed solve time.  FP32 stage: 2 B_op (12 b N free space, 6 b N
@@ -906,6 +937,23 @@ class CpuSampler:
                 "reference's own iteration count" % (what, self.cores, self.n1, self.n2))
 
 
+def _cpu_tangential_solve():
+    """The reference's own solve_tangential (oracle/_ref) on the tangential
+    leg's problem, timed once on the host threads; None where the reference
+    library is not built."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    t = ref.Tangential(TAN_NS)
+    s = tangential_threshold(TAN_NS)
+    t0 = time.perf_counter()
+    _, d = t.solve(s, False, TAN_SHIFT, tol=1e-8, max_iter=20000)
+    return {"seconds": time.perf_counter() - t0, "status": d["status"],
+            "iterations": d["iterations"], "threads": ref.threads(),
+            "workload": "the tangential leg's solve (Ns=%d) on the reference's own C++"
+                        % TAN_NS}
+
+
 def cpu_baseline(**_unused):
     """The CPU baseline of our arm's line (rank 0, N = 1): one sampling pass
     over the six problems and one complete solve of the cheapest (about
@@ -922,7 +970,7 @@ def cpu_baseline(**_unused):
         sec = cs.workload_seconds()
         return {"value": len(BACKENDS) * len(LOADS) / sec, "unit": "solves/s",
                 "cores": cs.cores, "kind": cs.kind, "sample": cs.describe(),
-                "validation": val}
+                "validation": val, "tangential_solve": _cpu_tangential_solve()}
     except Exception as e:  # the baseline must never sink the GPU line
         return {"value": None, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                 "sample": "unavailable: %s" % e}
