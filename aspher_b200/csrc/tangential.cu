@@ -25,6 +25,7 @@
 // and written once per pass.  q and u may alias (q is consumed by the first
 // pass before u is written).
 #include "../../include/aspher_b200.h"
+#include "embed.cuh"
 #include "fft_kernels.cuh"
 #include "fft_launch.cuh"
 #include "functors.cuh"
@@ -217,8 +218,20 @@ col_pair_kernel(cplx<T>* __restrict__ spec, long bsp, int nrows, TanMix<T> mix,
 }  // namespace
 
 struct TanOperator {
-    int Ns = 0;
+    // Ns: the compute grid (a power of two in [16, 2048]); Nl: the caller's
+    // side.  Nl < Ns (a side that is not a power of two >= 16) runs
+    // embedded: the caller's cells are the top-left block of the compute
+    // grid, the Cerruti tables at the caller's cell size L / Nl, so the
+    // padded convolution of a field that is zero outside the block is the
+    // tangential operator of the Nl grid on the block
+    int Ns = 0, Nl = 0;
     double L = 1.0, E = 1.0, nu = 0.3;
+    bool embedded() const { return Nl != Ns; }
+    // embedded: two-field compute-grid scratch of the caller-facing apply
+    void* emb_q = nullptr;
+    void* emb_u = nullptr;
+    // caller-facing apply: q, u hold 2 Nl^2 values
+    void apply_caller(bool dbl, const void* q, void* u, cudaStream_t s);
     int device = 0;
     double max_im_ratio = 0.0;
     double* tab_xx = nullptr;  // FP64 tables [dy][dx], dx, dy in [0, Ns)
@@ -323,10 +336,14 @@ void TanOperator::build() {
     }
 
 TanOperator::TanOperator(int Ns_, double L_, double E_, double nu_)
-    : Ns(Ns_), L(L_), E(E_), nu(nu_) {
-    if (!is_pow2(Ns) || Ns < 16 || Ns > kTanMaxNs)
-        throw Error(ASPHER_EINVAL, "tangential operator: grid_size must be a power of two in "
-                                   "[16, 2048]");
+    : Ns(Ns_), Nl(Ns_), L(L_), E(E_), nu(nu_) {
+    if (Nl < 2 || Nl > kTanMaxNs)
+        throw Error(ASPHER_EINVAL, "tangential operator: grid_size must be in [2, 2048]");
+    if (!is_pow2(Nl) || Nl < 16) {  // embedded in the next power of two
+        int nc = 16;
+        while (nc < Nl) nc *= 2;
+        Ns = nc;
+    }
     if (!(L > 0.0) || !std::isfinite(L)) throw Error(ASPHER_EINVAL, "domain_size must be positive");
     if (!(E > 0.0) || !std::isfinite(E)) throw Error(ASPHER_EINVAL, "E_star must be positive");
     if (!(nu >= 0.0 && nu < 1.0)) throw Error(ASPHER_EINVAL, "nu must be in [0, 1)");
@@ -338,8 +355,9 @@ TanOperator::TanOperator(int Ns_, double L_, double E_, double nu_)
         ASB_CUDA(cudaMalloc(&tab_xx, n * sizeof(double)));
         ASB_CUDA(cudaMalloc(&tab_xy, n * sizeof(double)));
         // CerrutiKernel (cerruti_kernel.cpp:114-128): h = L / Ns, a = h / 2,
-        // prefactors 1 / (pi E* (1 - nu)) and nu times it
-        const double h = L / Ns, pref = 1.0 / (M_PI * E * (1.0 - nu));
+        // prefactors 1 / (pi E* (1 - nu)) and nu times it (h = L / Nl: the
+        // caller's cell size; tables for offsets up to the compute grid)
+        const double h = L / Nl, pref = 1.0 / (M_PI * E * (1.0 - nu));
         k_cerruti_tables<<<592, 256>>>(tab_xx, tab_xy, Ns, h, pref, nu * pref, nu);
         ASB_CUDA(cudaGetLastError());
         ASB_TAN_SIZE_SWITCH(Ns, build<NS>());
@@ -356,6 +374,9 @@ void TanOperator::release() {
     cudaFree(tab_xx);
     cudaFree(tab_xy);
     tab_xx = tab_xy = nullptr;
+    cudaFree(emb_q);
+    cudaFree(emb_u);
+    emb_q = emb_u = nullptr;
     for (int d = 0; d < 2; ++d) {
         for (int j = 0; j < 3; ++j) {
             cudaFree(kt[d][j]);
@@ -399,6 +420,35 @@ void TanOperator::matvec(bool dbl, const void* q, void* u, cudaStream_t s) {
     } else {
         ASB_TAN_SIZE_SWITCH(Ns, (apply<float, NS>((const float*)q, (float*)u, s)));
     }
+}
+
+void TanOperator::apply_caller(bool dbl, const void* q, void* u, cudaStream_t s) {
+    if (!embedded()) {
+        matvec(dbl, q, u, s);
+        return;
+    }
+    const long n = (long)Ns * Ns, nl = (long)Nl * Nl;
+    if (!emb_q) {
+        std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+        ASB_CUDA(cudaMalloc(&emb_q, 2 * n * sizeof(double)));
+        ASB_CUDA(cudaMalloc(&emb_u, 2 * n * sizeof(double)));
+    }
+    if (dbl) {
+        k_embed<double, double><<<embed_grid(2 * n), 256, 0, s>>>(Nl, Ns, 2, (const double*)q,
+                                                                  (double*)emb_q, 0.0);
+        matvec(true, emb_q, emb_u, s);
+        k_extract<double, double><<<embed_grid(2 * nl), 256, 0, s>>>(Nl, Ns, 2,
+                                                                     (const double*)emb_u,
+                                                                     (double*)u);
+    } else {
+        k_embed<float, float><<<embed_grid(2 * n), 256, 0, s>>>(Nl, Ns, 2, (const float*)q,
+                                                                (float*)emb_q, 0.0f);
+        matvec(false, emb_q, emb_u, s);
+        k_extract<float, float><<<embed_grid(2 * nl), 256, 0, s>>>(Nl, Ns, 2,
+                                                                   (const float*)emb_u, (float*)u);
+    }
+    count_launches(2);
+    ASB_CUDA(cudaGetLastError());
 }
 
 }  // namespace asb
@@ -664,13 +714,15 @@ __global__ void __launch_bounds__(kTanThreads) k_tan_kkt(
 }
 
 // [0] max s, [1] max |u_x| over the first N (the compliance scale of q = (s, 0))
-__global__ void __launch_bounds__(kTanThreads) k_tan_scales(long N, const double* __restrict__ s,
+// on the caller's Nl x Nl block of the Ns x Ns grid
+__global__ void __launch_bounds__(kTanThreads) k_tan_scales(long N, int Nl, int Ns,
+                                                            const double* __restrict__ s,
                                                             const double* __restrict__ u,
                                                             double* part) {
     double v[2] = {0.0, 0.0};
     TAN_LOOP(N) {
         v[0] = fmax(v[0], s[i]);
-        v[1] = fmax(v[1], fabs(u[i]));
+        if (Nl == Ns || (i / Ns < Nl && i % Ns < Nl)) v[1] = fmax(v[1], fabs(u[i]));
     }
     const int kind[2] = {1, 1};
     tan_block_out<2>(v, kind, part);
@@ -745,9 +797,13 @@ struct TanSolver {
     const double* s = nullptr;
     const double* hist = nullptr;
     double Stotal = 0.0;
+    // the caller's cell count (mean tractions, open cells); N for the
+    // operator's own grid, Nl^2 for an embedded one
+    double ncells = 0.0;
 
     TanSolver(TanOperator& o, cudaStream_t s_) : op(o), st(s_) {
         N = (long)op.Ns * op.Ns;
+        ncells = (double)op.Nl * (double)op.Nl;
         grid = (int)std::min<long>(kTanMaxBlocks, (N + kTanThreads - 1) / kTanThreads);
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         double** vs[] = {&q, &u, &g, &gp, &z, &t, &r, &qbest, &qw};
@@ -858,11 +914,13 @@ struct TanSolver {
         k_tan_classify<<<grid, kTanThreads, 0, st>>>(N, s, q, part);
         count_launches(1);
         const double* c = fold(5, {0, 0, 0, 0, 0});
-        res.q_mean.x = c[0] / N;
-        res.q_mean.y = c[1] / N;
+        res.q_mean.x = c[0] / ncells;
+        res.q_mean.y = c[1] / ncells;
         res.n_stick = (int)c[2];
         res.n_slip = (int)c[3];
-        res.n_open = (int)c[4];
+        // the cells outside an embedded grid's block are open (s = 0) and
+        // not the caller's
+        res.n_open = (int)(c[4] - ((double)N - ncells));
     }
 };
 
@@ -870,10 +928,11 @@ struct TanSolver {
 
 // solve_tangential (friction_solve.cpp:375-688) with the local KKT check of
 // check_tangential_kkt (:309-371); q_out receives the returned traction.
-void solve_tangential(TanOperator& op, const double* s, bool force_control, double tx,
-                      double ty, double tol, int max_iter, bool use_pr, double kkt_tol,
-                      const double* q_init, const double* u_hist, double* q_out,
-                      aspher_tan_result& out, cudaStream_t st) {
+// Fields in the operator's compute-grid layout (see solve_tangential).
+void solve_tangential_core(TanOperator& op, const double* s, bool force_control, double tx,
+                           double ty, double tol, int max_iter, bool use_pr, double kkt_tol,
+                           const double* q_init, const double* u_hist, double* q_out,
+                           aspher_tan_result& out, cudaStream_t st) {
     const long N = (long)op.Ns * op.Ns;
     TanSolver S(op, st);
     S.s = s;
@@ -904,7 +963,7 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
         // check_tangential_kkt: rho from the operator's own compliance scale
         k_tan_sfield<<<S.grid, kTanThreads, 0, st>>>(N, s, S.z);
         S.apply(S.z, S.r);
-        k_tan_scales<<<S.grid, kTanThreads, 0, st>>>(N, s, S.r, S.part);
+        k_tan_scales<<<S.grid, kTanThreads, 0, st>>>(N, op.Nl, op.Ns, s, S.r, S.part);
         count_launches(2);
         const double* sc = S.fold(2, {1, 1});
         const double s_ref = std::max(sc[0], 1e-300), w_ref = std::max(sc[1], 1e-300);
@@ -918,7 +977,7 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
         out.stick_residual = k[1];
         out.slip_residual = k[2];
         out.proj_residual = k[3];
-        const V2 qm{k[4] / N, k[5] / N};
+        const V2 qm{k[4] / S.ncells, k[5] / S.ncells};
         out.force_error = force_control ? v2norm({qm.x - target.x, qm.y - target.y}) / s_ref : 0.0;
         out.rho = rho;
         out.s_ref = s_ref;
@@ -962,7 +1021,7 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
     }
 
     // force control (friction_solve.cpp:460-688)
-    const double q_limit = S.Stotal / N;
+    const double q_limit = S.Stotal / S.ncells;
     if (v2norm(target) >= q_limit)
         throw Error(ASPHER_EINVAL, "solve_tangential: |q_bar| >= mean(s) -- at or beyond the "
                                    "gross-slip limit, no equilibrium exists");
@@ -979,7 +1038,7 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
     {
         k_tan_sfield<<<S.grid, kTanThreads, 0, st>>>(N, s, S.z);
         S.apply(S.z, S.r);
-        k_tan_scales<<<S.grid, kTanThreads, 0, st>>>(N, s, S.r, S.part);
+        k_tan_scales<<<S.grid, kTanThreads, 0, st>>>(N, op.Nl, op.Ns, s, S.r, S.part);
         count_launches(2);
         const double u_scale = S.fold(2, {1, 1})[1];
         if (u_scale <= 0.0)
@@ -1092,9 +1151,10 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
             k_tan_loadsums<<<S.grid, kTanThreads, 0, st>>>(N, s, S.q, S.part);
             count_launches(1);
             const double* ls = S.fold(3, {0, 0, 0});
-            const double cx = target.x * N - ls[0], cy = target.y * N - ls[1];
+            const double cx = target.x * S.ncells - ls[0], cy = target.y * S.ncells - ls[1];
             const double ni = ls[2];
-            if (ni <= 0.0 || (std::abs(cx) + std::abs(cy)) <= 1e-14 * N * target_scale) break;
+            if (ni <= 0.0 || (std::abs(cx) + std::abs(cy)) <= 1e-14 * S.ncells * target_scale)
+                break;
             k_tan_loadfix<<<S.grid, kTanThreads, 0, st>>>(N, s, cx / ni, cy / ni, S.q);
             count_launches(1);
         }
@@ -1105,6 +1165,57 @@ void solve_tangential(TanOperator& op, const double* s, bool force_control, doub
         else best.reason.clear();
         finish(best, delta_best, total_it);
     }
+}
+
+// The caller's fields (s: Nl^2 thresholds; q_init, u_hist, q_out: 2 Nl^2)
+// around the core: for an embedded operator they are copied into
+// compute-grid fields whose cells outside the caller's block have s = 0
+// (open: the solve never gives them traction, as the reference never does
+// an open cell) and zero warm start and history, and the traction's block is
+// copied back.
+void solve_tangential(TanOperator& op, const double* s, bool force_control, double tx,
+                      double ty, double tol, int max_iter, bool use_pr, double kkt_tol,
+                      const double* q_init, const double* u_hist, double* q_out,
+                      aspher_tan_result& out, cudaStream_t st) {
+    if (!op.embedded()) {
+        solve_tangential_core(op, s, force_control, tx, ty, tol, max_iter, use_pr, kkt_tol,
+                              q_init, u_hist, q_out, out, st);
+        return;
+    }
+    const long n = (long)op.Ns * op.Ns;
+    std::vector<double*> bufs;
+    auto alloc = [&](long count) {
+        double* p = nullptr;
+        ASB_CUDA(cudaMallocAsync((void**)&p, (size_t)count * sizeof(double), st));
+        bufs.push_back(p);
+        return p;
+    };
+    auto embed = [&](const double* src, int fields) -> const double* {
+        if (!src) return nullptr;
+        double* d = alloc(fields * n);
+        k_embed<double, double><<<embed_grid(fields * n), 256, 0, st>>>(op.Nl, op.Ns, fields,
+                                                                         src, d, 0.0);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+        return d;
+    };
+    try {
+        const double* sc = embed(s, 1);
+        const double* qi = embed(q_init, 2);
+        const double* uh = embed(u_hist, 2);
+        double* qc = alloc(2 * n);
+        solve_tangential_core(op, sc, force_control, tx, ty, tol, max_iter, use_pr, kkt_tol, qi,
+                              uh, qc, out, st);
+        k_extract<double, double><<<embed_grid(2 * (long)op.Nl * op.Nl), 256, 0, st>>>(
+            op.Nl, op.Ns, 2, qc, q_out);
+        count_launches(1);
+        ASB_CUDA(cudaGetLastError());
+    } catch (...) {
+        for (double* p : bufs) cudaFreeAsync(p, st);
+        throw;
+    }
+    for (double* p : bufs) cudaFreeAsync(p, st);
+    ASB_CUDA(cudaStreamSynchronize(st));
 }
 
 }  // namespace asb
@@ -1155,7 +1266,8 @@ int aspher_tan_matvec(aspher_tan_op* op, int dtype, const void* q_dev, void* u_d
             throw asb::Error(ASPHER_EINVAL, "aspher_tan_matvec: buffers must be 16-byte aligned");
         if (dtype != ASPHER_F32 && dtype != ASPHER_F64)
             throw asb::Error(ASPHER_EINVAL, "aspher_tan_matvec: dtype must be F32 or F64");
-        op->impl->matvec(dtype == ASPHER_F64, q_dev, u_dev, static_cast<cudaStream_t>(stream));
+        op->impl->apply_caller(dtype == ASPHER_F64, q_dev, u_dev,
+                               static_cast<cudaStream_t>(stream));
         return ASPHER_OK;
     } catch (const asb::Error& e) {
         asb::set_last_error(e.what());
@@ -1208,8 +1320,9 @@ int aspher_tan_tables(const aspher_tan_op* op, double* xx_host, double* yy_host,
     try {
         if (!op || !op->impl || !xx_host || !yy_host || !xy_host)
             throw asb::Error(ASPHER_EINVAL, "aspher_tan_tables: NULL argument");
-        const int Ns = op->impl->Ns;
-        std::vector<double> xx((size_t)Ns * Ns), xy((size_t)Ns * Ns);
+        // the caller's offsets |d| < Nl of the tables (pitch: the compute grid)
+        const int Ns = op->impl->Nl, P = op->impl->Ns;
+        std::vector<double> xx((size_t)P * P), xy((size_t)P * P);
         ASB_CUDA(cudaMemcpy(xx.data(), op->impl->tab_xx, xx.size() * sizeof(double),
                             cudaMemcpyDeviceToHost));
         ASB_CUDA(cudaMemcpy(xy.data(), op->impl->tab_xy, xy.size() * sizeof(double),
@@ -1219,9 +1332,9 @@ int aspher_tan_tables(const aspher_tan_op* op, double* xx_host, double* yy_host,
             for (int dx = -(Ns - 1); dx < Ns; ++dx) {
                 const int ax = dx < 0 ? -dx : dx, ay = dy < 0 ? -dy : dy;
                 const size_t at = (size_t)(dy + Ns - 1) * W + (dx + Ns - 1);
-                xx_host[at] = xx[(size_t)ay * Ns + ax];
-                yy_host[at] = xx[(size_t)ax * Ns + ay];
-                const double v = xy[(size_t)ay * Ns + ax];
+                xx_host[at] = xx[(size_t)ay * P + ax];
+                yy_host[at] = xx[(size_t)ax * P + ay];
+                const double v = xy[(size_t)ay * P + ax];
                 xy_host[at] = (dx == 0 || dy == 0) ? 0.0 : (((dx > 0) == (dy > 0)) ? v : -v);
             }
         return ASPHER_OK;

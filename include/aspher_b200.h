@@ -371,7 +371,9 @@ typedef struct aspher_tan_op aspher_tan_op;
  * src/cerruti_kernel.cpp:114-128, src/tangential_operator.cpp:18-77): the
  * Cerruti tables and their three real spectra built on the device in FP64,
  * with the reference's realness check (ASPHER_EBUILD when it fails).
- * grid_size: a power of two in [16, 2048]; nu in [0, 1).  Synchronous. */
+ * grid_size in [2, 2048] (one that is not a power of two >= 16 runs
+ * embedded in the next power of two, as for aspher_op_create; every entry
+ * point still takes 2 grid_size^2 fields); nu in [0, 1).  Synchronous. */
 int aspher_tan_create(int grid_size, double domain_size, double E_star, double nu,
                       aspher_tan_op** out);
 int aspher_tan_destroy(aspher_tan_op* op);

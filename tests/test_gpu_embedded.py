@@ -153,3 +153,26 @@ def test_embedded_rejects_what_needs_a_power_of_two():
         Operator("fft", 1)
     with pytest.raises(ValueError):
         Operator("periodic", 16385)
+
+
+def test_embedded_warm_start_and_history():
+    """p_init on an embedded grid: the caller's Nl^2 warm start (the
+    converged pressure) is embedded with zero outside the block; the solve
+    restarts at the optimum (the reference's test_certification.cpp:76-148
+    warm start) and keeps its certificate; the error history has one entry
+    per iteration."""
+    from aspher_b200 import ContactSolver
+    Ns, pbar, tol = 60, 0.005, 1e-8
+    g0 = _gap(Ns)
+    s = ContactSolver(Ns, backend="fft")
+    r = s.solve(g0, pbar, tol, precond="fourier")
+    assert r.status == "converged"
+    w = s.solve(g0, pbar, tol, precond="fourier", p_init=np.asarray(r.pressure))
+    assert w.status == "converged"
+    assert w.iterations <= 2
+    assert _rel(w.pressure, r.pressure) <= 10 * tol
+    from aspher_b200 import Operator, solve_device
+    op = Operator("periodic", 45)
+    g = torch.as_tensor(_gap(45), device="cuda")
+    h = solve_device(op, g, pbar, tol=tol, record_history=True, precond="fourier")
+    assert h.status == "converged" and len(h.error_history) == h.iterations

@@ -200,3 +200,74 @@ def test_tangential_solve_rejects():
         op.solve(-s, target=(1e-3, 0.0))
     with pytest.raises(ValueError, match="everywhere"):
         op.solve(np.zeros(Ns * Ns), target=(1e-3, 0.0))
+
+
+@pytest.mark.parametrize("Ns", [5, 12, 37, 100])
+def test_tangential_embedded_grid_matches_reference(Ns):
+    """Grids that are not powers of two (the reference's TangentialFFTOperator
+    takes any Ns): the caller's block inside the next power of two's
+    pipeline, the Cerruti tables at the caller's cell size.  Against the
+    dense block of the reference's own tables (FP64 1e-13, FP32 1e-5) and
+    the reference's own apply where it is built."""
+    from aspher_b200 import TangentialOperator
+    L, E, nu = 1.3, 0.9, 0.25
+    op = TangentialOperator(Ns, L, E, nu)
+    if ref.available():
+        tabs = ref.cerruti_tables(Ns, L, E, nu)
+    else:
+        C = CerrutiKernel(Ns, L, E, nu)
+        d = np.arange(-(Ns - 1), Ns)
+        tabs = C.offsets(d[None, :], d[:, None])
+    got_tabs = op.tables()
+    scale = np.max(np.abs(tabs[0]))
+    for a, b in zip(got_tabs, tabs):
+        assert np.max(np.abs(a - b)) <= 1e-14 * scale
+    D = _dense_from_tables(Ns, *tabs)
+    q = np.random.default_rng(3 + Ns).uniform(-1, 1, 2 * Ns * Ns)
+    want = D @ q
+    assert _rel(op.matvec(q), want) < 1e-13
+    q32 = torch.as_tensor(q, dtype=torch.float32, device="cuda")
+    u32 = torch.empty_like(q32)
+    op.matvec_(q32, u32)
+    assert _rel(u32.double().cpu().numpy(), want) < 1e-5
+    if ref.available():
+        assert _rel(op.matvec(q), ref.Tangential(Ns, L, E, nu).matvec(q)) < 1e-13
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("mode", ["displacement", "force"])
+def test_tangential_embedded_solve_matches_reference(mode):
+    """solve_tangential on a 40 x 40 grid (embedded in 64): the cells outside
+    the caller's block are open (s = 0), the mean traction and the cell
+    counts are the caller's.  Displacement control: traction to 1e-6; force
+    control: at the reference's acceptance (see
+    test_tangential_solve_matches_reference); the warm chain step by step."""
+    from aspher_b200 import TangentialOperator
+    Ns = 40
+    s = _hertz_threshold(Ns)
+    op = TangentialOperator(Ns)
+    if mode == "displacement":
+        fc, target = False, (2e-3, -1e-3)
+    else:
+        fc, target = True, (0.3 * s.mean(), 0.1 * s.mean())
+    qr, dr = ref.Tangential(Ns).solve(s, fc, target, tol=1e-8, max_iter=5000)
+    q, d = op.solve(s, force_control=fc, target=target, tol=1e-8, max_iter=5000)
+    assert q.shape == (2 * Ns * Ns,)
+    assert dr["status"] == "converged" and d["status"] == "converged", d
+    assert d["n_stick"] + d["n_slip"] + d["n_open"] == Ns * Ns
+    assert d["n_open"] == dr["n_open"]
+    assert abs(d["n_stick"] - dr["n_stick"]) <= 3
+    assert d["cone_violation"] <= 1e-9 and d["proj_residual"] <= d["kkt_tol"]
+    assert abs(d["w_ref"] - dr["w_ref"]) <= 1e-12 * dr["w_ref"]
+    if fc:
+        assert _rel(q, qr) <= 1e-2
+        assert abs(d["q_mean"][0] - target[0]) <= 1e-12 * abs(target[0])
+        assert abs(d["delta_t"][0] - dr["delta_x"]) <= 1e-3 * abs(dr["delta_x"])
+    else:
+        assert _rel(q, qr) <= 1e-6
+        delta = (target[0] * 1.0001, target[1])
+        qr2, dr2 = ref.Tangential(Ns).solve(s, False, delta, tol=1e-8, max_iter=5000, q_init=qr)
+        q2, d2 = op.solve(s, force_control=False, target=delta, tol=1e-8, max_iter=5000,
+                          q_init=qr)
+        assert d2["iterations"] == dr2["iterations"]
+        assert _rel(q2, qr2) <= 1e-12
