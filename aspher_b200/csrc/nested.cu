@@ -353,9 +353,9 @@ void active_level(Operator& op, const aspher_solve_opts& o, bool level_float, co
             if (level_float) {
                 k_cast_f32<<<gb, 256, 0, s>>>(n2, p_out, p32);
                 count_launches(1);
-                op.matvec(false, p32, u, s);
+                op.apply_caller(false, p32, u, s);
             } else {
-                op.matvec(true, p_out, u, s);
+                op.apply_caller(true, p_out, u, s);
             }
             const double a = rr.approach - datum;  // centred approach
             if (level_float)
@@ -509,10 +509,15 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
     for (int n = np.coarsest; n <= Ns; n *= 2) levels.push_back(n);
     if (levels.empty() || levels.back() != Ns)
         throw Error(ASPHER_EINVAL, "solve_contact_nested: Ns must equal coarsest * 2^k");
-    for (int n : levels)
-        if (!pow2(n) || n < 16)
-            throw Error(ASPHER_EINVAL, "solve_contact_nested: every level must be a power of two "
-                                       ">= 16 on this device path");
+    // levels that are not powers of two >= 16 run on embedded operators;
+    // the FFT preconditioner engine needs power-of-two levels
+    const int engine0 = (kind == OP_PERIODIC && np.precond_engine == 0) ? 2 : np.precond_engine;
+    for (int n : levels) {
+        if (n > kMaxNs) throw Error(ASPHER_EINVAL, "solve_contact_nested: Ns must be <= 16384");
+        if (np.precond && engine0 == 2 && (!pow2(n) || n < 16))
+            throw Error(ASPHER_EINVAL, "solve_contact_nested: the fft preconditioner engine needs "
+                                       "power-of-two levels >= 16 (use precond_engine='stencil')");
+    }
     if (np.active_set && levels.size() < 2)
         throw Error(ASPHER_EINVAL, "solve_contact_nested: active_set needs a coarse level "
                                    "(Ns > coarsest)");
@@ -578,8 +583,11 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
             std::shared_ptr<Operator> op = cached_operator(kind, n, L, E);
             // periodic: `auto` means the FFT engine (nested_solve.cpp:717-721)
             const int engine = (kind == OP_PERIODIC && np.precond_engine == 0) ? 2 : np.precond_engine;
-            const bool use_stencil = stencil_for_level(engine, np.precond != 0, prev_occupancy,
-                                                       np.precond_occupancy_max);
+            bool use_stencil = stencil_for_level(engine, np.precond != 0, prev_occupancy,
+                                                 np.precond_occupancy_max);
+            // an embedded level has no FFT preconditioner: under `auto` it
+            // keeps the stencil where the reference would switch
+            if (!use_stencil && np.precond && engine == 0 && op->embedded()) use_stencil = true;
             const int r_lvl = std::min({np.precond_radius, std::max(1, n / 4), np.leaf_side});
             const int pc = use_stencil ? ASPHER_PRECOND_STENCIL
                                        : (np.precond ? ASPHER_PRECOND_FFT : ASPHER_PRECOND_NONE);
