@@ -2526,11 +2526,9 @@ __global__ void __launch_bounds__(kRedThreads, kRedMinBlocks) k_adj_out(const Pk
 }  // namespace
 
 template <typename T>
-void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
+void adjoint_core(Operator& op, const double* p, const double* w, double tol, int max_iter,
                   int precond, int radius, double* grad_g0, double* grad_pbar,
                   aspher_adjoint_info* info, cudaStream_t s) {
-    if (op.embedded())
-        throw Error(ASPHER_EINVAL, "adjoint needs a power-of-two grid_size in [16, 16384]");
     if (!(tol > 0.0)) throw Error(ASPHER_EINVAL, "adjoint: tol must be positive");
     if (max_iter < 1) throw Error(ASPHER_EINVAL, "adjoint: max_iter must be >= 1");
     if (precond != ASPHER_PRECOND_NONE && precond != ASPHER_PRECOND_STENCIL)
@@ -2539,7 +2537,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     const long N = (long)op.Ns * op.Ns;
     const size_t vb = (size_t)N * sizeof(T);
     StencilW W{};
-    if (precond == ASPHER_PRECOND_STENCIL) W = stencil_weights(make_stencil_taps(op.Ns, radius));
+    if (precond == ASPHER_PRECOND_STENCIL) W = stencil_weights(make_stencil_taps(op.Nl, radius));
     T *wT = nullptr, *r = nullptr, *z = nullptr, *d = nullptr, *q = nullptr, *lam = nullptr;
     uint8_t* mask = nullptr;
     double* part = nullptr;
@@ -2555,7 +2553,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     PkParams P{};
     P.N = N;
     P.Ns = op.Ns;
-    P.Nl = op.Ns;
+    P.Nl = op.Nl;
     P.tol = tol;
     P.max_iter = max_iter;
     P.precond = precond;
@@ -2575,8 +2573,8 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
         for (int k = 0; k < 16; ++k) {  // kernels return at entry once halted
             const T* zz = r;
             if (precond == ASPHER_PRECOND_STENCIL) {
-                launch_stencil<T, false, false>(radius, op.Ns, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st, W, r,
-                                                nullptr, mask, z, part, 1);
+                launch_stencil<T, false, false>(radius, op.Ns, op.Nl, dim3(stencil_grid(op.Nl)),
+                                                s, Pd, st, W, r, nullptr, mask, z, part, 1);
                 zz = z;
             }
             k_adj_rz<T><<<grid, kRedThreads, 0, s>>>(Pd, st, zz, r, mask, part);
@@ -2595,7 +2593,7 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     ASB_CUDA(cudaGetLastError());
     read();
     const double mu = h.red[0];
-    if (grad_pbar) *grad_pbar = -mu * (double)N;
+    if (grad_pbar) *grad_pbar = -mu * (double)op.Nl * (double)op.Nl;  // P = p_bar Nl^2
     if (info) {
         std::memset(info, 0, sizeof(*info));
         info->status = h.status;
@@ -2607,6 +2605,21 @@ void adjoint_impl(Operator& op, const double* p, const double* w, double tol, in
     }
     void* all[] = {wT, r, z, d, q, lam, mask, part, st, Pd};
     for (void* v : all) cudaFreeAsync(v, s);
+    ASB_CUDA(cudaStreamSynchronize(s));
+}
+// the caller's fields around the core (embedded operators: p and w into
+// compute-grid fields that are 0 outside the caller's block, so the contact
+// set and the constraint are the caller's; dL/dg0's block copied back)
+template <typename T>
+void adjoint_impl(Operator& op, const double* p, const double* w, double tol, int max_iter,
+                  int precond, int radius, double* grad_g0, double* grad_pbar,
+                  aspher_adjoint_info* info, cudaStream_t s) {
+    EmbedIO io(op, s);
+    const double* pc = io.in(p, 0.0);
+    const double* wc = io.in(w, 0.0);
+    double* gc = io.out(grad_g0);
+    adjoint_core<T>(op, pc, wc, tol, max_iter, precond, radius, gc, grad_pbar, info, s);
+    io.back(gc, grad_g0);
     ASB_CUDA(cudaStreamSynchronize(s));
 }
 template void adjoint_impl<float>(Operator&, const double*, const double*, double, int, int, int,

@@ -77,10 +77,12 @@ def test_oracle_adjoint_matches_finite_differences(backend):
 @pytest.mark.parametrize("backend", ["periodic", "fft"])
 @pytest.mark.parametrize("dt,bound", [("f64", 1e-8), ("f32", 1e-4)])
 @pytest.mark.parametrize("precond", ["fourier", "none"])
-def test_gpu_adjoint_matches_dense(backend, dt, bound, precond):
+@pytest.mark.parametrize("Ns", [32, 30])
+def test_gpu_adjoint_matches_dense(backend, dt, bound, precond, Ns):
+    """Ns = 30 runs embedded (the caller's block of a 32 x 32 grid)."""
     torch = pytest.importorskip("torch")
     from aspher_b200 import ContactSolver, adjoint
-    Ns, pbar = 32, 0.005
+    pbar = 0.005
     s = ContactSolver(Ns, backend=backend)
     g0 = _gap(Ns, seed=3)
     r = s.solve(g0, pbar, tol=1e-12, max_iter=20000, precond="fourier")
