@@ -553,7 +553,9 @@ def run_ours(args):
             "config": {"workload": "Ns=2048 solves: fft+periodic x p_nominal "
                                    "{0.001,0.005,0.02}, tol 1e-6, stencil precond, "
                                    "FP32 CG (FP64 reductions) to the float floor 2e-5 + "
-                                   "FP64 polish to tol/2, the 3 loads of a backend batched",
+                                   "FP64 polish to tol/2, through the library's batch call "
+                                   "(the 3 loads of a backend batched, the two backends' "
+                                   "batches concurrent)",
                        "grid_size": Ns, "solves_per_step_per_gpu": len(probs), "tol": TOL,
                        "float_tol": FLOAT_TOL, "polish_tol": POLISH_TOL,
                        "l2": "256 MB buffer written between steps; working set "
