@@ -2271,11 +2271,30 @@ void solve_batch_mixed_core(Operator& op, const aspher_solve_opts& o, int B,
 
 // Standalone preconditioner apply: z = M^-1 g on contact, contact-mean removed.
 template <typename T>
-void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
-                        const uint8_t* mask, T* z, cudaStream_t s) {
-    if (op.embedded())
-        throw Error(ASPHER_EINVAL, "precond_apply needs a power-of-two grid_size in [16, 16384]");
+void precond_apply_impl(Operator& op, int precond, int radius, const T* g_in,
+                        const uint8_t* mask_in, T* z_out, cudaStream_t s) {
+    if (op.embedded() && precond != 1)
+        throw Error(ASPHER_EINVAL, "precond 'fourier-fft' needs a power-of-two grid_size in "
+                                   "[16, 16384]");
     const long N = (long)op.Ns * op.Ns;
+    // embedded: g and the contact flags into compute-grid fields (0 outside
+    // the caller's block: no contact there), z's block copied back
+    const T* g = g_in;
+    const uint8_t* mask = mask_in;
+    T* z = z_out;
+    void* tmp[3] = {nullptr, nullptr, nullptr};
+    if (op.embedded()) {
+        ASB_CUDA(cudaMallocAsync(&tmp[0], (size_t)N * sizeof(T), s));
+        ASB_CUDA(cudaMallocAsync(&tmp[1], (size_t)N, s));
+        ASB_CUDA(cudaMallocAsync(&tmp[2], (size_t)N * sizeof(T), s));
+        k_embed<T, T><<<embed_grid(N), 256, 0, s>>>(op.Nl, op.Ns, 1, g_in, (T*)tmp[0], T(0));
+        k_embed<uint8_t, uint8_t><<<embed_grid(N), 256, 0, s>>>(op.Nl, op.Ns, 1, mask_in,
+                                                                (uint8_t*)tmp[1], 0);
+        count_launches(2);
+        g = (const T*)tmp[0];
+        mask = (const uint8_t*)tmp[1];
+        z = (T*)tmp[2];
+    }
     PkState* st = nullptr;
     double* part = nullptr;
     ASB_CUDA(cudaMallocAsync((void**)&st, sizeof(PkState), s));
@@ -2284,7 +2303,7 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     PkParams P{};
     P.N = N;
     P.Ns = op.Ns;
-    P.Nl = op.Ns;
+    P.Nl = op.Nl;
     P.precond = precond;
     PkParams* Pd = nullptr;
     ASB_CUDA(cudaMallocAsync((void**)&Pd, sizeof(PkParams), s));
@@ -2292,14 +2311,19 @@ void precond_apply_impl(Operator& op, int precond, int radius, const T* g,
     const int grid = red_grid(N);
     k_gmean<T><<<grid, kRedThreads, 0, s>>>(N, st, g, mask, part);
     if (precond == 1) {
-        StencilTaps taps = make_stencil_taps(op.Ns, radius);
-        launch_stencil<T, false, false>(radius, op.Ns, op.Ns, dim3(stencil_grid(op.Ns)), s, Pd, st,
-                                        stencil_weights(taps), g, nullptr, mask, z, part, 0);
+        StencilTaps taps = make_stencil_taps(op.Nl, radius);
+        launch_stencil<T, false, false>(radius, op.Ns, op.Nl, dim3(stencil_grid(op.Nl)), s, Pd,
+                                        st, stencil_weights(taps), g, nullptr, mask, z, part, 0);
     } else {
         fourier_precond_pk<T>(op, g, mask, st, z, part, s, nullptr);
     }
     k_sub_zmean<T><<<grid, kRedThreads, 0, s>>>(N, z, mask, st);
     count_launches(2);
+    if (op.embedded()) {
+        k_extract<T, T><<<embed_grid((long)op.Nl * op.Nl), 256, 0, s>>>(op.Nl, op.Ns, 1, z, z_out);
+        count_launches(1);
+        for (void* v : tmp) cudaFreeAsync(v, s);
+    }
     ASB_CUDA(cudaGetLastError());
     ASB_CUDA(cudaStreamSynchronize(s));
     cudaFreeAsync(st, s);

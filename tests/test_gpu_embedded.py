@@ -176,3 +176,29 @@ def test_embedded_warm_start_and_history():
     g = torch.as_tensor(_gap(45), device="cuda")
     h = solve_device(op, g, pbar, tol=tol, record_history=True, precond="fourier")
     assert h.status == "converged" and len(h.error_history) == h.iterations
+
+
+@pytest.mark.parametrize("Ns,radius", [(50, 2), (37, 3), (200, 2)])
+def test_embedded_stencil_preconditioner_matches_reference(Ns, radius):
+    """The standalone stencil apply on an embedded grid wraps at the
+    caller's side (stencil_precond.cpp:63-109 on the Nl torus) with the taps
+    of min(Nl, 512); against the reference's own apply (oracle/_ref) where it
+    is built, else the numpy restatement; FP64 1e-13, FP32 2e-6."""
+    from aspher_b200 import Operator
+    from oracle.precond import StencilPreconditioner
+    rng = np.random.default_rng(5 + Ns)
+    g = rng.standard_normal(Ns * Ns)
+    c = (rng.random(Ns * Ns) < 0.35).astype(np.uint8)
+    op = Operator("fft", Ns)
+    if ref.available():
+        want = ref.ContactSolver(Ns, backend="fft").precond_apply(g, c, "fourier", radius)
+    else:
+        want = StencilPreconditioner(Ns, radius).apply(g, c.astype(bool), np.float64)
+    for dt, tol in ((torch.float64, 1e-13), (torch.float32, 2e-6)):
+        gd = torch.as_tensor(g, dtype=dt, device="cuda")
+        cd = torch.as_tensor(c, device="cuda")
+        z = torch.empty_like(gd)
+        op.precond_("stencil", gd, cd, z, radius=radius)
+        got = z.cpu().numpy().astype(np.float64)
+        assert np.all(got[c == 0] == 0.0)
+        assert _rel(got, want) < tol
