@@ -514,9 +514,9 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
     const int engine0 = (kind == OP_PERIODIC && np.precond_engine == 0) ? 2 : np.precond_engine;
     for (int n : levels) {
         if (n > kMaxNs) throw Error(ASPHER_EINVAL, "solve_contact_nested: Ns must be <= 16384");
-        if (np.precond && engine0 == 2 && (!pow2(n) || n < 16))
+        if (np.precond && engine0 == 2 && (!pow2(n) || n < 16) && n % 2)
             throw Error(ASPHER_EINVAL, "solve_contact_nested: the fft preconditioner engine needs "
-                                       "power-of-two levels >= 16 (use precond_engine='stencil')");
+                                       "even levels (use precond_engine='stencil')");
     }
     if (np.active_set && levels.size() < 2)
         throw Error(ASPHER_EINVAL, "solve_contact_nested: active_set needs a coarse level "
@@ -585,9 +585,10 @@ void solve_nested(int kind, int Ns, double L, double E, const double* g0, double
             const int engine = (kind == OP_PERIODIC && np.precond_engine == 0) ? 2 : np.precond_engine;
             bool use_stencil = stencil_for_level(engine, np.precond != 0, prev_occupancy,
                                                  np.precond_occupancy_max);
-            // an embedded level has no FFT preconditioner: under `auto` it
-            // keeps the stencil where the reference would switch
-            if (!use_stencil && np.precond && engine == 0 && op->embedded()) use_stencil = true;
+            // an odd embedded level has no FFT preconditioner: under `auto`
+            // it keeps the stencil where the reference would switch
+            if (!use_stencil && np.precond && engine == 0 && op->embedded() && n % 2)
+                use_stencil = true;
             const int r_lvl = std::min({np.precond_radius, std::max(1, n / 4), np.leaf_side});
             const int pc = use_stencil ? ASPHER_PRECOND_STENCIL
                                        : (np.precond ? ASPHER_PRECOND_FFT : ASPHER_PRECOND_NONE);

@@ -404,14 +404,14 @@ struct FreeImpl {
     // row_fwd(ld) -> col(x Kh) -> row_inv(st); ld / st see the Ns x Ns field(s)
     template <class Load, class Store>
     static void apply(const Operator& op, Load ld, Store st, cplx<T>* spec, cudaStream_t s,
-                      const int* gate, int B) {
+                      const int* gate, int B, const T* kh_over = nullptr) {
         if constexpr (!kSupported) {
             throw Error(-1, "free-space FP64 apply above grid_size 8192 is not supported (its "
                             "rows and half columns do not fit one CTA's shared memory); use FP32");
         } else {
             const int dbl = sizeof(T) == 8;
             const int rv = op.rowv[dbl], cv = op.colv[dbl], c = op.ct[dbl];
-            const T* kh = dbl ? (const T*)op.kh_d : (const T*)op.kh_f;
+            const T* kh = kh_over ? kh_over : (dbl ? (const T*)op.kh_d : (const T*)op.kh_f);
             const long bsp = (long)(LR / c + 1) * NS * c;
             row_fwd_v<T, LR, true, kAllV>(rv, ld, StoreTiled<T>{spec, NS, c, bsp}, NS, s, gate, B);
             if (split(op)) {
@@ -569,18 +569,23 @@ struct KhBuild {
         return NS >= kSplitMin && op.split_kh;
     }
     static void run(Operator& op) {
-        constexpr int LR = NS, M = 2 * NS;
         const size_t nk = (size_t)(NS + 1) * (NS + 1);
         ASB_CUDA(cudaMalloc(&op.kh_canon, nk * sizeof(double)));
+        op.max_im_ratio = build(op, op.table, op.kh_canon);
+    }
+    // the canonical spectrum of an even table (tab, Ns x Ns) into canon
+    // ((Ns+1)^2); returns the realness ratio, throws when it fails
+    static double build(const Operator& op, const double* table, double* canon) {
+        constexpr int LR = NS, M = 2 * NS;
         double* yt = nullptr;
         unsigned long long* mx = nullptr;
         ASB_CUDA(cudaMalloc(&yt, (size_t)(NS + 1) * M * sizeof(double)));
         ASB_CUDA(cudaMalloc(&mx, 4 * sizeof(unsigned long long)));
         ASB_CUDA(cudaMemset(mx, 0, 4 * sizeof(unsigned long long)));
         StoreRealTracked sa{yt, M, nullptr, nullptr, 0, 0, 0, 0.0, mx, 0.0, 0.0};
-        StoreRealTracked sb{nullptr, M, op.kh_canon, nullptr, NS + 1, 0, 0,
+        StoreRealTracked sb{nullptr, M, canon, nullptr, NS + 1, 0, 0,
                             1.0 / ((double)M * (double)M), mx + 2, 0.0, 0.0};
-        const LoadEmbedded emb{op.table, NS, M};
+        const LoadEmbedded emb{table, NS, M};
         if (split(op)) {
             if constexpr (NS >= kSplitMin) {
                 constexpr int LH = NS / 2;  // real length Ns per parity
@@ -624,11 +629,12 @@ struct KhBuild {
         for (int i = 0; i < 4; ++i) std::memcpy(&v[i], &h[i], sizeof(double));
         const double ra = v[1] > 0 ? v[0] / v[1] : 0.0;
         const double rbt = v[3] > 0 ? v[2] / v[3] : 0.0;
-        op.max_im_ratio = ra > rbt ? ra : rbt;
+        const double ratio = ra > rbt ? ra : rbt;
         // fft_operator.cpp:57-60: the embedding is even, so the spectrum is real
         if (v[0] > 1e-10 * v[1] || v[2] > 1e-10 * v[3])
             throw Error(-3, "FFTOperator: kernel spectrum has a non-negligible imaginary "
                             "part; wrap-around embedding is broken");
+        return ratio;
     }
 };
 
@@ -664,7 +670,10 @@ __device__ __forceinline__ void kahan_add(double& sum, double& comp, double term
 
 // A[ky][dx] = sum_{kx < nh} w(kx) sigma(kx, ky) cos(2 pi kx dx / Nl), ky < nh
 // (block: one ky, threads over dx; shared: the cosine table and sigma's row)
-__global__ void k_periodic_rows(int Nl, double scale, const double* __restrict__ ctab,
+// symbol 0: scale / |m| (the periodic operator); 1: the full-grid |k|
+// preconditioner's float symbol, float(normf |k|) with normf = float(1 / Nl^2)
+// as the reference stores it (fourier_precond.cpp:12-28); both 0 at DC
+__global__ void k_periodic_rows(int Nl, int symbol, double scale, const double* __restrict__ ctab,
                                 double* __restrict__ A) {
     extern __shared__ double sh[];
     const int nh = Nl / 2 + 1;
@@ -674,7 +683,16 @@ __global__ void k_periodic_rows(int Nl, double scale, const double* __restrict__
     for (int r = threadIdx.x; r < Nl; r += blockDim.x) cs[r] = ctab[r];
     for (int kx = threadIdx.x; kx < nh; kx += blockDim.x) {
         const double m2 = (double)kx * kx + (double)ky * ky;
-        sg[kx] = m2 > 0.0 ? half_weight(kx, Nl) * (scale / sqrt(m2)) : 0.0;
+        double sym = 0.0;
+        if (m2 > 0.0) {
+            if (symbol == 0) {
+                sym = scale / sqrt(m2);
+            } else {
+                const float normf = 1.0f / ((float)Nl * (float)Nl);
+                sym = (double)(normf * hypotf((float)kx, (float)ky));
+            }
+        }
+        sg[kx] = half_weight(kx, Nl) * sym;
     }
     __syncthreads();
     const int dx = blockIdx.x * blockDim.x + threadIdx.x;
@@ -707,7 +725,7 @@ __global__ void k_periodic_cols(int Nl, int Ns, const double* __restrict__ ctab,
     tab[(size_t)dy * Ns + dx] = sum;
 }
 
-void periodic_kernel_table(int Nl, int Ns, double scale, double* tab) {
+void periodic_kernel_table(int Nl, int Ns, double scale, double* tab, int symbol = 0) {
     const int nh = Nl / 2 + 1;
     double *ctab = nullptr, *A = nullptr;
     ASB_CUDA(cudaMalloc(&ctab, (size_t)Nl * sizeof(double)));
@@ -716,7 +734,7 @@ void periodic_kernel_table(int Nl, int Ns, double scale, double* tab) {
     k_cos_table<<<(Nl + 255) / 256, 256>>>(Nl, ctab);
     const int smem = (Nl + nh) * (int)sizeof(double);
     smem_optin((const void*)k_periodic_rows, smem);
-    k_periodic_rows<<<dim3((Nl + 127) / 128, nh), 128, smem>>>(Nl, scale, ctab, A);
+    k_periodic_rows<<<dim3((Nl + 127) / 128, nh), 128, smem>>>(Nl, symbol, scale, ctab, A);
     k_periodic_cols<<<dim3((Nl + 127) / 128, Nl), 128>>>(Nl, Ns, ctab, A, tab);
     count_launches(3);
     ASB_CUDA(cudaGetLastError());
@@ -818,6 +836,9 @@ Operator::~Operator() {
     ctx_d.reset();
     cudaFree(emb_x);
     cudaFree(emb_y);
+    cudaFree(khp_canon);
+    cudaFree(khp_d);
+    cudaFree(khp_f);
     cudaFree(kh_d);
     cudaFree(kh_f);
     cudaFree(kh_canon);
@@ -844,9 +865,13 @@ void Operator::set_variants(bool dbl, int rv, int cv) {
     std::lock_guard<std::recursive_mutex> setup(setup_mutex());
     const int c = col_tile(dbl, cv);
     if (kind == OP_FFT && c != ct[dbl]) {
-        // re-tile Kh of this precision for the new column tile width
+        // re-tile Kh of this precision for the new column tile width (and
+        // the preconditioner's spectrum of an embedded grid)
         k_retile_kh<<<1184, 256>>>(Ns, kh_canon, c, dbl ? kh_d : nullptr, c,
                                    dbl ? nullptr : kh_f);
+        if (khp_canon)
+            k_retile_kh<<<1184, 256>>>(Ns, khp_canon, c, dbl ? khp_d : nullptr, c,
+                                       dbl ? nullptr : khp_f);
         ASB_CUDA(cudaGetLastError());
         ASB_CUDA(cudaDeviceSynchronize());
     }
@@ -1036,9 +1061,71 @@ void Operator::apply_caller(bool dbl, const void* x, void* y, cudaStream_t s) {
     ASB_CUDA(cudaGetLastError());
 }
 
+void Operator::ensure_precond_spectrum() {
+    if (khp_canon) return;
+    if (!embedded() || kind != OP_FFT)
+        throw Error(-1, "ensure_precond_spectrum: embedded grids only");
+    if (Nl % 2)
+        throw Error(-1, "precond 'fourier-fft' on a grid that is not a power of two needs an "
+                        "even grid_size (its |k| symbol is not even on an odd torus)");
+    std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+    double* tab = nullptr;
+    const size_t nk = (size_t)(Ns + 1) * (Ns + 1), nt = (size_t)(Ns + 16) * (Ns + 1);
+    try {
+        ASB_CUDA(cudaMalloc(&tab, (size_t)Ns * Ns * sizeof(double)));
+        periodic_kernel_table(Nl, Ns, 0.0, tab, 1);
+        ASB_CUDA(cudaMalloc(&khp_canon, nk * sizeof(double)));
+        ASB_SIZE_SWITCH(Ns, (void)KhBuild<NS>::build(*this, tab, khp_canon));
+        if (supports(true)) {
+            ASB_CUDA(cudaMalloc(&khp_d, nt * sizeof(double)));
+            ASB_CUDA(cudaMemset(khp_d, 0, nt * sizeof(double)));
+            k_retile_kh<<<1184, 256>>>(Ns, khp_canon, ct[1], khp_d, ct[1], nullptr);
+        }
+        ASB_CUDA(cudaMalloc(&khp_f, nt * sizeof(float)));
+        ASB_CUDA(cudaMemset(khp_f, 0, nt * sizeof(float)));
+        k_retile_kh<<<1184, 256>>>(Ns, khp_canon, ct[0], nullptr, ct[0], khp_f);
+        ASB_CUDA(cudaGetLastError());
+        ASB_CUDA(cudaDeviceSynchronize());
+    } catch (...) {
+        cudaFree(tab);
+        cudaFree(khp_canon);
+        cudaFree(khp_d);
+        cudaFree(khp_f);
+        khp_canon = nullptr;
+        khp_d = nullptr;
+        khp_f = nullptr;
+        throw;
+    }
+    cudaFree(tab);
+}
+
+// the full-grid |k| preconditioner of an embedded grid: the masked centred
+// residual convolved with the symbol's real-space kernel on the Nl torus by
+// the compute grid's padded pipeline, gathered on contact with its contact
+// sum (the same load and store as the periodic form)
+template <typename T, int NS>
+struct EmbeddedFourierImpl {
+    static void run(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
+                    double* part, cudaStream_t s, const int* gate, int B, void* spec_b) {
+        if (!op.khp_canon)
+            throw Error(-1, "fourier-fft preconditioner spectrum not built (set-up order)");
+        cplx<T>* spec = static_cast<cplx<T>*>(spec_b ? spec_b : op.spectrum(sizeof(T) == 8, s));
+        const long bx = (long)NS * NS;
+        const T* kh = sizeof(T) == 8 ? (const T*)op.khp_d : (const T*)op.khp_f;
+        FreeImpl<T, NS>::apply(op, LoadMaskCentered<T>{g, mask, st, NS, bx},
+                               StoreGather<T>{z, mask, NS, st, part, bx, 0.0}, spec, s, gate, B,
+                               kh);
+    }
+};
+
 template <typename T>
 void fourier_precond_pk(Operator& op, const T* g, const uint8_t* mask, PkState* st, T* z,
                         double* part, cudaStream_t s, const int* gate, int B, void* spec) {
+    if (op.embedded()) {
+        ASB_SIZE_SWITCH(op.Ns, EmbeddedFourierImpl<T, NS>::run(op, g, mask, st, z, part, s, gate,
+                                                               B, spec));
+        return;
+    }
     ASB_SIZE_SWITCH(op.Ns, FourierImpl<T, NS>::run(op, g, mask, st, z, part, s, gate, B, spec));
 }
 template void fourier_precond_pk<float>(Operator&, const float*, const uint8_t*, PkState*, float*,

@@ -106,6 +106,13 @@ struct Operator {
     // caller-facing apply: x, y hold Nl*Nl values (embedded: copied into the
     // compute grid's block and back; otherwise matvec)
     void apply_caller(bool dbl, const void* x, void* y, cudaStream_t s);
+    // embedded grids (even Nl) with the full-grid |k| preconditioner: the
+    // spectrum of its real-space kernel on the Nl torus, canonical and tiled
+    // like Kh; built by ensure_precond_spectrum() (set-up, not under capture)
+    double* khp_canon = nullptr;
+    double* khp_d = nullptr;
+    float* khp_f = nullptr;
+    void ensure_precond_spectrum();
     int device = 0;
     // free space: real half spectrum Kh (1/M^2 folded in), rows ky in [0, Ns]
     // only (Kh is even in ky): canonical [ky][kx] FP64, plus FP64 / FP32

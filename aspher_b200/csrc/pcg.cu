@@ -1265,9 +1265,13 @@ struct SolverCtx : SolverCtxBase {
     }
     void configure(int pc, int R) {
         if (pc == precond && (pc != 1 || R == radius)) return;
-        if (pc == 2 && op.embedded())
-            throw Error(ASPHER_EINVAL, "precond 'fourier-fft' needs a power-of-two grid_size in "
-                                       "[16, 16384] (use 'fourier', the stencil, on this grid)");
+        if (pc == 2 && op.embedded()) {
+            if (op.Nl % 2)
+                throw Error(ASPHER_EINVAL, "precond 'fourier-fft' on a grid that is not a power "
+                                           "of two needs an even grid_size (use 'fourier', the "
+                                           "stencil, on this grid)");
+            op.ensure_precond_spectrum();  // set-up before any capture
+        }
         if (pc == 1) {
             taps = make_stencil_taps(op.Nl, R);
             W = stencil_weights(taps);
@@ -2273,9 +2277,12 @@ void solve_batch_mixed_core(Operator& op, const aspher_solve_opts& o, int B,
 template <typename T>
 void precond_apply_impl(Operator& op, int precond, int radius, const T* g_in,
                         const uint8_t* mask_in, T* z_out, cudaStream_t s) {
-    if (op.embedded() && precond != 1)
-        throw Error(ASPHER_EINVAL, "precond 'fourier-fft' needs a power-of-two grid_size in "
-                                   "[16, 16384]");
+    if (op.embedded() && precond != 1) {
+        if (op.Nl % 2)
+            throw Error(ASPHER_EINVAL, "precond 'fourier-fft' on a grid that is not a power of "
+                                       "two needs an even grid_size");
+        op.ensure_precond_spectrum();
+    }
     const long N = (long)op.Ns * op.Ns;
     // embedded: g and the contact flags into compute-grid fields (0 outside
     // the caller's block: no contact there), z's block copied back

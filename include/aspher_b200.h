@@ -79,9 +79,9 @@ typedef struct aspher_op aspher_op;
  * power-of-two grid's free-space pipeline, whose kernel table is the Love
  * table at cell size domain_size / grid_size (FFT) or the real-space kernel
  * of the periodic symbol on the grid_size torus (PERIODIC); every entry
- * point still takes grid_size^2 fields.  Creation flags and the FFT
- * preconditioner need a power of two >= 16 (ASPHER_EINVAL otherwise); the
- * nested driver takes such levels with the stencil preconditioner engine. */
+ * point still takes grid_size^2 fields.  Creation flags need a power of
+ * two >= 16 and the FFT preconditioner an even grid_size (ASPHER_EINVAL
+ * otherwise). */
 int aspher_op_create(int backend, int grid_size, double domain_size, double E_star,
                      aspher_op** out);
 /* The same with creation flags (the survey's aspher_op_create(kind, Ns, L,

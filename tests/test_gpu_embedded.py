@@ -144,9 +144,9 @@ def test_embedded_batch_and_many():
 
 def test_embedded_rejects_what_needs_a_power_of_two():
     from aspher_b200 import ContactSolver, Operator
-    s = ContactSolver(60, backend="fft")
-    with pytest.raises(ValueError, match="fourier-fft"):
-        s.solve(_gap(60), 0.005, 1e-8, precond="fourier-fft")
+    s = ContactSolver(61, backend="fft")
+    with pytest.raises(ValueError, match="even grid_size"):
+        s.solve(_gap(61), 0.005, 1e-8, precond="fourier-fft")
     with pytest.raises(ValueError, match="power-of-two"):
         Operator("fft", 60, flags=1)
     with pytest.raises(ValueError):
@@ -202,3 +202,44 @@ def test_embedded_stencil_preconditioner_matches_reference(Ns, radius):
         got = z.cpu().numpy().astype(np.float64)
         assert np.all(got[c == 0] == 0.0)
         assert _rel(got, want) < tol
+
+
+@pytest.mark.parametrize("Ns", [50, 100])
+def test_embedded_fourier_preconditioner_matches_reference(Ns):
+    """The full-grid |k| preconditioner on an even grid that is not a power
+    of two: the circulant of the reference's float symbol |k| / Ns^2 on the
+    Ns torus (fourier_precond.cpp:12-116) as a padded convolution with its
+    real-space kernel.  Against the reference's own apply (oracle/_ref) or
+    the numpy restatement: FP64 1e-12 (the kernel table is a cosine sum
+    over Ns^2 terms), FP32 2e-6."""
+    from aspher_b200 import Operator
+    from oracle.precond import FourierPreconditioner
+    rng = np.random.default_rng(17 + Ns)
+    g = rng.standard_normal(Ns * Ns)
+    c = (rng.random(Ns * Ns) < 0.35).astype(np.uint8)
+    op = Operator("fft", Ns)
+    if ref.available():
+        want = ref.ContactSolver(Ns, backend="fft").precond_apply(g, c, "fourier-fft")
+    else:
+        want = FourierPreconditioner(Ns).apply(g, c.astype(bool), np.float64)
+    for dt, tol in ((torch.float64, 1e-12), (torch.float32, 2e-6)):
+        gd = torch.as_tensor(g, dtype=dt, device="cuda")
+        cd = torch.as_tensor(c, device="cuda")
+        z = torch.empty_like(gd)
+        op.precond_("fft", gd, cd, z)
+        got = z.cpu().numpy().astype(np.float64)
+        assert np.all(got[c == 0] == 0.0)
+        assert _rel(got, want) < tol
+
+
+@pytest.mark.parametrize("backend", ["fft", "periodic"])
+def test_embedded_solve_with_fourier_preconditioner(backend):
+    from aspher_b200 import ContactSolver
+    Ns, pbar, tol = 100, 0.005, 1e-8
+    g0 = _gap(Ns)
+    r = ContactSolver(Ns, backend=backend).solve(g0, pbar, tol, 5000, precond="fourier-fft")
+    o = _oracle(Ns, backend).solve(g0, pbar, tol, 5000, precond="fourier-fft")
+    assert o.status == "converged" and r.status == "converged", (r.status, r.status_reason)
+    assert _rel(r.pressure, o.pressure) <= 10 * tol
+    assert abs(r.contact_area - o.contact_area) <= 1e-4
+    assert abs(r.iterations - o.iterations) <= 6

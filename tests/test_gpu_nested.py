@@ -203,5 +203,10 @@ def test_nested_non_power_of_two_levels_match_oracle(active):
     assert abs(r.contact_area - o.contact_area) <= 1e-4
     full = hc.ContactSolver(ns, backend="fft").solve(g, pbar, tol, precond="fourier")
     assert rel(r.pressure, full.pressure) <= 10 * tol
-    with pytest.raises(ValueError, match="power-of-two levels"):
+    with pytest.raises(ValueError, match="even levels"):
         hc.solve_nested(ns, g, pbar, coarsest=25, backend="periodic", tol=tol)
+    # even levels: the periodic backend's default fft engine runs embedded
+    rp = hc.solve_nested(ns, g, pbar, coarsest=50, backend="periodic", tol=tol)
+    op_ = osolve(ns, g, pbar, coarsest=50, backend="periodic", tol=tol)
+    assert rp.status == "converged" and op_.status == "converged"
+    assert rel(rp.pressure, op_.pressure) <= 10 * tol
