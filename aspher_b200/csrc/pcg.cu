@@ -317,9 +317,11 @@ __device__ __forceinline__ void beta_update(const PkParams& P, PkState* st, doub
 // summed in the reference's tap order (dy-major, dx-minor).
 constexpr int kStX = 64, kStY = 32, kStRows = 8, kMaxR = 4;
 
-// the disc's weights by (|dy|, |dx|) (they depend on the distance only)
+// the disc's weights by signed offset, w[dy + kMaxR][dx + kMaxR] (even in
+// each offset on an even kernel grid; on an odd one the reference's
+// wavenumber convention leaves them slightly uneven)
 struct StencilW {
-    double w[kMaxR + 1][kMaxR + 1];
+    double w[2 * kMaxR + 1][2 * kMaxR + 1];
 };
 
 // LAZY: g holds v uncentred (the solve loop; centred by Real(alpha) on the
@@ -415,7 +417,7 @@ __global__ void __launch_bounds__(256) k_stencil_t(const PkParams* __restrict__ 
 #pragma unroll
                 for (int dx = -R; dx <= R; ++dx)
                     if (dx * dx + dy * dy <= R * R)
-                        a += W.w[dy < 0 ? -dy : dy][dx < 0 ? -dx : dx] *
+                        a += W.w[dy + kMaxR][dx + kMaxR] *
                              tile[(ly + R + dy) * TW + (tx + R + dx)];
             const T zT = (T)a;
             z[i] = zT;
@@ -570,7 +572,7 @@ __global__ void __launch_bounds__(32 * kSwWarps) k_stencil_w(const PkParams* __r
 #pragma unroll
                 for (int dx = -R; dx <= R; ++dx) {
                     if (dx * dx + dy * dy > R * R) continue;
-                    const double w = W.w[dy < 0 ? -dy : dy][dx < 0 ? -dx : dx];
+                    const double w = W.w[dy + kMaxR][dx + kMaxR];
 #pragma unroll
                     for (int j = 0; j < 4; ++j) a[j] += w * at(R + dy, j + dx);
                 }
@@ -636,7 +638,7 @@ inline int stencil_grid(int Ns) {
 StencilW stencil_weights(const StencilTaps& taps) {
     StencilW W{};
     for (int t = 0; t < taps.n; ++t)
-        W.w[std::abs(taps.dy[t])][std::abs(taps.dx[t])] = taps.w[t];
+        W.w[taps.dy[t] + kMaxR][taps.dx[t] + kMaxR] = taps.w[t];
     return W;
 }
 
@@ -1975,11 +1977,17 @@ StencilTaps make_stencil_taps(int Ns, int R) {
     t.R = R;
     t.n = 0;
     const long double c0 = kgrid_value(Nw, 0, 0);
-    std::map<std::pair<int, int>, double> uniq;  // w depends on (|dx|, |dy|) only
+    // w depends on (|dx|, |dy|) only on an even Nw; on an odd one the
+    // reference's wavenumber convention (ky < Nw/2 ? ky : ky - Nw) makes the
+    // kernel slightly uneven, and the reference reads it at the signed
+    // offsets (stencil_precond.cpp:211-216)
+    const bool even = Nw % 2 == 0;
+    std::map<std::pair<int, int>, double> uniq;
     for (int dy = -R; dy <= R; ++dy)
         for (int dx = -R; dx <= R; ++dx) {
             if (dx * dx + dy * dy > R * R) continue;
-            const std::pair<int, int> key{std::abs(dx), std::abs(dy)};
+            const std::pair<int, int> key = even ? std::make_pair(std::abs(dx), std::abs(dy))
+                                                 : std::make_pair(dx, dy);
             auto u = uniq.find(key);
             double v;
             if (dx == 0 && dy == 0) v = 1.0;
