@@ -593,6 +593,9 @@ def run_ours(args):
                                              "at Ns=2048, q = [q_x; q_y], L2 flushed",
                                  **tangential},
             "gpu_launches": launches,
+            "gpu_launches_note": "the library's own launches in the timed region "
+                                 "(aspher_launch_count); a CUDA-graph launch -- a PK loop "
+                                 "running 10-12 of its kernels per iteration -- counts once",
             "clocks": clocks,
             "wall_s_timed": wall,
             "step_ms": {"batched": step_ms[0], "single_mixed": step_ms[1],
