@@ -479,6 +479,17 @@ class ContactSolver:
             r.fp64_status = rd.status
         return r
 
+    def block_layout(self):
+        """(0, 6) float64 array: the reference returns block rows only for the
+        'hmatrix' backend and an empty (0, 6) array for every other one
+        (bindings.cpp:240-242)."""
+        return np.zeros((0, 6), dtype=np.float64)
+
+    def recompress(self, svd_tol):
+        """No-op: the reference recompresses only 'hmatrix' operators
+        (bindings.cpp:258-260)."""
+        return None
+
     def hmatrix_info(self):
         inf = self.op.info()
         d = {"backend": self.backend, "n": int(inf.n)}

@@ -112,6 +112,21 @@ def test_status_taxonomy():
         s.solve(g0, 0.02, 1e-8, max_iter=-1)
 
 
+@pytest.mark.parametrize("backend", ["fft", "periodic"])
+def test_binding_surface_for_fourier_backends(backend):
+    """bindings.cpp:240-260: block_layout is (0, 6) and recompress a no-op for
+    every backend but 'hmatrix'; hmatrix_info names the backend."""
+    s = _solver(16, backend)
+    bl = s.block_layout()
+    assert bl.shape == (0, 6) and bl.dtype == np.float64
+    x = np.random.default_rng(3).standard_normal(256)
+    u0 = s.matvec(x)
+    assert s.recompress(1e-4) is None
+    assert np.array_equal(s.matvec(x), u0)
+    info = s.hmatrix_info()
+    assert info["backend"] == backend and info["n"] == 256
+
+
 def test_singleton_warm_start_repaired():
     """test_certification_py.py:42-73 on the fft backend."""
     ns = 16
