@@ -144,7 +144,8 @@ __device__ __forceinline__ V tw_apply(V a, V w) {
 // Shared-memory elements needed by one transform of length L (padded).
 __host__ __device__ constexpr int sm_len(int L) { return L + L / 16 + 1; }
 
-template <typename T, int L, int RPT, int DIR, int S, int STAGE, int SPAN, bool HZ>
+template <typename T, int L, int RPT, int DIR, int S, int STAGE, int SPAN, bool HZ, int ALT,
+          int P0>
 __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
                                            const cplx<T>* __restrict__ tw) {
     constexpr int RMAX = RPT < 16 ? RPT : 16;
@@ -155,6 +156,9 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
         constexpr int Q = RPT / R;    // butterflies per thread
         constexpr bool LAST = (STAGE == NST - 1);
         static_assert(RPT % R == 0, "radix must divide RPT");
+        // this round trip's workspace: with ALT > 0, round trips alternate
+        // between sm and sm + ALT, starting at parity P0
+        cplx<T>* ws = (ALT > 0 && ((STAGE + P0) & 1)) ? sm + ALT : sm;
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = t + q * TT;
@@ -210,15 +214,19 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
             } else {
                 const int base = (j / SPAN) * SPAN * R + (j % SPAN);
 #pragma unroll
-                for (int r = 0; r < R; ++r) sm[smaddr_run<SPAN, SPAN * R>(base, r, S, off)] = a[r];
+                for (int r = 0; r < R; ++r) ws[smaddr_run<SPAN, SPAN * R>(base, r, S, off)] = a[r];
             }
         }
         if constexpr (!LAST) {
             __syncthreads();
 #pragma unroll
-            for (int m = 0; m < RPT; ++m) v[m] = sm[smaddr_run<TT, 1 << 30>(t, m, S, off)];
-            __syncthreads();
-            fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R, HZ>(v, t, sm, off, tw);
+            for (int m = 0; m < RPT; ++m) v[m] = ws[smaddr_run<TT, 1 << 30>(t, m, S, off)];
+            // one workspace: nobody writes it again before everyone has read
+            // it.  Two (ALT > 0): the next round trip writes the other one,
+            // and the one after that follows the next round trip's barrier,
+            // which every thread reaches only after this read.
+            if constexpr (ALT == 0) __syncthreads();
+            fft_stages<T, L, RPT, DIR, S, STAGE + 1, SPAN * R, HZ, ALT, P0>(v, t, sm, off, tw);
         }
     }
 }
@@ -231,11 +239,24 @@ __device__ __forceinline__ void fft_stages(cplx<T> (&v)[RPT], int t, cplx<T>* sm
 // call this (it contains __syncthreads), including threads whose transform
 // is a dummy.  HZ: the upper half of the input is zero (v[m] = 0 for
 // m >= RPT / 2, a zero-padded transform); its first stage skips the zeros.
-template <typename T, int L, int RPT, int DIR, int S, bool HZ = false>
+// ALT > 0: a second workspace of the same shape at sm + ALT (elements); the
+// shared-memory round trips alternate between the two, which saves the
+// barrier after each read.  The first round trip uses parity P0 (0: sm,
+// 1: sm + ALT); a caller that runs two transforms back to back without a
+// barrier between them starts the second at ping_pong_next<L, RPT>(P0), the
+// workspace the first one did not read last.
+template <typename T, int L, int RPT, int DIR, int S, bool HZ = false, int ALT = 0, int P0 = 0>
 __device__ __forceinline__ void block_fft(cplx<T> (&v)[RPT], int t, cplx<T>* sm, int off,
                                           const cplx<T>* __restrict__ tw) {
     static_assert(L % RPT == 0, "L must be a multiple of RPT");
-    fft_stages<T, L, RPT, DIR, S, 0, 1, HZ>(v, t, sm, off, tw);
+    fft_stages<T, L, RPT, DIR, S, 0, 1, HZ, ALT, P0>(v, t, sm, off, tw);
+}
+
+// parity of the first round trip after a ping-pong transform that started at
+// P0: the workspace its last round trip did not read
+template <int L, int RPT>
+__host__ __device__ constexpr int ping_pong_next(int p0) {
+    return (p0 + num_stages(L, RPT < 16 ? RPT : 16) - 1) & 1;
 }
 
 }  // namespace asb

@@ -27,6 +27,8 @@
 // precision (a default table, or the autotuner in operators.cu).
 #pragma once
 
+#include <type_traits>
+
 #include "fft_block.cuh"
 #include "pk_state.hpp"
 
@@ -223,12 +225,49 @@ __host__ __device__ constexpr bool col_staged() {
             col_stage_bytes<T, LC, NCM1, PAD, V>()) *
                col_minb<T>(LC, NCM1, V) <= kSmemPerSM;
 }
+// Unstaged column kernels take a second FFT workspace (ping-pong round
+// trips, one barrier each instead of two) where it fits beside the CTAs per
+// SM the variant asks for.
+template <typename T, int LC, int NCM1, bool PAD, int V>
+__host__ __device__ constexpr bool col_pp() {
+    return !col_staged<T, LC, NCM1, PAD, V>() &&
+           2 * align16(col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V))) * col_minb<T>(LC, NCM1, V) <=
+               kSmemPerSM;
+}
 template <typename T, int LC, int NCM1, bool PAD, int V>
 __host__ __device__ constexpr int col_smem_total() {
     return col_staged<T, LC, NCM1, PAD, V>()
                ? align16(col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V))) +
                      col_stage_bytes<T, LC, NCM1, PAD, V>()
+           : col_pp<T, LC, NCM1, PAD, V>()
+               ? 2 * align16(col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V)))
                : col_smem<T>(LC, col_ct_v<T>(LC, NCM1, V));
+}
+
+// ---- full row groups of the tiled half spectrum ---------------------------------
+// A full group (RB rows) moves its RB x ct tile chunks between shared memory
+// and HBM with compile-time strides when the tile width ct is a power of two
+// no larger than TT = LR / RPT (the threads of one row) and TT is a multiple
+// of 16: thread tid owns chunk element e = tid % (RB ct) -- row rr = e / ct,
+// column c = e % ct -- and the spectrum columns k = k0 + i TT, i < RPT, with
+// k0 = (tid / (RB ct)) ct + c < TT, at HBM offsets (tid / (RB ct)) nrows ct
+// + e + i TT nrows; column LR (tile LR / ct) belongs to the threads with
+// tid < RB ct and c = 0.  f(std::integral_constant<int, CT>) runs the form;
+// returns false (f not called) where the shape does not qualify.
+template <int TT, class F>
+__device__ __forceinline__ bool with_tile_width(int ct, F&& f) {
+    if constexpr (TT % 16 != 0) {
+        return false;
+    } else {
+        switch (ct) {
+            case 1: f(std::integral_constant<int, 1>{}); return true;
+            case 2: f(std::integral_constant<int, 2>{}); return true;
+            case 4: f(std::integral_constant<int, 4>{}); return true;
+            case 8: f(std::integral_constant<int, 8>{}); return true;
+            case 16: f(std::integral_constant<int, 16>{}); return true;
+            default: return false;
+        }
+    }
 }
 
 // ---- row forward ---------------------------------------------------------------
@@ -290,6 +329,7 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
         block_fft<T, LR, RPT, -1, 1, PAD>(v, t, sm, off, tw_lr);
 #pragma unroll
         for (int m = 0; m < RPT; ++m) sm[smaddr_run<TT, 1 << 30>(t, m, 1, off)] = v[m];
+        if (t == 0) sm[smaddr(LR, 1, off)] = v[0];  // Z[LR] = Z[0]: Z[-0] without a mask
         __syncthreads();
         if constexpr (Store::kTiled) {
             // each output reads Z[k] and Z[-k] from shared memory and goes
@@ -297,6 +337,31 @@ row_fwd_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             const int row0 = grp * RB;
             const int nr = nrows - row0 < RB ? nrows - row0 : RB;
             const int ct = st.ct;
+            cplx<T>* gbase = st.base + blockIdx.y * st.bs + (size_t)row0 * ct;
+            auto store_full = [&](auto ctc) {
+                constexpr int CT = decltype(ctc)::value;
+                constexpr int CH = RB * CT;
+                constexpr int ASTEP = TT + TT / 16;  // smaddr(k + TT) - smaddr(k)
+                if constexpr (CT <= TT) {
+                    const int tid = threadIdx.x, e = tid % CH, c = e % CT;
+                    const int k0 = (tid / CH) * CT + c;
+                    const int o = (e / CT) * sm_len(LR + 1);
+                    const int ak = smaddr(k0, 1, o), an = smaddr(LR - k0, 1, o);
+                    cplx<T>* dst = gbase + (size_t)(tid / CH) * st.nrows * CT + e;
+                    const size_t jstep = (size_t)TT * st.nrows;
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i)
+                        dst[i * jstep] = split_w(sm[ak + i * ASTEP], sm[an - i * ASTEP],
+                                                 __ldg(&tw_2lr[k0 + i * TT]));
+                    if (tid < CH && c == 0) {  // k == LR: X = Re Z0 - Im Z0
+                        const cplx<T> z0 = sm[ak];
+                        gbase[(size_t)(LR / CT) * st.nrows * CT + e] = mk<T>(z0.x - z0.y, T(0));
+                    }
+                }
+            };
+            if (nr == RB && RB * TT == (int)blockDim.x && ct <= TT &&
+                with_tile_width<TT>(ct, store_full))
+                return;
             const int chunk = nr * ct;
             const int ntiles = LR / ct + 1;
             const int lct = __ffs(ct) - 1;  // ct is a power of two
@@ -429,6 +494,30 @@ row_inv_kernel(Load ld, Store st, int nrows, const cplx<T>* __restrict__ tw_lr,
             const int lchunk = lct + ilog2c(RB);
             const cplx<T>* base = ld.base + blockIdx.y * ld.bs + (size_t)row0 * ct;
             const int total = ntiles * chunk;
+            auto fast = [&](auto ctc) {  // a full group: every load in flight at once
+                constexpr int CT = decltype(ctc)::value;
+                constexpr int CH = RB * CT;
+                constexpr int ASTEP = TT + TT / 16;  // smaddr(k + TT) - smaddr(k)
+                if constexpr (CT <= TT) {
+                    const int tid = threadIdx.x, e = tid % CH, c = e % CT;
+                    const int k0 = (tid / CH) * CT + c;
+                    const int o = (e / CT) * sm_len(LR + 1);
+                    const cplx<T>* src = base + (size_t)(tid / CH) * ld.nrows * CT + e;
+                    const size_t jstep = (size_t)TT * ld.nrows;
+                    const bool last = tid < CH && c == 0;  // column LR
+                    cplx<T> val[RPT], vl;
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i) val[i] = src[i * jstep];
+                    if (last) vl = base[(size_t)(LR / CT) * ld.nrows * CT + e];
+                    const int ak = smaddr(k0, 1, o);
+#pragma unroll
+                    for (int i = 0; i < RPT; ++i) dst[ak + i * ASTEP] = val[i];
+                    if (last) dst[smaddr(LR, 1, o)] = vl;
+                }
+            };
+            if (!STAGED && full && RB * TT == (int)blockDim.x && ct <= TT &&
+                with_tile_width<TT>(ct, fast))
+                return;
             if constexpr (STAGED) {
                 for (int f = threadIdx.x; f < total; f += blockDim.x) {
                     const int j = full ? f >> lchunk : f / chunk, e = f - j * chunk;
@@ -542,6 +631,10 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     constexpr int NTILES = NCM1 / CT + 1;
     constexpr bool STAGED = col_staged<T, LC, NCM1, PAD, V>();
     constexpr int ROWS = PAD ? LC / 2 : LC;  // stored rows of a tile
+    // second workspace (elements from sm) of the ping-pong form, else 0
+    constexpr int ALT = col_pp<T, LC, NCM1, PAD, V>()
+                            ? align16(col_smem<T>(LC, CT)) / (int)sizeof(cplx<T>) : 0;
+    constexpr int P1 = ALT ? ping_pong_next<LC, RPT>(0) : 0;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
     cplx<T>* stg = reinterpret_cast<cplx<T>*>(smraw + align16(col_smem<T>(LC, CT)));
@@ -559,11 +652,11 @@ col_kernel(cplx<T>* __restrict__ spec, int nrows, Mult mul,
     // transform, multiply, inverse and store of tile `tile` from registers v
     auto body = [&](int tile, cplx<T> (&v)[RPT]) {
         cplx<T>* base = inst + (size_t)tile * nrows * CT;
-        block_fft<T, LC, RPT, -1, CT, PAD>(v, t, sm, c, tw_lc);
+        block_fft<T, LC, RPT, -1, CT, PAD, ALT>(v, t, sm, c, tw_lc);
         const int kx = tile * CT + c;
 #pragma unroll
         for (int m = 0; m < RPT; ++m) v[m] = mul(v[m], kx, t + m * TT);
-        block_fft<T, LC, RPT, +1, CT>(v, t, sm, c, tw_lc);
+        block_fft<T, LC, RPT, +1, CT, false, ALT, P1>(v, t, sm, c, tw_lc);
 #pragma unroll
         for (int m = 0; m < RPT; ++m) {
             if (PAD && m >= RPT / 2) continue;

@@ -23,6 +23,7 @@
 #include "pcg.hpp"
 #include "reduce.cuh"
 
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdlib>
@@ -274,7 +275,13 @@ std::mutex g_attr_mu;
 std::map<std::pair<const void*, int>, int> g_attr_done;
 }  // namespace
 
-// max dynamic shared memory + max-shared carveout, once per kernel per device
+// Max dynamic shared memory and the shared-memory carveout, once per kernel
+// per device.  The carveout asks for the shared memory of as many CTAs as
+// fit on an SM (registers, threads and shared memory counted with every
+// byte available to shared memory) and no more: the rest of the SM's
+// unified L1 / shared storage stays L1 cache, which holds the twiddle
+// tables and multiplier rows the pass kernels read through the read-only
+// path.  The driver rounds the request up to a supported split.
 void fft_attrs(const void* func, int bytes) {
     int dev = 0;
     ASB_CUDA(cudaGetDevice(&dev));
@@ -286,6 +293,18 @@ void fft_attrs(const void* func, int bytes) {
         ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
     ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   cudaSharedmemCarveoutMaxShared));
+    cudaFuncAttributes fa{};
+    ASB_CUDA(cudaFuncGetAttributes(&fa, func));
+    int per_sm = 0, sm_bytes = 0, reserved = 0;
+    ASB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, func, fa.maxThreadsPerBlock,
+                                                           bytes));
+    ASB_CUDA(cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    ASB_CUDA(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+    if (per_sm > 0 && sm_bytes > 0) {
+        const long need = (long)per_sm * ((long)bytes + (long)fa.sharedSizeBytes + reserved);
+        const int pct = (int)std::min<long>(100, (need * 100 + sm_bytes - 1) / sm_bytes);
+        ASB_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    }
     g_attr_done[key] = bytes;
 }
 
