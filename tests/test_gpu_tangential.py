@@ -175,13 +175,24 @@ def test_tangential_warm_solve_equals_reference(Ns):
     the same iteration count and tractions equal to 1e-10 (the unpreconditioned
     tangential PCG stalls at a local-KKT floor of 1e-4 .. 1e-3 at this load,
     so cold solves from roundoff-different starts part ways at that level;
-    the warm chain does not)."""
+    the warm chain does not).
+
+    The reference runs on one OpenMP thread here: its sums are OpenMP
+    reductions (friction_solve.cpp:102, 198, 219), which combine the
+    threads' partial sums in arrival order, so with three or more threads
+    its own trajectory changes from run to run in the last bits, and the
+    iteration count of a run that ends on the stall rule with it."""
     from aspher_b200 import TangentialOperator
     s = _hertz_threshold(Ns)
     target = (0.3 * s.mean(), 0.1 * s.mean())
-    q0, d0 = ref.Tangential(Ns).solve(s, True, target, tol=1e-8, max_iter=5000)
-    delta = (d0["delta_x"] * 1.0001, d0["delta_y"])
-    qr, dr = ref.Tangential(Ns).solve(s, False, delta, tol=1e-8, max_iter=5000, q_init=q0)
+    nt = ref.threads()
+    ref.set_threads(1)
+    try:
+        q0, d0 = ref.Tangential(Ns).solve(s, True, target, tol=1e-8, max_iter=5000)
+        delta = (d0["delta_x"] * 1.0001, d0["delta_y"])
+        qr, dr = ref.Tangential(Ns).solve(s, False, delta, tol=1e-8, max_iter=5000, q_init=q0)
+    finally:
+        ref.set_threads(nt)
     q, d = TangentialOperator(Ns).solve(s, force_control=False, target=delta, tol=1e-8,
                                         max_iter=5000, q_init=q0)
     assert d["status"] == dr["status"]
