@@ -226,15 +226,16 @@ std::mutex g_tuned_mu;
 std::map<std::tuple<int, int, int>, std::pair<int, int>> g_tuned;
 }  // namespace
 
-// Fastest (row, column) variant pairs measured on B200 with
-// `python -m aspher_b200.matvec_bench --sweep --variants` (L2 flushed
-// between applies); sizes not listed use variant 0.
+// Fastest (row, column) variant pairs measured on B200: every pair set on
+// one operator (aspher_op_set_variants) and its apply timed with CUDA
+// events, L2 flushed between applies, median of 15; sizes not listed use
+// variant 0.  Operator::autotune repeats the search in-process.
 void default_variants(int kind, int dbl, int Ns, int& rv, int& cv) {
     static const int table[][5] = {
         // kind, dbl, Ns, row variant, column variant
-        {0, 0, 256, 3, 3}, {0, 0, 512, 2, 1}, {0, 0, 1024, 1, 1}, {0, 0, 2048, 1, 0},
+        {0, 0, 256, 2, 3}, {0, 0, 512, 2, 1}, {0, 0, 1024, 1, 1}, {0, 0, 2048, 1, 0},
         {0, 0, 4096, 0, 1}, {0, 0, 8192, 1, 2}, {0, 1, 256, 1, 1}, {0, 1, 512, 1, 1},
-        {0, 1, 1024, 0, 0}, {0, 1, 2048, 0, 0}, {0, 1, 4096, 0, 0}, {1, 0, 256, 3, 3},
+        {0, 1, 1024, 0, 1}, {0, 1, 2048, 2, 0}, {0, 1, 4096, 0, 0}, {1, 0, 256, 3, 3},
         {1, 0, 512, 0, 3}, {1, 0, 1024, 2, 3}, {1, 0, 2048, 1, 1}, {1, 0, 4096, 1, 0},
         {1, 0, 8192, 0, 1}, {1, 1, 256, 3, 3}, {1, 1, 512, 1, 3}, {1, 1, 1024, 2, 2},
         {1, 1, 2048, 2, 0}, {1, 1, 4096, 2, 0}, {1, 1, 8192, 0, 0},
