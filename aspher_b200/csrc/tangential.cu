@@ -151,6 +151,23 @@ __host__ __device__ constexpr int tan_ct(int LC, int Ns) {
     return ct;
 }
 
+// two FFT workspaces of the column-pair kernel fit one CTA
+template <typename T>
+__host__ __device__ constexpr bool col_pair_pp(int LC, int CT) {
+    return 2 * align16(col_smem<T>(LC, 2 * CT)) <= kSmemPerSM;
+}
+
+// Row-pass launch variant of the tangential apply (its rows are the free-
+// space operator's zero-padded transforms, two fields as gridDim.y = 2),
+// measured on B200 with the column-pair kernel: FP32 the free-space
+// defaults (2048: 0.220 -> 0.210 ms per apply against variant 0, 256: 0.028
+// -> 0.024 ms); FP64 variant 1 up to 512, else 0 (variant 2, the free-space
+// default at 2048, took the two-field apply from 0.396 to 0.441 ms)
+template <typename T>
+__host__ __device__ constexpr int tan_row_variant(int Ns) {
+    return vclamp(Ns, sizeof(T) == 4 ? (Ns <= 512 ? 2 : 1) : (Ns <= 512 ? 1 : 0));
+}
+
 template <typename T>
 struct TanMix {
     const T* kxx;
@@ -184,8 +201,16 @@ col_pair_kernel(cplx<T>* __restrict__ spec, long bsp, int nrows, TanMix<T> mix,
     constexpr int RPT = col_rpt<T>(LC, 0);
     constexpr int TT = LC / RPT;
     constexpr int S = 2 * CT;
+    // second FFT workspace (elements from sm) where two fit one CTA, else 0:
+    // the round trips alternate between them (one barrier each), and the
+    // exchange of the two fields' spectra uses the one the forward
+    // transform's last round trip did not read
+    constexpr int ALT = col_pair_pp<T>(LC, CT) ? align16(col_smem<T>(LC, S)) / (int)sizeof(cplx<T>)
+                                               : 0;
+    constexpr int PX = ALT ? ping_pong_next<LC, RPT>(0) : 0;
     extern __shared__ __align__(16) unsigned char smraw[];
     cplx<T>* sm = reinterpret_cast<cplx<T>*>(smraw);
+    cplx<T>* xs = sm + (PX ? ALT : 0);
     const int c = threadIdx.x % S, t = threadIdx.x / S;
     const int f = c / CT, cc = c % CT;
     const int tile = blockIdx.x;
@@ -194,23 +219,25 @@ col_pair_kernel(cplx<T>* __restrict__ spec, long bsp, int nrows, TanMix<T> mix,
 #pragma unroll
     for (int m = 0; m < RPT; ++m)
         v[m] = m >= RPT / 2 ? mk<T>(0, 0) : base[(size_t)(t + m * TT) * CT + cc];
-    block_fft<T, LC, RPT, -1, S, true>(v, t, sm, c, tw_lc);
+    block_fft<T, LC, RPT, -1, S, true, ALT>(v, t, sm, c, tw_lc);
     // every thread publishes its column's spectrum, then reads the other
     // field's column at the same kx (the forward transform's last stage ran
-    // in registers, after its last barrier: the workspace is free)
-    __syncthreads();
+    // in registers; with one workspace, after every thread's last read of it)
+    if constexpr (ALT == 0) __syncthreads();
 #pragma unroll
-    for (int m = 0; m < RPT; ++m) sm[smaddr(t + m * TT, S, c)] = v[m];
+    for (int m = 0; m < RPT; ++m) xs[smaddr(t + m * TT, S, c)] = v[m];
     __syncthreads();
     const int pc = f ? c - CT : c + CT;
     const int kx = tile * CT + cc;
 #pragma unroll
     for (int m = 0; m < RPT; ++m) {
         const int ky = t + m * TT;
-        v[m] = mix(f, v[m], sm[smaddr(ky, S, pc)], kx, ky);
+        v[m] = mix(f, v[m], xs[smaddr(ky, S, pc)], kx, ky);
     }
-    __syncthreads();  // the workspace is reused by the inverse transform
-    block_fft<T, LC, RPT, +1, S>(v, t, sm, c, tw_lc);
+    // one workspace: reused by the inverse transform; two: the inverse
+    // starts in the other one and reaches xs after its first barrier
+    if constexpr (ALT == 0) __syncthreads();
+    block_fft<T, LC, RPT, +1, S, false, ALT, ALT ? (PX ^ 1) : 0>(v, t, sm, c, tw_lc);
 #pragma unroll
     for (int m = 0; m < RPT / 2; ++m) base[(size_t)(t + m * TT) * CT + cc] = v[m];
 }
@@ -397,18 +424,20 @@ void TanOperator::apply(const T* q, T* u, cudaStream_t s) {
     const long bsp = (long)(LR / CT + 1) * NS * CT;
     cplx<T>* sp = static_cast<cplx<T>*>(spec[dbl]);
     // both fields' rows (instances 0 = q_x, 1 = q_y)
-    launch_row_fwd<T, LR, true, 0>(LoadRealRows<T>{q, NS, N}, StoreTiled<T>{sp, NS, CT, bsp}, NS,
+    constexpr int RV = tan_row_variant<T>(NS);
+    launch_row_fwd<T, LR, true, RV>(LoadRealRows<T>{q, NS, N}, StoreTiled<T>{sp, NS, CT, bsp}, NS,
                                    s, nullptr, 2);
     {
         constexpr int thr = 2 * CT * (LC / col_rpt<T>(LC, 0));
-        constexpr int sm = col_smem<T>(LC, 2 * CT);
+        constexpr int sm = col_pair_pp<T>(LC, CT) ? 2 * align16(col_smem<T>(LC, 2 * CT))
+                                                  : col_smem<T>(LC, 2 * CT);
         auto k = col_pair_kernel<T, LC, CT>;
         fft_attrs((const void*)k, sm);
         const TanMix<T> mix{static_cast<const T*>(kt[dbl][0]), static_cast<const T*>(kt[dbl][1]),
                             static_cast<const T*>(kt[dbl][2]), NS + 1, CT, LC};
         k<<<NS / CT + 1, thr, sm, s>>>(sp, bsp, NS, mix, tw<T>(LC));
     }
-    launch_row_inv<T, LR, true, 0>(LoadTiled<T>{sp, NS, CT, bsp}, StoreRealRows<T>{u, NS, N}, NS,
+    launch_row_inv<T, LR, true, RV>(LoadTiled<T>{sp, NS, CT, bsp}, StoreRealRows<T>{u, NS, N}, NS,
                                    s, nullptr, 2);
     count_launches(3);
     ASB_CUDA(cudaGetLastError());
