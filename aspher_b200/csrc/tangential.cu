@@ -533,14 +533,18 @@ __device__ __forceinline__ void tan_block_out(double (&v)[NV], const int (&kind)
 }
 
 // one block: out[j] = fold of part[b * nv + j] over b in block order
-__global__ void k_tan_fold(const double* __restrict__ part, int nb, int nv, const int* kinds,
+struct TanKinds {  // per value: 0 sum, 1 max
+    int k[8];
+};
+__global__ void k_tan_fold(const double* __restrict__ part, int nb, int nv, TanKinds kinds,
                            double* __restrict__ out) {
     const int j = threadIdx.x;
     if (j >= nv) return;
-    double a = kinds[j] ? -INFINITY : 0.0;
+    const int kind = kinds.k[j];
+    double a = kind ? -INFINITY : 0.0;
     for (int b = 0; b < nb; ++b) {
         const double x = part[b * nv + j];
-        a = kinds[j] ? fmax(a, x) : a + x;
+        a = kind ? fmax(a, x) : a + x;
     }
     out[j] = a;
 }
@@ -819,9 +823,13 @@ struct TanSolver {
     int grid;
     double *q = nullptr, *u = nullptr, *g = nullptr, *gp = nullptr, *z = nullptr, *t = nullptr,
            *r = nullptr, *qbest = nullptr, *qw = nullptr;
+    // block partials: part (the reduction just launched), part_dir (the
+    // direction pass's dots, folded with the evaluation's), part_q (the
+    // partition flag of the last update, folded with the next iteration's)
     double* part = nullptr;
-    double* red = nullptr;  // folded results
-    int* kinds = nullptr;
+    double* part_dir = nullptr;
+    double* part_q = nullptr;
+    double* red = nullptr;    // folded results
     double* red_h = nullptr;  // pinned host copy
     const double* s = nullptr;
     const double* hist = nullptr;
@@ -837,30 +845,37 @@ struct TanSolver {
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         double** vs[] = {&q, &u, &g, &gp, &z, &t, &r, &qbest, &qw};
         for (double** v : vs) ASB_CUDA(cudaMalloc((void**)v, 2 * N * sizeof(double)));
-        ASB_CUDA(cudaMalloc((void**)&part, (size_t)kTanMaxBlocks * 8 * sizeof(double)));
+        ASB_CUDA(cudaMalloc((void**)&part, (size_t)3 * kTanMaxBlocks * 8 * sizeof(double)));
+        part_dir = part + (size_t)kTanMaxBlocks * 8;
+        part_q = part + (size_t)2 * kTanMaxBlocks * 8;
         ASB_CUDA(cudaMalloc((void**)&red, 8 * sizeof(double)));
-        ASB_CUDA(cudaMalloc((void**)&kinds, 8 * sizeof(int)));
         ASB_CUDA(cudaMallocHost((void**)&red_h, 8 * sizeof(double)));
     }
     ~TanSolver() {
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
         double* vs[] = {q, u, g, gp, z, t, r, qbest, qw, part, red};
         for (double* v : vs) cudaFree(v);
-        cudaFree(kinds);
         cudaFreeHost(red_h);
+    }
+    // fold the block partials `src` (nv values, kinds) into red[at ...]
+    void fold_into(const double* src, int nv, std::initializer_list<int> kind, int at) {
+        TanKinds k{};
+        int j = 0;
+        for (int v : kind) k.k[j++] = v;
+        k_tan_fold<<<1, 32, 0, st>>>(src, grid, nv, k, red + at);
+        count_launches(1);
+    }
+    // bring red[0 .. n) to the host (one synchronisation)
+    const double* fetch(int n) {
+        ASB_CUDA(cudaMemcpyAsync(red_h, red, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        ASB_CUDA(cudaStreamSynchronize(st));
+        return red_h;
     }
     // fold the partials of the last reduction kernel (nv values, kinds) and
     // bring them to the host
     const double* fold(int nv, std::initializer_list<int> kind) {
-        int kh[8] = {0};
-        int j = 0;
-        for (int k : kind) kh[j++] = k;
-        ASB_CUDA(cudaMemcpyAsync(kinds, kh, sizeof(kh), cudaMemcpyHostToDevice, st));
-        k_tan_fold<<<1, 32, 0, st>>>(part, grid, nv, kinds, red);
-        ASB_CUDA(cudaMemcpyAsync(red_h, red, nv * sizeof(double), cudaMemcpyDeviceToHost, st));
-        ASB_CUDA(cudaStreamSynchronize(st));
-        count_launches(1);
-        return red_h;
+        fold_into(part, nv, kind, 0);
+        return fetch(nv);
     }
     void apply(const double* x, double* y) { op.matvec(true, x, y, st); }
 
@@ -877,12 +892,27 @@ struct TanSolver {
         int stall = 0;
         const int stall_limit = 200;
         int it = 0;
+        // the last update's partition flag, folded with the next evaluation
+        bool q_flag_pending = false;
+        // Two host synchronisations per iteration.  The direction pass needs
+        // g only, so it runs right after the evaluation and its dots come
+        // back with the evaluation's (a last iteration that stops on the
+        // evaluation discards them); the update's partition flag -- read by
+        // the next direction step only -- comes back with the next
+        // iteration's.  Every value and decision is the one-fold-at-a-time
+        // loop's.
         for (it = 0; it < max_iter; ++it) {
             apply(q, u);
             k_tan_eval<<<grid, kTanThreads, 0, st>>>(N, s, q, u, hist, dt.x, dt.y, g, part);
-            count_launches(1);
-            const double* ev = fold(2, {0, 1});
-            const double e = ev[0], gmax = ev[1];
+            k_tan_dir<<<grid, kTanThreads, 0, st>>>(N, s, q, g, gp, z, part_dir);
+            count_launches(2);
+            fold_into(part, 2, {0, 1}, 0);
+            fold_into(part_dir, 2, {0, 0}, 2);
+            if (q_flag_pending) fold_into(part_q, 1, {1}, 4);
+            const double* ev = fetch(q_flag_pending ? 5 : 4);
+            const double e = ev[0], gmax = ev[1], G = ev[2], G_pr = ev[3];
+            if (q_flag_pending) delta_conj = ev[4] > 0.0 ? 0.0 : 1.0;
+            q_flag_pending = false;
             if (it == 0) g_scale = std::max(gmax > 0.0 ? gmax : 1.0, g_floor);
             res.error = e / (Stotal * g_scale);
             if (res.error < err_best) {
@@ -904,11 +934,8 @@ struct TanSolver {
             }
             double num = 0.0, den = 0.0;
             for (int attempt = 0;; ++attempt) {
+                // a retry reuses z, G, G_pr: q, g and gp are unchanged
                 if (attempt == 1) delta_conj = 0.0;  // steepest descent
-                k_tan_dir<<<grid, kTanThreads, 0, st>>>(N, s, q, g, gp, z, part);
-                count_launches(1);
-                const double* dv = fold(2, {0, 0});
-                const double G = dv[0], G_pr = dv[1];
                 const double beta =
                     delta_conj * (use_pr ? std::max(0.0, G_pr / G_old) : G / G_old);
                 k_tan_tupd<<<grid, kTanThreads, 0, st>>>(N, s, z, beta, t);
@@ -928,9 +955,9 @@ struct TanSolver {
                 continue;
             }
             const double tau = num / den;
-            k_tan_qupd<<<grid, kTanThreads, 0, st>>>(N, s, t, tau, q, part);
+            k_tan_qupd<<<grid, kTanThreads, 0, st>>>(N, s, t, tau, q, part_q);
             count_launches(1);
-            delta_conj = fold(1, {1})[0] > 0.0 ? 0.0 : 1.0;
+            q_flag_pending = true;
         }
         // the best iterate seen (friction_solve.cpp:278-283)
         ASB_CUDA(cudaMemcpyAsync(q, qbest, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
