@@ -52,6 +52,48 @@ __device__ __forceinline__ cplx<T> rot_const(cplx<T> a, int k) {
     return mk<T>(a.x * c - a.y * sn, a.x * sn + a.y * c);
 }
 
+// cos and tan of 2 pi k / 16, k in {1, 2, 3, 5, 6, 7}, as plain
+// mathematical constants (tan(pi/8) = sqrt(2) - 1, tan(3 pi/8) = sqrt(2) + 1)
+template <typename T>
+__device__ __forceinline__ void unit16_cos_tan(int k, T& c, T& t) {
+    const T c1 = T(0.92387953251128675613), s1 = T(0.38268343236508977173);
+    const T h = T(0.70710678118654752440);
+    const T t1 = T(0.41421356237309504880), t3 = T(2.41421356237309504880);
+    switch (k) {
+        case 1: c = c1; t = t1; break;
+        case 2: c = h; t = T(1); break;
+        case 3: c = s1; t = t3; break;
+        case 5: c = -s1; t = -t3; break;
+        case 6: c = -h; t = T(-1); break;
+        default: c = -c1; t = -t1; break;
+    }
+}
+
+// The radix-2 butterfly with the odd input rotated by exp(DIR 2 pi i k / R):
+// lo = e + w o, hi = e - w o.  A general rotation is factored as
+// w o = c (o.x - t o.y, o.y + t o.x), t = tan of the angle (cos c != 0), and
+// the factor c is folded into the two outputs' fused multiply-adds: six
+// instructions instead of a four-instruction rotation and four additions.
+template <int R, int DIR, typename T>
+__device__ __forceinline__ void bfly_rot(cplx<T> e, cplx<T> o, int k, cplx<T>& lo, cplx<T>& hi) {
+    const int k16 = k * (16 / R);
+    if (k16 == 0) {
+        lo = cadd(e, o);
+        hi = csub(e, o);
+    } else if (k16 == 4) {
+        const cplx<T> w = mul_i<DIR>(o);
+        lo = cadd(e, w);
+        hi = csub(e, w);
+    } else {
+        T c, t;
+        unit16_cos_tan<T>(k16, c, t);
+        if (DIR < 0) t = -t;
+        const T ux = fma(-t, o.y, o.x), uy = fma(t, o.x, o.y);
+        lo = mk<T>(fma(c, ux, e.x), fma(c, uy, e.y));
+        hi = mk<T>(fma(-c, ux, e.x), fma(-c, uy, e.y));
+    }
+}
+
 // In-register DFT of R points (natural order in and out), radix-2 DIT split.
 template <int R, int DIR, typename T>
 __device__ __forceinline__ void dft(cplx<T>* a) {
@@ -76,11 +118,7 @@ __device__ __forceinline__ void dft(cplx<T>* a) {
         dft<R / 2, DIR, T>(e);
         dft<R / 2, DIR, T>(o);
 #pragma unroll
-        for (int k = 0; k < R / 2; ++k) {
-            const cplx<T> w = rot_const<R, DIR, T>(o[k], k);
-            a[k] = cadd(e[k], w);
-            a[k + R / 2] = csub(e[k], w);
-        }
+        for (int k = 0; k < R / 2; ++k) bfly_rot<R, DIR, T>(e[k], o[k], k, a[k], a[k + R / 2]);
     }
 }
 
