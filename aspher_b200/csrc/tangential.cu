@@ -575,10 +575,23 @@ __global__ void k_tan_start(long N, const double* __restrict__ s, const double* 
 
 // residual g = u + u_hist - delta on A and the KKT stationarity error
 // (friction_solve.cpp:93-125): [0] e, [1] max |g|
+// The per-iteration scalars of the loop kernels live in device memory (a
+// TanScalars record) so that the kernel sequences of an iteration can be
+// captured once and replayed as CUDA graphs.
+struct TanScalars {
+    double beta;    // conjugate-direction weight (k_tan_tupd)
+    double tau;     // step (k_tan_qupd)
+    double skip;    // nonzero: k_tan_qupd leaves q unchanged
+    double dx, dy;  // the imposed shift (k_tan_eval)
+};
+
+// residual g = u + u_hist - delta on A and the KKT stationarity error
+// (friction_solve.cpp:93-125): [0] e, [1] max |g|
 __global__ void __launch_bounds__(kTanThreads) k_tan_eval(
     long N, const double* __restrict__ s, const double* __restrict__ q,
-    const double* __restrict__ u, const double* __restrict__ hist, double dx, double dy,
-    double* __restrict__ g, double* part) {
+    const double* __restrict__ u, const double* __restrict__ hist,
+    const TanScalars* __restrict__ sc, double* __restrict__ g, double* part) {
+    const double dx = sc->dx, dy = sc->dy;
     double v[2] = {0.0, 0.0};
     TAN_LOOP(N) {
         const double si = s[i];
@@ -644,7 +657,8 @@ __global__ void __launch_bounds__(kTanThreads) k_tan_dir(
 
 // t = chi_A (z + beta t)
 __global__ void k_tan_tupd(long N, const double* __restrict__ s, const double* __restrict__ z,
-                           double beta, double* __restrict__ t) {
+                           const TanScalars* __restrict__ sc, double* __restrict__ t) {
+    const double beta = sc->beta;
     TAN_LOOP(N) {
         const bool a = s[i] > 0.0;
         t[i] = a ? z[i] + beta * t[i] : 0.0;
@@ -669,8 +683,10 @@ __global__ void __launch_bounds__(kTanThreads) k_tan_numden(
 // q <- clamp(q - tau t) on A; [0] partition changed (max)
 // (friction_solve.cpp:258-276)
 __global__ void __launch_bounds__(kTanThreads) k_tan_qupd(
-    long N, const double* __restrict__ s, const double* __restrict__ t, double tau,
-    double* __restrict__ q, double* part) {
+    long N, const double* __restrict__ s, const double* __restrict__ t,
+    const TanScalars* __restrict__ sc, double* __restrict__ q, double* part) {
+    if (sc->skip != 0.0) return;  // no update this iteration (partials unused)
+    const double tau = sc->tau;
     double v[1] = {0.0};
     TAN_LOOP(N) {
         const double si = s[i];
@@ -831,6 +847,19 @@ struct TanSolver {
     double* part_q = nullptr;
     double* red = nullptr;    // folded results
     double* red_h = nullptr;  // pinned host copy
+    // the loop kernels' scalars: written on the host (pinned), copied to the
+    // device by the iteration's first node
+    TanScalars* sc_d = nullptr;
+    TanScalars* sc_h = nullptr;
+    // The two kernel sequences of an iteration, captured once (on a private
+    // stream: a caller's legacy stream cannot capture) and replayed on st:
+    // [0] the previous iteration's update, the apply, the evaluation, the
+    // direction pass and their folds; [1] the direction update, the apply of
+    // t, the line-search dots and their fold.  Their buffers and the scalars
+    // record are fixed for the solver's lifetime.
+    cudaGraph_t seg_graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t seg_exec[2] = {nullptr, nullptr};
+    bool seg_ran[2] = {false, false};
     const double* s = nullptr;
     const double* hist = nullptr;
     double Stotal = 0.0;
@@ -850,20 +879,99 @@ struct TanSolver {
         part_q = part + (size_t)2 * kTanMaxBlocks * 8;
         ASB_CUDA(cudaMalloc((void**)&red, 8 * sizeof(double)));
         ASB_CUDA(cudaMallocHost((void**)&red_h, 8 * sizeof(double)));
+        ASB_CUDA(cudaMalloc((void**)&sc_d, sizeof(TanScalars)));
+        ASB_CUDA(cudaMallocHost((void**)&sc_h, sizeof(TanScalars)));
+        *sc_h = TanScalars{};
     }
     ~TanSolver() {
         std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+        for (int k = 0; k < 2; ++k) {
+            if (seg_exec[k]) cudaGraphExecDestroy(seg_exec[k]);
+            if (seg_graph[k]) cudaGraphDestroy(seg_graph[k]);
+        }
         double* vs[] = {q, u, g, gp, z, t, r, qbest, qw, part, red};
         for (double* v : vs) cudaFree(v);
+        cudaFree(sc_d);
         cudaFreeHost(red_h);
+        cudaFreeHost(sc_h);
     }
     // fold the block partials `src` (nv values, kinds) into red[at ...]
-    void fold_into(const double* src, int nv, std::initializer_list<int> kind, int at) {
+    void fold_into(const double* src, int nv, std::initializer_list<int> kind, int at,
+                   cudaStream_t ss = nullptr) {
         TanKinds k{};
         int j = 0;
         for (int v : kind) k.k[j++] = v;
-        k_tan_fold<<<1, 32, 0, st>>>(src, grid, nv, k, red + at);
+        k_tan_fold<<<1, 32, 0, ss ? ss : st>>>(src, grid, nv, k, red + at);
         count_launches(1);
+    }
+    // the scalars record, host -> device (pinned source, read when the copy
+    // runs: the host writes it only while no segment is in flight)
+    void put_scalars(cudaStream_t ss) {
+        ASB_CUDA(cudaMemcpyAsync(sc_d, sc_h, sizeof(TanScalars), cudaMemcpyHostToDevice, ss));
+    }
+    // segment 0 of iteration k >= 1 (iteration 0 has no update to apply and
+    // runs its evaluation eagerly): gp <- g (the previous iteration's g), the
+    // previous iteration's update unless sc.skip, then the evaluation and the
+    // direction pass; red[0..4] = e, max |g|, G, G_pr, partition flag
+    void enqueue_seg0(cudaStream_t ss) {
+        ASB_CUDA(cudaMemcpyAsync(gp, g, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, ss));
+        put_scalars(ss);
+        k_tan_qupd<<<grid, kTanThreads, 0, ss>>>(N, s, t, sc_d, q, part_q);
+        op.matvec(true, q, u, ss);
+        k_tan_eval<<<grid, kTanThreads, 0, ss>>>(N, s, q, u, hist, sc_d, g, part);
+        k_tan_dir<<<grid, kTanThreads, 0, ss>>>(N, s, q, g, gp, z, part_dir);
+        count_launches(3);
+        fold_into(part, 2, {0, 1}, 0, ss);
+        fold_into(part_dir, 2, {0, 0}, 2, ss);
+        fold_into(part_q, 1, {1}, 4, ss);
+        ASB_CUDA(cudaMemcpyAsync(red_h, red, 5 * sizeof(double), cudaMemcpyDeviceToHost, ss));
+    }
+    // segment 1: t = chi_A (z + beta t), r = S t, red[0..1] = num, den
+    void enqueue_seg1(cudaStream_t ss) {
+        put_scalars(ss);
+        k_tan_tupd<<<grid, kTanThreads, 0, ss>>>(N, s, z, sc_d, t);
+        op.matvec(true, t, r, ss);
+        k_tan_numden<<<grid, kTanThreads, 0, ss>>>(N, s, g, t, r, part);
+        count_launches(2);
+        fold_into(part, 2, {0, 0}, 0, ss);
+        ASB_CUDA(cudaMemcpyAsync(red_h, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, ss));
+    }
+    // run segment k and wait for it: the first time kernel by kernel (every
+    // kernel in it then has been loaded and set up outside any capture),
+    // then captured once and replayed
+    const double* run_seg(int k) {
+        if (!seg_ran[k]) {
+            if (k == 0) enqueue_seg0(st);
+            else enqueue_seg1(st);
+            ASB_CUDA(cudaGetLastError());
+            ASB_CUDA(cudaStreamSynchronize(st));
+            seg_ran[k] = true;
+            return red_h;
+        }
+        if (!seg_exec[k]) {
+            std::lock_guard<std::recursive_mutex> setup(setup_mutex());
+            cudaStream_t cs = nullptr;
+            ASB_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+            ASB_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeRelaxed));
+            try {
+                if (k == 0) enqueue_seg0(cs);
+                else enqueue_seg1(cs);
+            } catch (...) {
+                cudaGraph_t partial = nullptr;
+                cudaStreamEndCapture(cs, &partial);
+                if (partial) cudaGraphDestroy(partial);
+                cudaGetLastError();
+                cudaStreamDestroy(cs);
+                throw;
+            }
+            ASB_CUDA(cudaStreamEndCapture(cs, &seg_graph[k]));
+            ASB_CUDA(cudaStreamDestroy(cs));
+            ASB_CUDA(cudaGraphInstantiate(&seg_exec[k], seg_graph[k], 0));
+        }
+        ASB_CUDA(cudaGraphLaunch(seg_exec[k], st));
+        count_launches(1);
+        ASB_CUDA(cudaStreamSynchronize(st));
+        return red_h;
     }
     // bring red[0 .. n) to the host (one synchronisation)
     const double* fetch(int n) {
@@ -892,27 +1000,32 @@ struct TanSolver {
         int stall = 0;
         const int stall_limit = 200;
         int it = 0;
-        // the last update's partition flag, folded with the next evaluation
-        bool q_flag_pending = false;
-        // Two host synchronisations per iteration.  The direction pass needs
-        // g only, so it runs right after the evaluation and its dots come
-        // back with the evaluation's (a last iteration that stops on the
-        // evaluation discards them); the update's partition flag -- read by
-        // the next direction step only -- comes back with the next
-        // iteration's.  Every value and decision is the one-fold-at-a-time
-        // loop's.
+        // The iteration's kernels run as two segments (enqueue_seg0 / seg1),
+        // one host synchronisation each.  Segment 0 applies the previous
+        // iteration's update first, so a loop that stops (converged,
+        // stalled, out of iterations) never evaluates an update it would
+        // discard: q returns to the best evaluated iterate below either way.
+        // Every value and decision is the plain loop's.
+        sc_h->dx = dt.x;
+        sc_h->dy = dt.y;
+        sc_h->skip = 1.0;
+        bool q_flag_pending = false;  // segment 0 folds an update's partition flag
+        // iteration 0: no update to apply
+        put_scalars(st);
+        apply(q, u);
+        k_tan_eval<<<grid, kTanThreads, 0, st>>>(N, s, q, u, hist, sc_d, g, part);
+        k_tan_dir<<<grid, kTanThreads, 0, st>>>(N, s, q, g, gp, z, part_dir);
+        count_launches(2);
+        fold_into(part, 2, {0, 1}, 0);
+        fold_into(part_dir, 2, {0, 0}, 2);
+        const double* ev = fetch(4);
         for (it = 0; it < max_iter; ++it) {
-            apply(q, u);
-            k_tan_eval<<<grid, kTanThreads, 0, st>>>(N, s, q, u, hist, dt.x, dt.y, g, part);
-            k_tan_dir<<<grid, kTanThreads, 0, st>>>(N, s, q, g, gp, z, part_dir);
-            count_launches(2);
-            fold_into(part, 2, {0, 1}, 0);
-            fold_into(part_dir, 2, {0, 0}, 2);
-            if (q_flag_pending) fold_into(part_q, 1, {1}, 4);
-            const double* ev = fetch(q_flag_pending ? 5 : 4);
+            if (it > 0) {
+                ev = run_seg(0);
+                if (q_flag_pending) delta_conj = ev[4] > 0.0 ? 0.0 : 1.0;
+                q_flag_pending = false;
+            }
             const double e = ev[0], gmax = ev[1], G = ev[2], G_pr = ev[3];
-            if (q_flag_pending) delta_conj = ev[4] > 0.0 ? 0.0 : 1.0;
-            q_flag_pending = false;
             if (it == 0) g_scale = std::max(gmax > 0.0 ? gmax : 1.0, g_floor);
             res.error = e / (Stotal * g_scale);
             if (res.error < err_best) {
@@ -936,27 +1049,20 @@ struct TanSolver {
             for (int attempt = 0;; ++attempt) {
                 // a retry reuses z, G, G_pr: q, g and gp are unchanged
                 if (attempt == 1) delta_conj = 0.0;  // steepest descent
-                const double beta =
-                    delta_conj * (use_pr ? std::max(0.0, G_pr / G_old) : G / G_old);
-                k_tan_tupd<<<grid, kTanThreads, 0, st>>>(N, s, z, beta, t);
-                count_launches(1);
+                sc_h->beta = delta_conj * (use_pr ? std::max(0.0, G_pr / G_old) : G / G_old);
                 G_old = G > 0.0 ? G : 1.0;
-                apply(t, r);
-                k_tan_numden<<<grid, kTanThreads, 0, st>>>(N, s, g, t, r, part);
-                count_launches(1);
-                const double* nd = fold(2, {0, 0});
+                const double* nd = run_seg(1);
                 num = nd[0];
                 den = nd[1];
                 if (num > 0.0 || attempt == 1) break;
             }
-            ASB_CUDA(cudaMemcpyAsync(gp, g, 2 * N * sizeof(double), cudaMemcpyDeviceToDevice, st));
             if (den <= 0.0 || num <= 0.0) {
                 delta_conj = 0.0;
+                sc_h->skip = 1.0;
                 continue;
             }
-            const double tau = num / den;
-            k_tan_qupd<<<grid, kTanThreads, 0, st>>>(N, s, t, tau, q, part_q);
-            count_launches(1);
+            sc_h->tau = num / den;
+            sc_h->skip = 0.0;
             q_flag_pending = true;
         }
         // the best iterate seen (friction_solve.cpp:278-283)
