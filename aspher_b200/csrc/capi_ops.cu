@@ -103,6 +103,8 @@ int aspher_op_get_info(const aspher_op* op, aspher_op_info* info) {
     info->n = (int64_t)o.Nl * o.Nl;
     if (o.kind == asb::OP_FFT)
         info->bytes_spectrum = (int64_t)(o.Ns + 16) * (o.Ns + 1) * 12 + (int64_t)(o.Ns + 1) * (o.Ns + 1) * 8;
+    else  // the periodic multiplier tables (FP32, and FP64 where FP64 applies exist)
+        info->bytes_spectrum = (int64_t)(o.Ns / 2 + 16) * (o.Ns / 2 + 1) * (o.psym_d ? 12 : 4);
     info->bytes_scratch = (int64_t)(o.spec_d_bytes + o.spec_f_bytes);
     info->bytes_total = (int64_t)o.resident_bytes();
     info->max_im_ratio = o.max_im_ratio;

@@ -484,12 +484,21 @@ struct PeriodicImpl {
         }
     }
 
+    // the multiplier scale / |m| from the operator's table of this precision
+    // (the values PeriodicMult forms per element, one load instead of an
+    // FP64 square root and division)
+    static KhMult<T> mult(const Operator& op) {
+        const int dbl = sizeof(T) == 8;
+        const T* tab = dbl ? (const T*)(const void*)op.psym_d : (const T*)(const void*)op.psym_f;
+        return KhMult<T>{tab, NS / 2 + 1, NS, op.ct[dbl]};
+    }
+
     static void matvec(const Operator& op, const T* x, T* y, cplx<T>* spec, cudaStream_t s,
                        const int* gate, int B, const PkState* sc) {
         const int dbl = sizeof(T) == 8;
         const long bx = (long)NS * NS;
-        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS, bx, sc},
-              PeriodicMult<T>{op.scale, NS}, StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
+        apply(op.rowv[dbl], op.colv[dbl], LoadRealRows<T>{x, NS, bx, sc}, mult(op),
+              StoreRealRows<T>{y, NS, bx}, spec, s, gate, B);
     }
 };
 
@@ -777,6 +786,26 @@ __global__ void k_retile_kh(int Ns, const double* __restrict__ canon, int ct_d,
     }
 }
 
+// The periodic multiplier (periodic_fft_operator.cpp:34-47) as a table:
+// w(kx, kf) = scale / sqrt(kx^2 + kf^2) in FP64 (0 at the mean), the value
+// PeriodicMult forms per element, for kx in [0, ncols) (columns past Ns/2
+// pad the last tile: 0) and kf = |m_y| in [0, Ns/2], tiled for column tile
+// width ct as Kh is: [kx / ct][kf][kx % ct]
+__global__ void k_periodic_symbol(int Ns, double scale, int ncols, int ct,
+                                  double* __restrict__ sd, float* __restrict__ sf) {
+    const int nk = Ns / 2 + 1;
+    const long n = (long)ncols * nk;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x) {
+        const int kf = (int)(i / ncols), kx = (int)(i % ncols);
+        const double m2 = (double)kx * kx + (double)kf * kf;
+        const double w = (kx <= Ns / 2 && m2 > 0.0) ? scale / sqrt(m2) : 0.0;
+        const size_t at = (size_t)(kx / ct) * nk * ct + (size_t)kf * ct + (kx % ct);
+        if (sd) sd[at] = w;
+        if (sf) sf[at] = (float)w;
+    }
+}
+
 // ----------------------------------------------------------------------------
 // size dispatch
 // ----------------------------------------------------------------------------
@@ -840,6 +869,10 @@ Operator::Operator(int kind_, int Ns_, double L_, double E_, int flags)
         }
         ASB_CUDA(cudaMalloc(&kh_f, nt * sizeof(float)));
         ASB_CUDA(cudaMemset(kh_f, 0, nt * sizeof(float)));
+    } else {
+        const size_t nt = (size_t)(Ns / 2 + 16) * (Ns / 2 + 1);  // widest tiling
+        if (supports(true)) ASB_CUDA(cudaMalloc(&psym_d, nt * sizeof(double)));
+        ASB_CUDA(cudaMalloc(&psym_f, nt * sizeof(float)));
     }
     for (int dbl = 0; dbl < 2; ++dbl) {
         int rv = 0, cv = 0;
@@ -862,6 +895,8 @@ Operator::~Operator() {
     cudaFree(kh_d);
     cudaFree(kh_f);
     cudaFree(kh_canon);
+    cudaFree(psym_d);
+    cudaFree(psym_f);
     cudaFree(spec_d);
     cudaFree(spec_f);
     cudaFree(table);
@@ -892,6 +927,14 @@ void Operator::set_variants(bool dbl, int rv, int cv) {
         if (khp_canon)
             k_retile_kh<<<1184, 256>>>(Ns, khp_canon, c, dbl ? khp_d : nullptr, c,
                                        dbl ? nullptr : khp_f);
+        ASB_CUDA(cudaGetLastError());
+        ASB_CUDA(cudaDeviceSynchronize());
+    }
+    if (kind == OP_PERIODIC && c != ct[dbl] && (dbl ? psym_d != nullptr : true)) {
+        // the multiplier table of this precision for the new tile width
+        const int ncols = (Ns / 2 / c + 1) * c;
+        k_periodic_symbol<<<1184, 256>>>(Ns, scale, ncols, c, dbl ? psym_d : nullptr,
+                                         dbl ? nullptr : psym_f);
         ASB_CUDA(cudaGetLastError());
         ASB_CUDA(cudaDeviceSynchronize());
     }
@@ -993,6 +1036,9 @@ size_t Operator::resident_bytes() const {
         n += nt * (sizeof(double) + sizeof(float));
         n += (size_t)(Ns + 1) * (Ns + 1) * sizeof(double);  // canonical Kh
         n += (size_t)Ns * Ns * sizeof(double);              // Love table
+    } else {
+        const size_t nt = (size_t)(Ns / 2 + 16) * (Ns / 2 + 1);  // multiplier tables
+        n += nt * ((psym_d ? sizeof(double) : 0) + sizeof(float));
     }
     return n;
 }
@@ -1048,7 +1094,7 @@ void Operator::matvec_defect(const double* x, const double* x0, double* y, const
     } else {
         ASB_SIZE_SWITCH(Ns, PeriodicImpl<float, NS>::apply(
                                 rowv[0], colv[0], LoadDiffRows{x, x0, NS, bx, sc},
-                                PeriodicMult<float>{scale, NS}, StoreAddRows{y, y0, NS, bx},
+                                PeriodicImpl<float, NS>::mult(*this), StoreAddRows{y, y0, NS, bx},
                                 (float2*)spec, s, gate, B));
     }
 }

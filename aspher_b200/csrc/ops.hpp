@@ -120,6 +120,11 @@ struct Operator {
     double* kh_canon = nullptr;
     double* kh_d = nullptr;
     float* kh_f = nullptr;
+    // periodic (power-of-two grid): the multiplier scale / |m| over
+    // kx in [0, Ns/2] and |m_y| in [0, Ns/2], evaluated in FP64 and rounded
+    // to each precision once, tiled like Kh for the active column tile width
+    double* psym_d = nullptr;
+    float* psym_f = nullptr;
     double max_im_ratio = 0.0;
     // launch variants per precision [F32, F64] and the column tile width
     // (half-spectrum layout) they imply
